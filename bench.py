@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark of the CK-MPM substep on B200: particle-substeps/s.
+
+Workload: sand column collapse -- Drucker-Prager sand, dx = 1/256 (64^3 blocks),
+cylinder r = 0.1, h = 0.4 on a slip floor, 8 particles per cell (~1.69M
+particles), dt = 5e-5, seeded synthetic particles.  A step is one substep of
+every particle.  Particle state (~190 MB) is larger than L2, so no L2 flush is
+needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun: each rank simulates an independent replica of the
+scene (the plain substep has no cross-GPU exchange), value is the aggregate.
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-substeps/s"
+WORKLOAD = "sand_column_collapse: drucker-prager, dx=1/256 (64^3 blocks), cylinder r=0.1 h=0.4, 8 ppc, dt=5e-5, slip floor"
+STATE_BYTES = {0: 48, 2: 52, 3: 16}  # x + F (+ logJp) or x + J, read once and written once per substep
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--profile-steps", type=int, default=200)
+    ap.add_argument("--e2e-frame", type=int, default=100, help="substeps between position exports in the e2e run")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str):
+        self.device_id = device_id
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.device_id, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def device_uuid(local_rank: int) -> str:
+    try:
+        import torch
+        u = torch.cuda.get_device_properties(local_rank).uuid
+        s = str(u)
+        return s if s.startswith("GPU-") else f"GPU-{s}"
+    except Exception:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        return vis.split(",")[local_rank] if vis else str(local_rank)
+
+
+def measured_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def committed_traffic() -> float | None:
+    """DRAM bytes per fused launch from the committed ncu summary, scaled to this workload."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return float(d["dram_bytes_per_particle"]) if "dram_bytes_per_particle" in d else None
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------- CPU baselines
+def cpu_baseline_oracle(cfg, models, seconds: float) -> dict:
+    """FP64 oracle (the reference algorithm restated serially) on the bench workload."""
+    from oracle import oracle as O
+    o = O.OracleScene(cfg, models)
+    o.setup()
+    n = sum(len(m.particle_position) for m in models)
+    dt = cfg.dt
+    t0 = time.perf_counter()
+    o.step(1, dt)
+    t1 = time.perf_counter() - t0
+    k = int(max(1, min(16, seconds / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    o.step(k, dt)
+    t = time.perf_counter() - t0
+    o.close()
+    return {"value": n * k / t, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"FP64 serial oracle (oracle/ckmpm_oracle.cpp), {k} substeps of the full {n}-particle scene "
+                      f"after one untimed substep, {t:.1f} s"}
+
+
+def cpu_baseline_pic(seconds: float) -> dict:
+    """python-src PIC demo restated in C++/OpenMP on the jelly cube, all host threads."""
+    import ctypes as C
+
+    from ckmpm_b200 import scenes
+    from oracle import oracle as O
+    O.build()
+    L = C.CDLL(str(O.PIC_LIB))
+    f = C.POINTER(C.c_float)
+    L.pic_run.restype = C.c_double
+    L.pic_run.argtypes = [C.c_int, f, f, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                          C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int)]
+    cfg, models = scenes.jelly_cube()
+    x = models[0].particle_position.copy()
+    v = models[0].particle_velocity.copy()
+    th = C.c_int()
+    steps = 50
+    t = L.pic_run(len(x), x.ctypes.data_as(f), v.ctypes.data_as(f), 1, 64, 5e4, 0.3, 1000.0, -9.8, 8, 1e-4, steps, 0,
+                  C.byref(th))
+    steps = int(max(50, min(5000, steps * seconds / max(t, 1e-6))))
+    x = models[0].particle_position.copy()
+    t = L.pic_run(len(x), x.ctypes.data_as(f), v.ctypes.data_as(f), 1, 64, 5e4, 0.3, 1000.0, -9.8, 8, 1e-4, steps, 0,
+                  C.byref(th))
+    return {"value": len(x) * steps / t, "unit": METRIC, "cores": th.value, "kind": "port",
+            "sample": f"python-src PIC CK-MPM restated in C++/OpenMP, jelly cube dx=1/64 ({len(x)} particles, "
+                      f"fixed-corotated), {steps} substeps"}
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from ckmpm_b200 import Scene, scenes
+
+    torch.cuda.set_device(local_rank)
+    # A side stream: the legacy default stream cannot be captured into a CUDA graph.
+    stream = torch.cuda.Stream()
+    cfg, models = scenes.sand_column(track_ids=False)
+    cfg.device = local_rank
+    dt = cfg.dt
+    n_total = sum(len(m.particle_position) for m in models)
+
+    # ---- device-resident throughput
+    s = Scene(cfg)
+    s.set_stream(stream.cuda_stream)
+    for m in models:
+        s.add_model(m)
+    s.setup()
+    s.step(args.warmup, dt)
+    n_live = sum(s.count(i) for i in range(len(models)))
+    sampler = ClockSampler(device_uuid(local_rank))
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    s.step_async(args.steps, dt)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    s.status_check()
+    ms = ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n_live * args.steps / (ms / 1e3)
+
+    # ---- per-kernel timing for the roofline (second pass, same scene, events per launch)
+    fused_ms, other_ms, launches = s.step_profiled(args.profile_steps, dt)
+    avg_fused = fused_ms / max(launches, 1)
+    grid_blocks = len(s.blocks(-1, 1)[0])
+    S = STATE_BYTES[models[0].material.kind_code]
+    alg_bytes = n_live * (2 * S + 8) + 7168 * grid_blocks
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / (avg_fused / 1e3) / 1e9
+    tpp = committed_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (tpp * n_live) if tpp else None,
+                "kernel": "g2p2g_kernel<DruckerPrager> (fused grid update + G2P + SVD/return map + rebin + P2G)",
+                "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_fused,
+                "peak_source": f"{peak_kind} hbm_gbs", "fused_share": fused_ms / max(fused_ms + other_ms, 1e-9)}
+    s.close()
+
+    # ---- end to end through the public API with host buffers
+    s2 = Scene(cfg)
+    s2.set_stream(stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for m in models:
+        s2.add_model(m)
+    s2.setup()
+    exports = 0
+    xbuf = np.zeros((n_total, 3), np.float32)
+    from ckmpm_b200 import _capi as capi
+    import ctypes as C
+    L = capi.lib()
+    nout = C.c_uint32()
+    for k in range(args.steps):
+        s2.step(1, dt)  # one substep + device->host read of its status word
+        if (k + 1) % args.e2e_frame == 0:
+            capi.check(L.ckmpm_get_state(s2._h, 0, capi.fptr(xbuf), None, None, None, None, n_total, C.byref(nout)),
+                       "ckmpm_get_state", s2._h)
+            exports += 1
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    s2.close()
+    e2e = {"value": world * n_live * args.steps / (e2e_ms / 1e3), "unit": METRIC,
+           "h2d_bytes_per_step": (n_total * 12 + 12) / args.steps,
+           "d2h_bytes_per_step": 64 + exports * (n_live * 12 + 4) / args.steps,
+           "includes": "setup (upload of x, v; binning; initial grid), every substep's status read, "
+                       f"a position export every {args.e2e_frame} substeps"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jittered lattice, numpy PCG64 seed 0)",
+        "config": {"workload": WORKLOAD, "particles": n_live, "grid_blocks": grid_blocks, "dt": dt,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "particle state ~190 MB > 126 MB L2: no flush"},
+        "roofline": roofline, "e2e": e2e, "clocks": clocks,
+        "gpu_launches": 1 + args.steps * (3 * len(models) + 1),
+    }
+    return line
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference CUDA build driven through its own MPMEngine API
+    (oracle/_ref, built from the reference's headers) when present, otherwise the
+    FP64 port of its algorithm on a bounded sample."""
+    from ckmpm_b200 import scenes
+    cfg, models = scenes.sand_column(track_ids=False)
+    harness = ROOT / "oracle" / "_ref" / "ref_sand"
+    if harness.exists():
+        from oracle import ref_runner
+        res = ref_runner.time_reference("sand", cfg, models, args.steps, args.warmup)
+        value = res["value"]
+        cpu = {"value": value, "unit": METRIC, "cores": 1, "kind": "reference", "sample": res["sample"]}
+    else:
+        cpu = cpu_baseline_oracle(cfg, models, args.cpu_seconds)
+        cpu["kind"] = "port"
+        value = cpu["value"]
+    return {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded jittered lattice, numpy PCG64 seed 0)",
+            "config": {"workload": WORKLOAD, "particles": sum(len(m.particle_position) for m in models)},
+            "impl": "reference", "cpu_baseline": cpu,
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        print(json.dumps(run_reference(args, rank, world)), flush=True)
+        return
+    if world > 1:
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    line = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            from ckmpm_b200 import scenes
+            cfg, models = scenes.sand_column(track_ids=False)
+            line["cpu_baseline"] = cpu_baseline_oracle(cfg, models, args.cpu_seconds)
+            line["cpu_pic_baseline"] = cpu_baseline_pic(min(args.cpu_seconds, 10.0))
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

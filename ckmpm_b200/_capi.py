@@ -1,0 +1,139 @@
+"""ctypes binding of the C ABI in include/ckmpm.h.
+
+The CUDA library is required: importing a function from here loads
+ckmpm_b200/_lib/libckmpm_b200.so and raises if it is missing.  There is no CPU
+fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libckmpm_b200.so"
+
+CKMPM_OK = 0
+STATUS_NAMES = {
+    0: "CKMPM_OK",
+    1: "CKMPM_ERR_INVALID",
+    2: "CKMPM_ERR_CUDA",
+    3: "CKMPM_ERR_CAPACITY",
+    4: "CKMPM_ERR_NUMERIC",
+    5: "CKMPM_ERR_TIMEOUT",
+    6: "CKMPM_ERR_NOT_FOUND",
+}
+
+FIXED_COROTATED = 0
+DRUCKER_PRAGER = 2
+FLUID = 3
+
+BOUNDARY_STICKY_BLOCKS = 0
+BOUNDARY_SLIP_FLOOR = 1
+
+FLAG_TRACK_IDS = 1
+
+# Every symbol include/ckmpm.h declares.
+EXPORTED = (
+    "ckmpm_create", "ckmpm_add_model", "ckmpm_setup", "ckmpm_step", "ckmpm_step_async",
+    "ckmpm_status_check", "ckmpm_step_adaptive", "ckmpm_set_stream", "ckmpm_get_count",
+    "ckmpm_get_state", "ckmpm_get_blocks", "ckmpm_get_counters", "ckmpm_get_dt",
+    "ckmpm_step_profiled", "ckmpm_debug_constitutive", "ckmpm_destroy", "ckmpm_last_error",
+    "ckmpm_version",
+)
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("dx", C.c_float),
+        ("domain_blocks", C.c_int32 * 3),
+        ("gravity", C.c_float),
+        ("mass_clamp", C.c_float),
+        ("boundary", C.c_int32),
+        ("floor_cells", C.c_float),
+        ("max_particles_per_block", C.c_uint32),
+        ("device", C.c_int32),
+        ("flags", C.c_uint32),
+    ]
+
+
+class Material(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("p", C.c_float * 4)]
+
+
+class CkmpmError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where}: {STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load the CUDA engine; raise loudly if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build the CUDA engine first (python -m ckmpm_b200.build). "
+                "There is no CPU fallback.")
+        L = C.CDLL(str(LIB_PATH))
+        P = C.c_void_p
+        f32p = C.POINTER(C.c_float)
+        u32p = C.POINTER(C.c_uint32)
+        i32p = C.POINTER(C.c_int32)
+        L.ckmpm_create.argtypes = [C.POINTER(SceneDesc), C.POINTER(P)]
+        L.ckmpm_add_model.argtypes = [P, C.POINTER(Material), C.c_uint32, f32p, f32p, C.c_uint32, C.c_float,
+                                      C.c_float, i32p]
+        L.ckmpm_setup.argtypes = [P]
+        L.ckmpm_step.argtypes = [P, C.c_uint32, C.c_float]
+        L.ckmpm_step_async.argtypes = [P, C.c_uint32, C.c_float]
+        L.ckmpm_status_check.argtypes = [P]
+        L.ckmpm_step_adaptive.argtypes = [P, C.c_uint32, C.c_float, C.c_float, C.c_double, C.POINTER(C.c_double)]
+        L.ckmpm_set_stream.argtypes = [P, P]
+        L.ckmpm_get_count.argtypes = [P, C.c_int32, u32p]
+        L.ckmpm_get_state.argtypes = [P, C.c_int32, f32p, f32p, f32p, f32p, u32p, C.c_uint32, u32p]
+        L.ckmpm_get_blocks.argtypes = [P, C.c_int32, C.c_int32, i32p, u32p, C.c_uint32, u32p]
+        L.ckmpm_get_counters.argtypes = [P, C.POINTER(C.c_uint64)]
+        L.ckmpm_get_dt.argtypes = [P, f32p]
+        L.ckmpm_step_profiled.argtypes = [P, C.c_uint32, C.c_float, C.POINTER(C.c_double)]
+        L.ckmpm_debug_constitutive.argtypes = [C.POINTER(Material), C.c_uint32, f32p, C.c_float, f32p, f32p, f32p,
+                                               f32p, f32p, f32p]
+        L.ckmpm_destroy.argtypes = [P]
+        L.ckmpm_last_error.argtypes = [P]
+        L.ckmpm_last_error.restype = C.c_char_p
+        L.ckmpm_version.restype = C.c_char_p
+        for name in EXPORTED:
+            fn = getattr(L, name)
+            if name not in ("ckmpm_last_error", "ckmpm_version"):
+                fn.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def fptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def uptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.uint32 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def iptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def check(code: int, where: str, handle=None) -> None:
+    if code != CKMPM_OK:
+        msg = lib().ckmpm_last_error(handle)
+        raise CkmpmError(code, where, msg.decode() if msg else "")

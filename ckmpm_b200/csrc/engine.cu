@@ -1,0 +1,705 @@
+// Host side of the B200 CK-MPM engine: scene/model lifetime, device memory,
+// setup, CUDA-graph substep replay and the C ABI declared in include/ckmpm.h.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/ckmpm.h"
+#include "kernels.cuh"
+
+using namespace ckmpm;
+
+namespace {
+
+constexpr int kFusedThreads = 256;
+constexpr int kProbeThreads = 256;
+constexpr int kGraphChunk = 8;
+constexpr const char* kVersion = "ckmpm-b200 0.1.0";
+
+thread_local std::string g_create_error;
+
+struct ModelHost {
+  ckmpm_material mat{};
+  float mass = 0.f, vol = 0.f;
+  uint32_t n = 0;       // particles passed in
+  uint32_t n_valid = 0; // particles binned at setup
+  std::vector<float> x, v;
+  uint32_t nv = 0;
+  ModelDev dev{};
+  uint32_t ntiles = 0;
+  // Export buffers (device), allocated on the first ckmpm_get_state.
+  float* ox = nullptr;
+  float* ov = nullptr;
+  float* oF = nullptr;
+  float* oaux = nullptr;
+  uint32_t* oid = nullptr;
+  std::vector<float> hx, hv, hF, ha;
+  std::vector<uint32_t> hid;
+};
+
+}  // namespace
+
+struct ckmpm_scene {
+  ckmpm_scene_desc desc{};
+  SceneDev sc{};
+  std::vector<ModelHost> models;
+  GridDev grid{};
+  Scalars* scal = nullptr;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  bool setup_done = false;
+  std::string err;
+  int sm_count = 0;
+  int fused_ctas = 0;
+  std::vector<void*> allocs;
+  cudaGraphExec_t graph_chunk = nullptr;
+  cudaGraphExec_t graph_one = nullptr;
+  uint64_t host_step = 0;
+};
+
+namespace {
+
+ckmpm_status fail(ckmpm_scene* s, ckmpm_status code, const std::string& msg) {
+  if (s) s->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+#define CK_CUDA(s, call)                                                                              \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
+    if (e_ != cudaSuccess)                                                                            \
+      return fail((s), CKMPM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));           \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(ckmpm_scene* s, T** p, size_t count) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e == cudaSuccess) s->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return e;
+}
+
+void free_graphs(ckmpm_scene* s) {
+  if (s->graph_chunk) cudaGraphExecDestroy(s->graph_chunk);
+  if (s->graph_one) cudaGraphExecDestroy(s->graph_one);
+  s->graph_chunk = s->graph_one = nullptr;
+}
+
+template <int KIND>
+cudaError_t launch_fused(ckmpm_scene* s, const ModelHost& m) {
+  g2p2g_kernel<KIND, kFusedThreads><<<s->fused_ctas, kFusedThreads, kSmemFused, s->stream>>>(s->sc, m.dev, s->grid,
+                                                                                             s->scal);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fused_any(ckmpm_scene* s, const ModelHost& m) {
+  switch (m.mat.kind) {
+    case CKMPM_FIXED_COROTATED: return launch_fused<kFixedCorotated>(s, m);
+    case CKMPM_DRUCKER_PRAGER: return launch_fused<kDruckerPrager>(s, m);
+    default: return launch_fused<kFluid>(s, m);
+  }
+}
+
+// Compaction of one model's next block list into list `out`.
+cudaError_t launch_compact(ckmpm_scene* s, const ModelHost& m, const BlockListDev& out) {
+  compact_reduce_kernel<<<m.ntiles, kCompactThreads, 0, s->stream>>>(s->sc, m.dev.dense_total, m.dev.tile_sums);
+  compact_scatter_kernel<<<m.ntiles, kCompactThreads, 0, s->stream>>>(s->sc, m.dev.dense_total, m.dev.tile_sums, out,
+                                                                       m.dev.cap_slots, m.dev.ticket, s->scal);
+  return cudaGetLastError();
+}
+
+__global__ void set_next_dt_kernel(Scalars* scal, float dt) {
+  if (threadIdx.x == 0) scal->next_dt = dt;
+}
+
+// Enqueue one substep for every model.  The compaction of each model writes
+// the block list the fused kernel did not read: that of the other parity.
+
+cudaError_t enqueue_substep(ckmpm_scene* s, int parity_of_step) {
+  for (auto& m : s->models) {
+    cudaError_t e = launch_fused_any(s, m);
+    if (e != cudaSuccess) return e;
+    e = launch_compact(s, m, m.dev.bl[parity_of_step ^ 1]);
+    if (e != cudaSuccess) return e;
+  }
+  end_substep_kernel<<<1, 32, 0, s->stream>>>(s->scal);
+  return cudaGetLastError();
+}
+
+cudaError_t build_graph(ckmpm_scene* s, int nsub, int first_parity, cudaGraphExec_t* exec) {
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  for (int i = 0; i < nsub; ++i) {
+    e = enqueue_substep(s, (first_parity + i) & 1);
+    if (e != cudaSuccess) break;
+  }
+  cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
+  if (e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return e;
+  }
+  if (e2 != cudaSuccess) return e2;
+  e = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  return e;
+}
+
+ckmpm_status status_from(ckmpm_scene* s, const Scalars& h) {
+  if (h.status & kStatusTimeout) return fail(s, CKMPM_ERR_TIMEOUT, "a bounded device wait gave up (flush ordering)");
+  if (h.status & kStatusCapacity)
+    return fail(s, CKMPM_ERR_CAPACITY, "block capacity exceeded (particles per block or block table)");
+  if (h.status & kStatusNumeric) return fail(s, CKMPM_ERR_NUMERIC, "non-finite or out-of-range P2G contribution");
+  if (h.status & kStatusConsistency) return fail(s, CKMPM_ERR_INVALID, "rebin consistency check failed");
+  if (h.status & kStatusOutsideBlock)
+    return fail(s, CKMPM_ERR_NUMERIC, "a particle was outside the stencil window of its block");
+  return CKMPM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ckmpm_version(void) { return kVersion; }
+
+const char* ckmpm_last_error(const ckmpm_scene* s) { return s ? s->err.c_str() : g_create_error.c_str(); }
+
+ckmpm_status ckmpm_create(const ckmpm_scene_desc* desc, ckmpm_scene** out) {
+  if (!desc || !out) return fail(nullptr, CKMPM_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (!(desc->dx > 0.f)) return fail(nullptr, CKMPM_ERR_INVALID, "dx must be positive");
+  for (int a = 0; a < 3; ++a)
+    if (desc->domain_blocks[a] < 1 || desc->domain_blocks[a] > 4096)
+      return fail(nullptr, CKMPM_ERR_INVALID, "domain_blocks out of range");
+  const uint64_t nbd = static_cast<uint64_t>(desc->domain_blocks[0]) * desc->domain_blocks[1] * desc->domain_blocks[2];
+  if (nbd > (1ull << 28)) return fail(nullptr, CKMPM_ERR_INVALID, "domain too large for the dense block table");
+  if (desc->boundary != CKMPM_BOUNDARY_STICKY_BLOCKS && desc->boundary != CKMPM_BOUNDARY_SLIP_FLOOR)
+    return fail(nullptr, CKMPM_ERR_INVALID, "unknown boundary kind");
+  if (desc->max_particles_per_block > static_cast<uint32_t>(kMaxParticlesPerBlock))
+    return fail(nullptr, CKMPM_ERR_INVALID, "max_particles_per_block > 4096");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, CKMPM_ERR_CUDA, "no CUDA device is available");
+  if (desc->device < 0 || desc->device >= ndev) return fail(nullptr, CKMPM_ERR_INVALID, "bad device ordinal");
+
+  ckmpm_scene* s = new ckmpm_scene();
+  s->desc = *desc;
+  if (s->desc.max_particles_per_block == 0) s->desc.max_particles_per_block = kMaxParticlesPerBlock;
+  auto bail = [&](ckmpm_status st) {
+    g_create_error = s->err;
+    ckmpm_destroy(s);
+    return st;
+  };
+  if (cudaSetDevice(desc->device) != cudaSuccess) return bail(fail(s, CKMPM_ERR_CUDA, "cudaSetDevice failed"));
+  cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, desc->device);
+  if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(s, CKMPM_ERR_CUDA, "cudaStreamCreate failed"));
+  s->stream = s->own_stream;
+
+  SceneDev& sc = s->sc;
+  sc.dx = desc->dx;
+  sc.inv_dx = static_cast<float>(1.0 / static_cast<double>(desc->dx));
+  for (int a = 0; a < 3; ++a) sc.dims[a] = desc->domain_blocks[a];
+  sc.gravity = desc->gravity;
+  sc.mass_clamp = desc->mass_clamp;
+  sc.boundary = desc->boundary;
+  sc.floor_cells = desc->floor_cells;
+  sc.nblocks_domain = static_cast<uint32_t>(nbd);
+  uint32_t base = 0;
+  for (int c = 0; c < 8; ++c) {
+    const int par[3] = {(c >> 2) & 1, (c >> 1) & 1, c & 1};
+    for (int a = 0; a < 3; ++a) sc.cdims[c][a] = (sc.dims[a] - par[a] + 1) / 2;
+    sc.cbase[c] = base;
+    base += static_cast<uint32_t>(sc.cdims[c][0]) * sc.cdims[c][1] * sc.cdims[c][2];
+  }
+  sc.cbase[8] = base;
+
+  // Dense grids and stamps.
+  for (int b = 0; b < 2; ++b) {
+    if (dalloc(s, &s->grid.grid[b], static_cast<size_t>(nbd) * 512) != cudaSuccess ||
+        dalloc(s, &s->grid.stamp[b], nbd) != cudaSuccess)
+      return bail(fail(s, CKMPM_ERR_CUDA, "grid allocation failed"));
+    cudaMemsetAsync(s->grid.stamp[b], 0xFF, sizeof(int32_t) * nbd, s->stream);
+  }
+  if (dalloc(s, &s->scal, 1) != cudaSuccess) return bail(fail(s, CKMPM_ERR_CUDA, "scalar allocation failed"));
+  cudaMemsetAsync(s->scal, 0, sizeof(Scalars), s->stream);
+
+  auto set_attr = [&](const void* fn) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemFused));
+  };
+  if (set_attr(reinterpret_cast<const void*>(g2p2g_kernel<kFixedCorotated, kFusedThreads>)) != cudaSuccess ||
+      set_attr(reinterpret_cast<const void*>(g2p2g_kernel<kDruckerPrager, kFusedThreads>)) != cudaSuccess ||
+      set_attr(reinterpret_cast<const void*>(g2p2g_kernel<kFluid, kFusedThreads>)) != cudaSuccess ||
+      set_attr(reinterpret_cast<const void*>(rasterize_kernel<kFusedThreads>)) != cudaSuccess)
+    return bail(fail(s, CKMPM_ERR_CUDA, "cudaFuncSetAttribute failed"));
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, g2p2g_kernel<kFixedCorotated, kFusedThreads>, kFusedThreads,
+                                                kSmemFused);
+  int occ2 = 0, occ3 = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, g2p2g_kernel<kDruckerPrager, kFusedThreads>, kFusedThreads,
+                                                kSmemFused);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, g2p2g_kernel<kFluid, kFusedThreads>, kFusedThreads, kSmemFused);
+  occ = std::max(1, std::min(occ, std::min(occ2, occ3)));
+  s->fused_ctas = occ * s->sm_count;
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return bail(fail(s, CKMPM_ERR_CUDA, "init sync failed"));
+  *out = s;
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_add_model(ckmpm_scene* s, const ckmpm_material* material, uint32_t n, const float* x,
+                             const float* v, uint32_t nv, float mass, float volume, int32_t* model_index) {
+  if (!s || !material || !x || !v) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  if (s->setup_done) return fail(s, CKMPM_ERR_INVALID, "models must be added before ckmpm_setup");
+  if (n == 0) return fail(s, CKMPM_ERR_INVALID, "empty model");
+  if (nv != 1 && nv != n) return fail(s, CKMPM_ERR_INVALID, "nv must be 1 or n");
+  if (material->kind != CKMPM_FIXED_COROTATED && material->kind != CKMPM_DRUCKER_PRAGER && material->kind != CKMPM_FLUID)
+    return fail(s, CKMPM_ERR_INVALID, "unsupported material kind");
+  if (!(mass > 0.f) || !(volume > 0.f)) return fail(s, CKMPM_ERR_INVALID, "mass and volume must be positive");
+  if ((material->kind != CKMPM_FLUID) && !(material->p[1] > 0.f))
+    return fail(s, CKMPM_ERR_INVALID, "mu must be positive");
+  ModelHost m;
+  m.mat = *material;
+  m.mass = mass;
+  m.vol = volume;
+  m.n = n;
+  m.nv = nv;
+  m.x.assign(x, x + 3 * static_cast<size_t>(n));
+  m.v.assign(v, v + 3 * static_cast<size_t>(nv));
+  s->models.push_back(std::move(m));
+  if (model_index) *model_index = static_cast<int32_t>(s->models.size()) - 1;
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_setup(ckmpm_scene* s) {
+  if (!s) return fail(s, CKMPM_ERR_INVALID, "null scene");
+  if (s->setup_done) return fail(s, CKMPM_ERR_INVALID, "setup already done");
+  if (s->models.empty()) return fail(s, CKMPM_ERR_INVALID, "no models");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  const uint32_t nbd = s->sc.nblocks_domain;
+  const bool track = (s->desc.flags & CKMPM_FLAG_TRACK_IDS) != 0;
+  uint32_t lost_at_setup = 0;
+  for (auto& m : s->models) {
+    ModelDev& d = m.dev;
+    const uint32_t n = m.n;
+    d.cap_particles = n;
+    d.cap_slots = std::max<uint32_t>(1, std::min<uint32_t>(nbd, n));
+    d.max_per_block = s->desc.max_particles_per_block;
+    d.track_ids = track ? 1 : 0;
+    d.mat.kind = m.mat.kind;
+    for (int k = 0; k < 4; ++k) d.mat.p[k] = m.mat.p[k];
+    d.mass = m.mass;
+    d.vol = m.vol;
+    m.ntiles = (nbd + kCompactTile - 1) / kCompactTile;
+    const bool hasF = m.mat.kind != CKMPM_FLUID;
+    const bool hasAux = m.mat.kind != CKMPM_FIXED_COROTATED;
+    for (int b = 0; b < 2; ++b) {
+      StateDev& st = d.st[b];
+      for (int a = 0; a < 3; ++a) CK_CUDA(s, dalloc(s, &st.x[a], n));
+      for (int k = 0; k < 9; ++k) {
+        st.F[k] = nullptr;
+        if (hasF) CK_CUDA(s, dalloc(s, &st.F[k], n));
+      }
+      st.aux = nullptr;
+      if (hasAux) CK_CUDA(s, dalloc(s, &st.aux, n));
+      st.id = nullptr;
+      if (track) CK_CUDA(s, dalloc(s, &st.id, n));
+      BlockListDev& bl = d.bl[b];
+      CK_CUDA(s, dalloc(s, &bl.keys, d.cap_slots));
+      CK_CUDA(s, dalloc(s, &bl.start, d.cap_slots));
+      CK_CUDA(s, dalloc(s, &bl.count, d.cap_slots));
+      CK_CUDA(s, dalloc(s, &bl.table, nbd));
+      CK_CUDA(s, dalloc(s, &bl.prefix28, static_cast<size_t>(d.cap_slots) * 28));
+      CK_CUDA(s, dalloc(s, &bl.idx, n));
+      CK_CUDA(s, dalloc(s, &bl.nblocks, 1));
+      CK_CUDA(s, dalloc(s, &bl.nparticles, 1));
+      CK_CUDA(s, cudaMemsetAsync(bl.nblocks, 0, sizeof(uint32_t), s->stream));
+      CK_CUDA(s, cudaMemsetAsync(bl.nparticles, 0, sizeof(uint32_t), s->stream));
+    }
+    CK_CUDA(s, dalloc(s, &d.dense_total, nbd));
+    CK_CUDA(s, cudaMemsetAsync(d.dense_total, 0, sizeof(uint32_t) * nbd, s->stream));
+    CK_CUDA(s, dalloc(s, &d.tile_sums, 2 * static_cast<size_t>(m.ntiles)));
+    CK_CUDA(s, dalloc(s, &d.ticket, 1));
+    CK_CUDA(s, cudaMemsetAsync(d.ticket, 0, sizeof(uint32_t), s->stream));
+    CK_CUDA(s, dalloc(s, &d.done, d.cap_slots));
+    CK_CUDA(s, cudaMemsetAsync(d.done, 0xFF, sizeof(int32_t) * d.cap_slots, s->stream));
+    CK_CUDA(s, dalloc(s, &d.vel_in, 3 * static_cast<size_t>(n)));
+
+    // Upload, bin, radix-sort by colour-major block index, compact.
+    float *dx_in = nullptr, *dv_in = nullptr;
+    uint32_t *k_in = nullptr, *k_out = nullptr, *v_in = nullptr, *v_out = nullptr;
+    CK_CUDA(s, cudaMalloc(&dx_in, sizeof(float) * 3 * n));
+    CK_CUDA(s, cudaMalloc(&dv_in, sizeof(float) * 3 * m.nv));
+    CK_CUDA(s, cudaMalloc(&k_in, sizeof(uint32_t) * n));
+    CK_CUDA(s, cudaMalloc(&k_out, sizeof(uint32_t) * n));
+    CK_CUDA(s, cudaMalloc(&v_in, sizeof(uint32_t) * n));
+    CK_CUDA(s, cudaMalloc(&v_out, sizeof(uint32_t) * n));
+    CK_CUDA(s, cudaMemcpyAsync(dx_in, m.x.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->stream));
+    CK_CUDA(s, cudaMemcpyAsync(dv_in, m.v.data(), sizeof(float) * 3 * m.nv, cudaMemcpyHostToDevice, s->stream));
+    setup_bin_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(s->sc, n, dx_in, k_in, v_in, d.dense_total);
+    size_t temp_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, k_in, k_out, v_in, v_out, static_cast<int>(n), 0, 32,
+                                    s->stream);
+    void* temp = nullptr;
+    CK_CUDA(s, cudaMalloc(&temp, std::max<size_t>(temp_bytes, 1)));
+    CK_CUDA(s, cub::DeviceRadixSort::SortPairs(temp, temp_bytes, k_in, k_out, v_in, v_out, static_cast<int>(n), 0, 32,
+                                               s->stream));
+    CK_CUDA(s, launch_compact(s, m, d.bl[0]));
+    uint32_t counts[2] = {0, 0};
+    CK_CUDA(s, cudaMemcpyAsync(&counts[0], d.bl[0].nblocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    CK_CUDA(s, cudaMemcpyAsync(&counts[1], d.bl[0].nparticles, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    CK_CUDA(s, cudaStreamSynchronize(s->stream));
+    m.n_valid = counts[1];
+    lost_at_setup += n - m.n_valid;
+    const float aux0 = m.mat.kind == CKMPM_FLUID ? m.mat.p[3] : 0.f;
+    if (m.n_valid > 0)
+      setup_gather_kernel<<<(m.n_valid + 255) / 256, 256, 0, s->stream>>>(d, m.n_valid, v_out, dx_in, dv_in, m.nv,
+                                                                           aux0);
+    // Identity previous-step structures in list 1.
+    CK_CUDA(s, cudaMemcpyAsync(d.bl[1].table, d.bl[0].table, sizeof(int32_t) * nbd, cudaMemcpyDeviceToDevice,
+                               s->stream));
+    CK_CUDA(s, cudaMemcpyAsync(d.bl[1].start, d.bl[0].start, sizeof(uint32_t) * d.cap_slots, cudaMemcpyDeviceToDevice,
+                               s->stream));
+    CK_CUDA(s, cudaMemcpyAsync(d.bl[1].count, d.bl[0].count, sizeof(uint32_t) * d.cap_slots, cudaMemcpyDeviceToDevice,
+                               s->stream));
+    CK_CUDA(s, cudaMemcpyAsync(d.bl[1].keys, d.bl[0].keys, sizeof(int4) * d.cap_slots, cudaMemcpyDeviceToDevice,
+                               s->stream));
+    CK_CUDA(s, cudaMemcpyAsync(d.bl[1].nblocks, d.bl[0].nblocks, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s->stream));
+    CK_CUDA(s, cudaMemcpyAsync(d.bl[1].nparticles, d.bl[0].nparticles, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                               s->stream));
+    if (counts[0] > 0) setup_identity_kernel<<<counts[0], 256, 0, s->stream>>>(d.bl[0], d.bl[1]);
+    CK_CUDA(s, cudaGetLastError());
+    CK_CUDA(s, cudaStreamSynchronize(s->stream));
+    cudaFree(dx_in);
+    cudaFree(dv_in);
+    cudaFree(k_in);
+    cudaFree(k_out);
+    cudaFree(v_in);
+    cudaFree(v_out);
+    cudaFree(temp);
+  }
+  // Initial grid: every model deposits mass and momentum into grid[0], epoch 0.
+  for (auto& m : s->models) {
+    CK_CUDA(s, cudaMemsetAsync(m.dev.ticket, 0, sizeof(uint32_t), s->stream));
+    rasterize_kernel<kFusedThreads><<<s->fused_ctas, kFusedThreads, kSmemFused, s->stream>>>(s->sc, m.dev, s->grid,
+                                                                                             s->scal);
+    CK_CUDA(s, cudaGetLastError());
+    CK_CUDA(s, cudaMemsetAsync(m.dev.ticket, 0, sizeof(uint32_t), s->stream));
+  }
+  Scalars h{};
+  h.step = 0;
+  h.cur_dt = 0.f;
+  h.next_dt = 0.f;
+  h.lost = lost_at_setup;
+  CK_CUDA(s, cudaMemcpyAsync(s->scal, &h, sizeof(Scalars), cudaMemcpyHostToDevice, s->stream));
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  s->setup_done = true;
+  s->host_step = 0;
+  Scalars r{};
+  CK_CUDA(s, cudaMemcpy(&r, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost));
+  return status_from(s, r);
+}
+
+ckmpm_status ckmpm_set_stream(ckmpm_scene* s, void* cuda_stream) {
+  if (!s) return fail(s, CKMPM_ERR_INVALID, "null scene");
+  s->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : s->own_stream;
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_step_async(ckmpm_scene* s, uint32_t nsteps, float dt) {
+  if (!s || !s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  if (!(dt >= 0.f)) return fail(s, CKMPM_ERR_INVALID, "dt must be non-negative");
+  if (nsteps == 0) return CKMPM_OK;
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  set_next_dt_kernel<<<1, 32, 0, s->stream>>>(s->scal, dt);
+  CK_CUDA(s, cudaGetLastError());
+  // The parity of the substep counter decides which block list each
+  // compaction writes.  The device counter only moves through these launches,
+  // so the host mirror is exact; chunk graphs are captured at even parity.
+  uint32_t done = 0;
+  while (done < nsteps) {
+    const int parity = static_cast<int>(s->host_step & 1);
+    if (parity == 0 && nsteps - done >= static_cast<uint32_t>(kGraphChunk)) {
+      if (!s->graph_chunk) CK_CUDA(s, build_graph(s, kGraphChunk, 0, &s->graph_chunk));
+      CK_CUDA(s, cudaGraphLaunch(s->graph_chunk, s->stream));
+      done += kGraphChunk;
+      s->host_step += kGraphChunk;
+    } else {
+      CK_CUDA(s, enqueue_substep(s, parity));
+      ++done;
+      ++s->host_step;
+    }
+  }
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_status_check(ckmpm_scene* s) {
+  if (!s) return fail(s, CKMPM_ERR_INVALID, "null scene");
+  Scalars h{};
+  CK_CUDA(s, cudaMemcpyAsync(&h, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  return status_from(s, h);
+}
+
+ckmpm_status ckmpm_step(ckmpm_scene* s, uint32_t nsteps, float dt) {
+  ckmpm_status st = ckmpm_step_async(s, nsteps, dt);
+  if (st != CKMPM_OK) return st;
+  return ckmpm_status_check(s);
+}
+
+ckmpm_status ckmpm_step_adaptive(ckmpm_scene* s, uint32_t, float, float, double, double*) {
+  return fail(s, CKMPM_ERR_INVALID, "adaptive stepping is not available in this build");
+}
+
+ckmpm_status ckmpm_get_count(ckmpm_scene* s, int32_t model, uint32_t* n_live) {
+  if (!s || !n_live) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  if (!s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  if (model < 0 || model >= static_cast<int32_t>(s->models.size())) return fail(s, CKMPM_ERR_NOT_FOUND, "no such model");
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  const BlockListDev& cur = s->models[model].dev.bl[s->host_step & 1];
+  CK_CUDA(s, cudaMemcpy(n_live, cur.nparticles, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_get_state(ckmpm_scene* s, int32_t model, float* x, float* v, float* F, float* aux, uint32_t* id,
+                             uint32_t cap, uint32_t* n_out) {
+  if (!s) return fail(s, CKMPM_ERR_INVALID, "null scene");
+  if (!s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  if (model < 0 || model >= static_cast<int32_t>(s->models.size())) return fail(s, CKMPM_ERR_NOT_FOUND, "no such model");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  ModelHost& m = s->models[model];
+  uint32_t n = 0;
+  ckmpm_status st = ckmpm_get_count(s, model, &n);
+  if (st != CKMPM_OK) return st;
+  if (n_out) *n_out = n;
+  if (cap < n) return fail(s, CKMPM_ERR_NOT_FOUND, "output capacity too small");
+  if (n == 0) return CKMPM_OK;
+  const size_t cap_p = m.dev.cap_particles;
+  if (!m.ox) {
+    CK_CUDA(s, dalloc(s, &m.ox, 3 * cap_p));
+    CK_CUDA(s, dalloc(s, &m.ov, 3 * cap_p));
+    CK_CUDA(s, dalloc(s, &m.oF, 9 * cap_p));
+    CK_CUDA(s, dalloc(s, &m.oaux, cap_p));
+    CK_CUDA(s, dalloc(s, &m.oid, cap_p));
+  }
+  const bool sorted = m.dev.track_ids != 0;
+  const bool want_id = sorted || id;
+  probe_kernel<kProbeThreads><<<s->sm_count * 4, kProbeThreads, kSmemVTile, s->stream>>>(
+      s->sc, m.dev, s->grid, s->scal, x ? m.ox : nullptr, v ? m.ov : nullptr,
+      (F && m.mat.kind != CKMPM_FLUID) ? m.oF : nullptr, (aux && m.mat.kind != CKMPM_FIXED_COROTATED) ? m.oaux : nullptr,
+      want_id ? m.oid : nullptr);
+  CK_CUDA(s, cudaGetLastError());
+  // Copy straight into the caller's arrays when no reordering is needed.
+  auto fetch = [&](void* dst_user, std::vector<float>& tmp, const float* src, size_t width) -> cudaError_t {
+    if (!dst_user) return cudaSuccess;
+    void* dst = dst_user;
+    if (sorted) {
+      tmp.resize(width * n);
+      dst = tmp.data();
+    }
+    return cudaMemcpyAsync(dst, src, sizeof(float) * width * n, cudaMemcpyDeviceToHost, s->stream);
+  };
+  CK_CUDA(s, fetch(x, m.hx, m.ox, 3));
+  CK_CUDA(s, fetch(v, m.hv, m.ov, 3));
+  if (F && m.mat.kind != CKMPM_FLUID) CK_CUDA(s, fetch(F, m.hF, m.oF, 9));
+  if (aux && m.mat.kind != CKMPM_FIXED_COROTATED) CK_CUDA(s, fetch(aux, m.ha, m.oaux, 1));
+  if (want_id) {
+    m.hid.resize(n);
+    CK_CUDA(s, cudaMemcpyAsync(m.hid.data(), m.oid, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s->stream));
+  }
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  if (F && m.mat.kind == CKMPM_FLUID)
+    for (uint32_t j = 0; j < n; ++j)
+      for (int k = 0; k < 9; ++k) F[9 * j + k] = (k & 3) ? 0.f : 1.f;
+  if (aux && m.mat.kind == CKMPM_FIXED_COROTATED) std::fill(aux, aux + n, 0.f);
+  if (sorted) {
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return m.hid[a] < m.hid[b]; });
+    for (uint32_t j = 0; j < n; ++j) {
+      const uint32_t i = order[j];
+      if (x) std::memcpy(x + 3 * j, &m.hx[3 * i], sizeof(float) * 3);
+      if (v) std::memcpy(v + 3 * j, &m.hv[3 * i], sizeof(float) * 3);
+      if (F && m.mat.kind != CKMPM_FLUID) std::memcpy(F + 9 * j, &m.hF[9 * i], sizeof(float) * 9);
+      if (aux && m.mat.kind != CKMPM_FIXED_COROTATED) aux[j] = m.ha[i];
+      if (id) id[j] = m.hid[i];
+    }
+  } else if (id) {
+    std::memcpy(id, m.hid.data(), sizeof(uint32_t) * n);
+  }
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_get_blocks(ckmpm_scene* s, int32_t model, int32_t which, int32_t* keys, uint32_t* counts,
+                              uint32_t cap, uint32_t* n_out) {
+  if (!s) return fail(s, CKMPM_ERR_INVALID, "null scene");
+  if (!s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  if (which < 0 || which > 2) return fail(s, CKMPM_ERR_INVALID, "which must be 0, 1 or 2");
+  if (model >= static_cast<int32_t>(s->models.size())) return fail(s, CKMPM_ERR_NOT_FOUND, "no such model");
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  const uint64_t step = s->host_step;
+  std::map<std::tuple<int, int, int>, uint32_t> set;
+  for (int32_t mi = 0; mi < static_cast<int32_t>(s->models.size()); ++mi) {
+    if (model >= 0 && mi != model) continue;
+    const BlockListDev& cur = s->models[mi].dev.bl[step & 1];
+    uint32_t nb = 0;
+    CK_CUDA(s, cudaMemcpy(&nb, cur.nblocks, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    std::vector<int4> hk(nb);
+    std::vector<uint32_t> hc(nb);
+    if (nb) {
+      CK_CUDA(s, cudaMemcpy(hk.data(), cur.keys, sizeof(int4) * nb, cudaMemcpyDeviceToHost));
+      CK_CUDA(s, cudaMemcpy(hc.data(), cur.count, sizeof(uint32_t) * nb, cudaMemcpyDeviceToHost));
+    }
+    for (uint32_t i = 0; i < nb; ++i) set[std::make_tuple(hk[i].x, hk[i].y, hk[i].z)] += hc[i];
+  }
+  if (which >= 1) {
+    const int lo = which == 1 ? 0 : -1;
+    std::map<std::tuple<int, int, int>, uint32_t> ext = set;
+    for (auto& kv : set) {
+      const int bx = std::get<0>(kv.first), by = std::get<1>(kv.first), bz = std::get<2>(kv.first);
+      for (int i = lo; i <= 1; ++i)
+        for (int j = lo; j <= 1; ++j)
+          for (int k = lo; k <= 1; ++k) {
+            const int x = bx + i, y = by + j, z = bz + k;
+            if (x < 0 || y < 0 || z < 0 || x >= s->sc.dims[0] || y >= s->sc.dims[1] || z >= s->sc.dims[2]) continue;
+            ext.emplace(std::make_tuple(x, y, z), 0u);
+          }
+    }
+    set.swap(ext);
+  }
+  const uint32_t n = static_cast<uint32_t>(set.size());
+  if (n_out) *n_out = n;
+  if (cap < n) return fail(s, CKMPM_ERR_NOT_FOUND, "output capacity too small");
+  uint32_t i = 0;
+  for (auto& kv : set) {
+    if (keys) {
+      keys[3 * i] = std::get<0>(kv.first);
+      keys[3 * i + 1] = std::get<1>(kv.first);
+      keys[3 * i + 2] = std::get<2>(kv.first);
+    }
+    if (counts) counts[i] = kv.second;
+    ++i;
+  }
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_get_counters(ckmpm_scene* s, uint64_t* out5) {
+  if (!s || !out5) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  Scalars h{};
+  CK_CUDA(s, cudaMemcpyAsync(&h, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  out5[0] = static_cast<uint64_t>(h.step);
+  out5[1] = h.lost;
+  out5[2] = h.window_skips;
+  out5[3] = h.status;
+  out5[4] = h.timeouts;
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_get_dt(ckmpm_scene* s, float* out2) {
+  if (!s || !out2) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  Scalars h{};
+  CK_CUDA(s, cudaMemcpyAsync(&h, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  out2[0] = h.cur_dt;
+  out2[1] = h.next_dt;
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_step_profiled(ckmpm_scene* s, uint32_t nsteps, float dt, double* ms_out3) {
+  if (!s || !s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  if (!ms_out3) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  const uint64_t step = s->host_step;
+  set_next_dt_kernel<<<1, 32, 0, s->stream>>>(s->scal, dt);
+  std::vector<cudaEvent_t> ev;
+  const size_t nm = s->models.size();
+  ev.resize(nsteps * nm * 3);
+  for (auto& x : ev) CK_CUDA(s, cudaEventCreate(&x));
+  for (uint32_t i = 0; i < nsteps; ++i) {
+    const int parity = static_cast<int>((step + i) & 1);
+    for (size_t mi = 0; mi < nm; ++mi) {
+      auto& m = s->models[mi];
+      cudaEvent_t* E = &ev[(i * nm + mi) * 3];
+      CK_CUDA(s, cudaEventRecord(E[0], s->stream));
+      CK_CUDA(s, launch_fused_any(s, m));
+      CK_CUDA(s, cudaEventRecord(E[1], s->stream));
+      CK_CUDA(s, launch_compact(s, m, m.dev.bl[parity ^ 1]));
+      CK_CUDA(s, cudaEventRecord(E[2], s->stream));
+    }
+    end_substep_kernel<<<1, 32, 0, s->stream>>>(s->scal);
+    ++s->host_step;
+  }
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  double fused = 0, other = 0;
+  for (uint32_t i = 0; i < nsteps * nm; ++i) {
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, ev[i * 3], ev[i * 3 + 1]);
+    cudaEventElapsedTime(&b, ev[i * 3 + 1], ev[i * 3 + 2]);
+    fused += a;
+    other += b;
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  ms_out3[0] = fused;
+  ms_out3[1] = other;
+  ms_out3[2] = static_cast<double>(nsteps * nm);
+  return ckmpm_status_check(s);
+}
+
+ckmpm_status ckmpm_debug_constitutive(const ckmpm_material* material, uint32_t n, const float* C, float dt, float* F,
+                                      float* aux, float* tau, float* U, float* S, float* V) {
+  if (!material || !C || !F || !tau || n == 0) return fail(nullptr, CKMPM_ERR_INVALID, "null argument");
+  MaterialParams mp{};
+  mp.kind = material->kind;
+  for (int k = 0; k < 4; ++k) mp.p[k] = material->p[k];
+  float *dC, *dF, *dA, *dT, *dU, *dS, *dV;
+  auto chk = [](cudaError_t e) { return e == cudaSuccess; };
+  if (!chk(cudaMalloc(&dC, sizeof(float) * 9 * n)) || !chk(cudaMalloc(&dF, sizeof(float) * 9 * n)) ||
+      !chk(cudaMalloc(&dA, sizeof(float) * n)) || !chk(cudaMalloc(&dT, sizeof(float) * 9 * n)) ||
+      !chk(cudaMalloc(&dU, sizeof(float) * 9 * n)) || !chk(cudaMalloc(&dS, sizeof(float) * 3 * n)) ||
+      !chk(cudaMalloc(&dV, sizeof(float) * 9 * n)))
+    return fail(nullptr, CKMPM_ERR_CUDA, "allocation failed");
+  cudaMemcpy(dC, C, sizeof(float) * 9 * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(dF, F, sizeof(float) * 9 * n, cudaMemcpyHostToDevice);
+  if (aux) cudaMemcpy(dA, aux, sizeof(float) * n, cudaMemcpyHostToDevice);
+  else cudaMemset(dA, 0, sizeof(float) * n);
+  debug_constitutive_kernel<<<(n + 127) / 128, 128>>>(mp, n, dC, dt, dF, dA, dT, dU, dS, dV);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) {
+    cudaMemcpy(F, dF, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost);
+    if (aux) cudaMemcpy(aux, dA, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(tau, dT, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost);
+    if (U) cudaMemcpy(U, dU, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost);
+    if (S) cudaMemcpy(S, dS, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost);
+    if (V) cudaMemcpy(V, dV, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(dC);
+  cudaFree(dF);
+  cudaFree(dA);
+  cudaFree(dT);
+  cudaFree(dU);
+  cudaFree(dS);
+  cudaFree(dV);
+  if (e != cudaSuccess) return fail(nullptr, CKMPM_ERR_CUDA, cudaGetErrorString(e));
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_destroy(ckmpm_scene* s) {
+  if (!s) return CKMPM_OK;
+  cudaSetDevice(s->desc.device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  free_graphs(s);
+  for (void* p : s->allocs) cudaFree(p);
+  if (s->own_stream) cudaStreamDestroy(s->own_stream);
+  delete s;
+  return CKMPM_OK;
+}
+
+}  // extern "C"

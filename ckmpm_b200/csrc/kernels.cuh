@@ -1,0 +1,1068 @@
+// Device kernels of the CK-MPM substep.
+//
+// Data layout (per scene):
+//  * grid[2]: dense over every 4^3 block of the domain, 2 KB per block:
+//    [m, mvx, mvy, mvz][grid -dx/4, +dx/4][cell i*16 + j*4 + k], the per-block
+//    SoA of the reference's MPMGridBlock (include/mpm_grid.cuh:18-67) but
+//    addressed directly by block coordinate instead of through a partition
+//    slot.  grid[s&1] is read by substep s, grid[(s+1)&1] written by it.
+//  * stamp[2]: per block, the epoch of the substep that last wrote it; a block
+//    whose stamp is stale reads as empty, so nothing is ever cleared.
+//  * per model, particle state SoA (x[3], F[9], aux, id) double-buffered and
+//    sorted by particle block; the block list (keys, start, count) in
+//    colour-major key order; a dense block table; 28 outgoing-direction prefix
+//    counts per block and a u16 per-particle index list that records, for each
+//    block, which of its particles leave in which of the 27 directions.
+//
+// Every substep is: one fused kernel per model (grid update + G2P + F update,
+// SVD, return map + rebin record + P2G, flushed deterministically), then the
+// colour-major compaction that builds the next block list.  No host sync.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mpm_math.cuh"
+
+namespace ckmpm {
+
+constexpr int kMaxParticlesPerBlock = 4096;  // u16 in-block index, 64 per cell x 64 cells as in the reference
+constexpr int kTileNodes = 1024;             // 2 grids x 8^3 nodes around a particle block
+constexpr int kCompactThreads = 256;
+constexpr int kCompactPerThread = 16;
+constexpr int kCompactTile = kCompactThreads * kCompactPerThread;
+constexpr float kFixScale = 68719476736.0f;        // 2^36: P2G fixed-point scale (per unit particle mass)
+constexpr float kFixInvScale = 1.4551915228366852e-11f;  // 2^-36
+constexpr float kFixMaxValue = 131072.0f;          // |contribution| bound per unit mass (2^17)
+constexpr uint32_t kSpinLimit = 1u << 20;          // polls per flush before a wait gives up (~0.1 s)
+
+enum StatusBits : uint32_t {
+  kStatusCapacity = 1u,
+  kStatusNumeric = 2u,
+  kStatusTimeout = 4u,
+  kStatusConsistency = 8u,
+  kStatusEscape = 16u,
+  kStatusOutsideBlock = 32u,
+};
+
+struct SceneDev {
+  float dx, inv_dx;
+  int32_t dims[3];
+  float gravity, mass_clamp;
+  int32_t boundary;
+  float floor_cells;
+  uint32_t cbase[9];     // colour-major traversal: first index of each colour class
+  int32_t cdims[8][3];   // sub-lattice extent of each colour class
+  uint32_t nblocks_domain;
+};
+
+struct Scalars {
+  int32_t step;        // substeps taken; epoch of the grid that the next substep reads
+  float cur_dt;        // dt the next substep advects with
+  float next_dt;       // dt the next substep deposits stress with
+  uint32_t status;     // StatusBits
+  uint32_t lost;       // particles that left the domain
+  uint32_t window_skips;
+  uint32_t timeouts;
+  uint32_t maxv2_bits; // max |v|^2 on the grid (float bits), adaptive dt
+  double time;         // simulated time, adaptive dt
+  double frame_end;    // adaptive dt: end of the current frame
+  float dt_max, cfl;   // adaptive dt parameters
+  uint32_t pad[2];
+};
+
+struct BlockListDev {
+  int4* keys;           // block coordinate and colour
+  uint32_t* start;      // first particle of the block in the state arrays
+  uint32_t* count;      // particles in the block
+  int32_t* table;       // dense: block -> slot, -1 when inactive
+  uint32_t* prefix28;   // per slot: prefix counts of outgoing directions (written by the fused kernel)
+  uint16_t* idx;        // per particle: in-block position, grouped by outgoing direction
+  uint32_t* nblocks;    // device scalar: active particle blocks
+  uint32_t* nparticles; // device scalar: particles in the list
+};
+
+struct StateDev {
+  float* x[3];
+  float* F[9];
+  float* aux;
+  uint32_t* id;
+};
+
+struct ModelDev {
+  StateDev st[2];
+  BlockListDev bl[2];
+  uint32_t* dense_total;  // per domain block: particles binned into it (zero between uses)
+  uint32_t* tile_sums;    // compaction partials
+  uint32_t* ticket;       // work counter of the fused kernel
+  int32_t* done;          // per slot: epoch of the last completed P2G flush
+  float* vel_in;          // setup: sorted initial velocities
+  uint32_t cap_slots;
+  uint32_t cap_particles;
+  uint32_t max_per_block;
+  int32_t track_ids;
+  MaterialParams mat;
+  float mass, vol;
+};
+
+struct GridDev {
+  float* grid[2];
+  int32_t* stamp[2];
+};
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ bool in_domain(const SceneDev& sc, int x, int y, int z) {
+  return (unsigned)x < (unsigned)sc.dims[0] && (unsigned)y < (unsigned)sc.dims[1] && (unsigned)z < (unsigned)sc.dims[2];
+}
+
+__device__ __forceinline__ int64_t flat_block(const SceneDev& sc, int x, int y, int z) {
+  return (static_cast<int64_t>(x) * sc.dims[1] + y) * sc.dims[2] + z;
+}
+
+__device__ __forceinline__ int colour_of(int x, int y, int z) { return ((x & 1) << 2) | ((y & 1) << 1) | (z & 1); }
+
+__device__ __forceinline__ int trunc_div4(int a) { return a / 4; }  // truncation toward zero, as the reference
+
+__device__ __forceinline__ int32_t ld_acquire(const int32_t* p) {
+  int32_t v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release(int32_t* p, int32_t v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void set_status(Scalars* s, uint32_t bits) { atomicOr(&s->status, bits); }
+
+// Grid update of one node (include/mpm_algorithm.cuh:739-869): v = mv / m,
+// gravity on y, boundary rule; zero when m <= mass clamp.
+__device__ __forceinline__ float4 node_velocity(const SceneDev& sc, const float* blk, int cell, int bx, int by, int bz,
+                                                int cell_y, float dt) {
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float m = blk[cell];
+  if (m > sc.mass_clamp) {
+    const float inv = 1.0f / m;
+    v.x = blk[128 + cell] * inv;
+    v.y = blk[256 + cell] * inv;
+    v.z = blk[384 + cell] * inv;
+    v.y += sc.gravity * dt;
+    if (sc.boundary == 0) {
+      const bool out = (bx < 2 || bx + 2 >= sc.dims[0]) || (by < 2 || by + 2 >= sc.dims[1]) ||
+                       (bz < 2 || bz + 2 >= sc.dims[2]);
+      if (out) v = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+      const bool out = (bx < 2 || bx + 2 >= sc.dims[0]) || (bz < 2 || bz + 2 >= sc.dims[2]) || (by + 2 >= sc.dims[1]);
+      if (out) {
+        v = make_float4(0.f, 0.f, 0.f, 0.f);
+      } else if (static_cast<float>(cell_y) < sc.floor_cells) {
+        v.y = fmaxf(v.y, 0.f);
+      }
+    }
+  }
+  return v;
+}
+
+// Loads the 2 x 8^3 velocity tile around particle block `key` from grid
+// buffer `gin`, applying the grid update on the fly.  Node (g, lx, ly, lz)
+// sits at tile index g*512 + lx*64 + ly*8 + lz.
+template <int NT>
+__device__ __forceinline__ void load_velocity_tile(const SceneDev& sc, const float* __restrict__ gin,
+                                                   const int32_t* __restrict__ stin, int32_t read_epoch, int4 key,
+                                                   float dt, float4* vtile) {
+  for (int i = threadIdx.x; i < kTileNodes; i += NT) {
+    const int gi = i >> 9, lx = (i >> 6) & 7, ly = (i >> 3) & 7, lz = i & 7;
+    const int bx = key.x + (lx >> 2), by = key.y + (ly >> 2), bz = key.z + (lz >> 2);
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (in_domain(sc, bx, by, bz)) {
+      const int64_t fb = flat_block(sc, bx, by, bz);
+      if (stin[fb] == read_epoch) {
+        const int cell = gi * 64 + (lx & 3) * 16 + (ly & 3) * 4 + (lz & 3);
+        v = node_velocity(sc, gin + fb * 512, cell, bx, by, bz, by * 4 + (ly & 3), dt);
+      }
+    }
+    vtile[i] = v;
+  }
+}
+
+// Per-axis stencil of one grid at scaled position xs (= x / dx): base cell,
+// offset o in [0,1) and weight w0 (include/mpm_algorithm.cuh:60-67,
+// include/mpm_kernel.cuh:91-114).  g = -1 or +1.
+struct AxisStencil {
+  int base;
+  float o, w0;
+};
+
+template <int G>
+__device__ __forceinline__ AxisStencil axis_stencil(float xs) {
+  AxisStencil s;
+  s.base = static_cast<int>(xs - 0.25f * G);
+  const float local = xs - static_cast<float>(s.base);
+  s.o = local - 0.25f * G;
+  s.w0 = ck_w0(s.o);
+  return s;
+}
+
+// First and second weighted moments of one grid along one axis (world units):
+// m1 = sum_d w_d (d - o) dx, m2 = sum_d w_d (d - o)^2 dx^2.  With a tensor
+// product kernel whose 1-D weights sum to one, D = sum_nodes w r r^T has
+// D_aa = m2_a and D_ab = m1_a m1_b for each grid.
+__device__ __forceinline__ void axis_moments(const AxisStencil& s, float dx, float& m1, float& m2) {
+  const float w1 = 1.0f - s.w0;
+  m1 = (w1 - s.o) * dx;
+  const float a = s.o, b = 1.0f - s.o;
+  m2 = (s.w0 * a * a + w1 * b * b) * dx * dx;
+}
+
+// D (symmetric, 6 entries: 00, 11, 22, 01, 02, 12) summed over both grids.
+__device__ __forceinline__ void d_matrix(const AxisStencil (&st)[2][3], float dx, float* D6) {
+  float m1[2][3], m2[2][3];
+#pragma unroll
+  for (int g = 0; g < 2; ++g)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) axis_moments(st[g][a], dx, m1[g][a], m2[g][a]);
+  D6[0] = m2[0][0] + m2[1][0];
+  D6[1] = m2[0][1] + m2[1][1];
+  D6[2] = m2[0][2] + m2[1][2];
+  D6[3] = m1[0][0] * m1[0][1] + m1[1][0] * m1[1][1];
+  D6[4] = m1[0][0] * m1[0][2] + m1[1][0] * m1[1][2];
+  D6[5] = m1[0][1] * m1[0][2] + m1[1][1] * m1[1][2];
+}
+
+__device__ __forceinline__ void sym_to_full(const float* s6, float* f) {
+  f[0] = s6[0];
+  f[4] = s6[1];
+  f[8] = s6[2];
+  f[1] = f[3] = s6[3];
+  f[2] = f[6] = s6[4];
+  f[5] = f[7] = s6[5];
+}
+
+// G2P on both grids (include/mpm_algorithm.cuh:1555-1638): returns the
+// halved interpolated velocity and C = B D^-1, where B = sum v_i (w r_i)^T
+// and D = sum w r_i r_i^T with r_i = x_i - x_p, both over the 16 nodes.
+// B is accumulated through the separable sums S = sum w v and
+// T_a = sum over nodes with d_a = 1 of w v:  B[r][a] = dx (T_a[r] - o_a S[r]).
+__device__ __forceinline__ void g2p(const float4* __restrict__ vtile, const float (&xs)[3], int4 key, float dx,
+                                    float* v, float* C, bool& inside) {
+  AxisStencil st[2][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    st[0][a] = axis_stencil<-1>(xs[a]);
+    st[1][a] = axis_stencil<1>(xs[a]);
+  }
+  float B[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) B[k] = 0.f;
+  float vs[3] = {0.f, 0.f, 0.f};
+  const int kb[3] = {key.x * 4, key.y * 4, key.z * 4};
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    int l[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      l[a] = st[g][a].base - kb[a];
+      if (l[a] < 0 || l[a] > 6) {
+        inside = false;
+        l[a] = min(max(l[a], 0), 6);
+      }
+    }
+    const float wx[2] = {st[g][0].w0, 1.f - st[g][0].w0};
+    const float wy[2] = {st[g][1].w0, 1.f - st[g][1].w0};
+    const float wz[2] = {st[g][2].w0, 1.f - st[g][2].w0};
+    float S[3] = {0.f, 0.f, 0.f}, T[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) T[r][0] = T[r][1] = T[r][2] = 0.f;
+    const float4* base = vtile + g * 512 + l[0] * 64 + l[1] * 8 + l[2];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      const int dxn = (n >> 2) & 1, dyn = (n >> 1) & 1, dzn = n & 1;
+      const float w = wx[dxn] * wy[dyn] * wz[dzn];
+      const float4 vi = base[dxn * 64 + dyn * 8 + dzn];
+      const float wv[3] = {w * vi.x, w * vi.y, w * vi.z};
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        S[r] += wv[r];
+        if (dxn) T[r][0] += wv[r];
+        if (dyn) T[r][1] += wv[r];
+        if (dzn) T[r][2] += wv[r];
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      vs[r] += S[r];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) B[r * 3 + a] += dx * (T[r][a] - st[g][a].o * S[r]);
+    }
+  }
+  float D6[6], Di6[6], Di[9];
+  d_matrix(st, dx, D6);
+  inv_sym3(D6[0], D6[1], D6[2], D6[3], D6[4], D6[5], Di6);
+  sym_to_full(Di6, Di);
+  matmul3(B, Di, C);
+#pragma unroll
+  for (int r = 0; r < 3; ++r) v[r] = 0.5f * vs[r];
+}
+
+// Scatter one particle's mass and momentum into the fixed-point tile.
+// Per unit particle mass: node mass w, node momentum w (v + Ah (d - o)) with
+// Ah = A dx / m (A the reference's affine contribution).  Integer atomics make
+// the tile sum independent of the order in which particles arrive.
+__device__ __forceinline__ void p2g_scatter(unsigned long long* __restrict__ ptile, const AxisStencil (&st)[2][3],
+                                            const int (&lbase)[2][3], const float* v, const float* Ah) {
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    float Q[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      Q[r] = v[r] - (Ah[r * 3] * st[g][0].o + Ah[r * 3 + 1] * st[g][1].o + Ah[r * 3 + 2] * st[g][2].o);
+    const float wx[2] = {st[g][0].w0 * kFixScale, (1.f - st[g][0].w0) * kFixScale};
+    const float wy[2] = {st[g][1].w0, 1.f - st[g][1].w0};
+    const float wz[2] = {st[g][2].w0, 1.f - st[g][2].w0};
+    unsigned long long* base = ptile + ((g * 8 + lbase[g][0]) * 64 + lbase[g][1] * 8 + lbase[g][2]) * 4;
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      const int dxn = (n >> 2) & 1, dyn = (n >> 1) & 1, dzn = n & 1;
+      const float w = wx[dxn] * wy[dyn] * wz[dzn];
+      float val[3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        val[r] = Q[r];
+        if (dxn) val[r] += Ah[r * 3];
+        if (dyn) val[r] += Ah[r * 3 + 1];
+        if (dzn) val[r] += Ah[r * 3 + 2];
+      }
+      unsigned long long* node = base + (dxn * 64 + dyn * 8 + dzn) * 4;
+      atomicAdd(node + 0, static_cast<unsigned long long>(__float2ll_rn(w)));
+      atomicAdd(node + 1, static_cast<unsigned long long>(__float2ll_rn(w * val[0])));
+      atomicAdd(node + 2, static_cast<unsigned long long>(__float2ll_rn(w * val[1])));
+      atomicAdd(node + 3, static_cast<unsigned long long>(__float2ll_rn(w * val[2])));
+    }
+  }
+}
+
+// Epilogue shared by the substep and the initial rasterisation: wait until
+// every lower-colour neighbour block has flushed (they were dequeued earlier,
+// so the waits end), then add this block's tile into the 2x2x2 grid blocks it
+// covers with plain loads and stores.  Writers of one grid block are its 8
+// covering particle blocks, one per colour, so flushes land in colour order
+// and the grid sums are deterministic.
+template <int NT>
+__device__ __forceinline__ void flush_tile(const SceneDev& sc, const BlockListDev& cur, int32_t* done, uint32_t item,
+                                           int4 key, const unsigned long long* __restrict__ ptile, float unit,
+                                           float* __restrict__ gout, int32_t* __restrict__ stout, int32_t epoch,
+                                           Scalars* scal, int* s_mode, bool waiter) {
+  if (waiter) {
+    // One spin budget for all waits of this flush; once any wait in the launch
+    // has given up (status bit set), later waits do not spin at all.
+    const int c0 = key.w;
+    bool give_up = (*reinterpret_cast<volatile uint32_t*>(&scal->status) & kStatusTimeout) != 0;
+    uint32_t spins = 0;
+    for (int nb = 0; nb < 27 && !give_up; ++nb) {
+      if (nb == 13) continue;
+      const int x = key.x + nb / 9 - 1, y = key.y + (nb / 3) % 3 - 1, z = key.z + nb % 3 - 1;
+      if (!in_domain(sc, x, y, z) || colour_of(x, y, z) >= c0) continue;
+      const int32_t slot = cur.table[flat_block(sc, x, y, z)];
+      if (slot < 0) continue;
+      while (ld_acquire(done + slot) != epoch) {
+        if (++spins > kSpinLimit) {
+          give_up = true;
+          set_status(scal, kStatusTimeout);
+          atomicAdd(&scal->timeouts, 1u);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    const int e = threadIdx.x;
+    const int x = key.x + (e >> 2), y = key.y + ((e >> 1) & 1), z = key.z + (e & 1);
+    int mode = 2;
+    if (in_domain(sc, x, y, z)) mode = (ld_acquire(stout + flat_block(sc, x, y, z)) == epoch) ? 1 : 0;
+    s_mode[e] = mode;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 8 * 512; i += NT) {
+    const int e = i >> 9;
+    const int mode = s_mode[e];
+    if (mode == 2) continue;
+    const int w = i & 511;
+    const int ch = w >> 7, gi = (w >> 6) & 1, cell = w & 63;
+    const int lx = (e >> 2) * 4 + (cell >> 4), ly = ((e >> 1) & 1) * 4 + ((cell >> 2) & 3), lz = (e & 1) * 4 + (cell & 3);
+    const long long sv = static_cast<long long>(ptile[((gi * 8 + lx) * 64 + ly * 8 + lz) * 4 + ch]);
+    const float val = __ll2float_rn(sv) * unit;
+    float* dst = gout + flat_block(sc, key.x + (e >> 2), key.y + ((e >> 1) & 1), key.z + (e & 1)) * 512 + w;
+    if (mode == 0)
+      *dst = val;
+    else
+      *dst = __ldcg(dst) + val;
+  }
+  __syncthreads();
+  if (threadIdx.x < 8 && s_mode[threadIdx.x] == 0) {
+    const int e = threadIdx.x;
+    stout[flat_block(sc, key.x + (e >> 2), key.y + ((e >> 1) & 1), key.z + (e & 1))] = epoch;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release(done + item, epoch);
+  }
+}
+
+// Incoming particle groups of block `key` (run by warp 0): for each of the
+// 27 directions d (source = key + dir(d)), the source block's group of
+// particles that moved here.  s_off: exclusive prefix over directions (28),
+// s_idx: where the group's in-block indices start in prev.idx, s_src: the
+// source block's first particle in the state arrays.
+__device__ __forceinline__ void incoming_groups(const SceneDev& sc, const BlockListDev& prev, int4 key, uint32_t* s_off,
+                                                uint32_t* s_idx, uint32_t* s_src) {
+  const int lane = threadIdx.x & 31;
+  uint32_t c = 0, ib = 0, ss = 0;
+  if (lane < 27) {
+    const int x = key.x + lane / 9 - 1, y = key.y + (lane / 3) % 3 - 1, z = key.z + lane % 3 - 1;
+    if (in_domain(sc, x, y, z)) {
+      const int32_t s = prev.table[flat_block(sc, x, y, z)];
+      if (s >= 0) {
+        const uint32_t a = prev.prefix28[s * 28 + lane], b = prev.prefix28[s * 28 + lane + 1];
+        c = b - a;
+        ss = prev.start[s];
+        ib = ss + a;
+      }
+    }
+  }
+  uint32_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane < 27) {
+    s_off[lane] = incl - c;
+    s_idx[lane] = ib;
+    s_src[lane] = ss;
+  }
+  if (lane == 26) s_off[27] = incl;
+}
+
+__device__ __forceinline__ int find_group(const uint32_t* s_off, uint32_t q) {
+  int lo = 0, hi = 27;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (s_off[mid] <= q)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+struct SharedSmall {
+  uint32_t item;
+  uint32_t off[28];
+  uint32_t idx[27];
+  uint32_t src[27];
+  uint32_t cnt[28];
+  uint32_t pre[28];
+  uint32_t run[28];
+  int mode[8];
+  uint32_t nflag;
+};
+
+constexpr size_t kSmemVTile = sizeof(float4) * kTileNodes;               // 16 KB
+constexpr size_t kSmemPTile = sizeof(unsigned long long) * kTileNodes * 4;  // 32 KB
+constexpr size_t kSmemCodes = kMaxParticlesPerBlock;                     // 4 KB
+constexpr size_t kSmemFused = kSmemVTile + kSmemPTile + kSmemCodes;
+
+// ------------------------------------------------------------------ fused substep
+//
+// One CTA per particle block at a time (persistent, blocks dequeued in
+// colour-major order).  Replaces the reference's G2P2G
+// (include/mpm_algorithm.cuh:1367-1845) together with the grid update
+// (:739-869), the advection record (mpm_particle.cuh:333-371) and the
+// per-block list build (:629-649, :1868-1918).
+template <int KIND, int NT>
+__global__ void __launch_bounds__(NT, 2)
+    g2p2g_kernel(SceneDev sc, ModelDev md, GridDev gd, Scalars* __restrict__ scal) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float4* vtile = reinterpret_cast<float4*>(smem);
+  unsigned long long* ptile = reinterpret_cast<unsigned long long*>(smem + kSmemVTile);
+  uint8_t* dcode = smem + kSmemVTile + kSmemPTile;
+  __shared__ SharedSmall sh;
+
+  const int32_t step = scal->step;
+  const int parity = step & 1;
+  const int32_t read_epoch = step, write_epoch = step + 1;
+  const float dt = scal->cur_dt, ndt = scal->next_dt;
+  const BlockListDev cur = md.bl[parity];
+  const BlockListDev prev = md.bl[parity ^ 1];
+  const StateDev sin = md.st[parity];
+  const StateDev sout = md.st[parity ^ 1];
+  const float* __restrict__ gin = gd.grid[parity];
+  float* __restrict__ gout = gd.grid[parity ^ 1];
+  const int32_t* __restrict__ stin = gd.stamp[parity];
+  int32_t* __restrict__ stout = gd.stamp[parity ^ 1];
+  const uint32_t nb = *cur.nblocks;
+  const float dx = sc.dx, inv_dx = sc.inv_dx;
+  const float vol_over_mass = md.vol / md.mass;
+  const uint32_t maxp = min(md.max_per_block, static_cast<uint32_t>(kMaxParticlesPerBlock));
+
+  for (;;) {
+    if (threadIdx.x == 0) sh.item = atomicAdd(md.ticket, 1u);
+    __syncthreads();
+    const uint32_t item = sh.item;
+    if (item >= nb) break;
+    const int4 key = cur.keys[item];
+    const uint32_t start = cur.start[item];
+    uint32_t n = cur.count[item];
+
+    if (threadIdx.x < 32) {
+      incoming_groups(sc, prev, key, sh.off, sh.idx, sh.src);
+      if (threadIdx.x < 28) sh.cnt[threadIdx.x] = 0;
+    }
+    load_velocity_tile<NT>(sc, gin, stin, read_epoch, key, dt, vtile);
+    for (int i = threadIdx.x; i < kTileNodes * 4; i += NT) ptile[i] = 0ull;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t flags = 0;
+      if (sh.off[27] != n) flags |= kStatusConsistency;
+      if (n > maxp) flags |= kStatusCapacity;
+      if (flags) set_status(scal, flags);
+    }
+    n = min(min(n, sh.off[27]), maxp);
+
+    for (uint32_t q = threadIdx.x; q < n; q += NT) {
+      const int d = find_group(sh.off, q);
+      const uint32_t ii = sh.idx[d] + (q - sh.off[d]);
+      uint32_t iin = ii < md.cap_particles ? sh.src[d] + prev.idx[ii] : 0xFFFFFFFFu;
+      if (iin >= md.cap_particles) {  // corrupted rebin record: flag, never read out of range
+        set_status(scal, kStatusConsistency);
+        iin = 0;
+      }
+      float x[3] = {sin.x[0][iin], sin.x[1][iin], sin.x[2][iin]};
+      float F[9];
+      float aux = 0.f;
+      if (KIND != kFluid) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) F[k] = sin.F[k][iin];
+      }
+      if (KIND != kFixedCorotated) aux = sin.aux[iin];
+      float xs[3] = {x[0] * inv_dx, x[1] * inv_dx, x[2] * inv_dx};
+      bool inside = true;
+      float v[3], C[9];
+      g2p(vtile, xs, key, dx, v, C, inside);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) x[a] += dt * v[a];
+
+      float tau[9];
+      if (KIND == kFluid) {
+        stress_fluid(md.mat.p[0], md.mat.p[1], md.mat.p[2], C, dt, aux, tau);
+      } else {
+        float dW[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) dW[k] = C[k] * dt + ((k & 3) ? 0.f : 1.f);
+        matmul3(dW, F, F);
+        if (KIND == kFixedCorotated)
+          stress_fixed_corotated(md.mat.p[0], md.mat.p[1], F, tau);
+        else
+          stress_drucker_prager(md.mat.p[0], md.mat.p[1], F, aux, tau);
+      }
+
+      const uint32_t o = start + q;
+      sout.x[0][o] = x[0];
+      sout.x[1][o] = x[1];
+      sout.x[2][o] = x[2];
+      if (KIND != kFluid) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) sout.F[k][o] = F[k];
+      }
+      if (KIND != kFixedCorotated) sout.aux[o] = aux;
+      if (md.track_ids) sout.id[o] = sin.id[iin];
+
+      // Rebin record: direction code of (old block - new block), 27 = lost.
+#pragma unroll
+      for (int a = 0; a < 3; ++a) xs[a] = x[a] * inv_dx;
+      int cn[3], sh3[3];
+      bool win = true, ok = true;
+      const int kk[3] = {key.x, key.y, key.z};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        cn[a] = static_cast<int>(xs[a] + 0.25f);
+        const int nbk = trunc_div4(cn[a] - 2);
+        sh3[a] = kk[a] - nbk;
+        ok &= (sh3[a] >= -1 && sh3[a] <= 1);
+        const int lc = cn[a] - 4 * kk[a];
+        win &= (lc > 0 && lc < 7);
+      }
+      ok &= in_domain(sc, kk[0] - sh3[0], kk[1] - sh3[1], kk[2] - sh3[2]);
+      const int code = ok ? (sh3[0] + 1) * 9 + (sh3[1] + 1) * 3 + (sh3[2] + 1) : 27;
+      dcode[q] = static_cast<uint8_t>(code);
+      atomicAdd(&sh.cnt[code], 1u);
+      if (!inside) set_status(scal, kStatusOutsideBlock);
+      if (!win) {
+        atomicAdd(&scal->window_skips, 1u);
+        continue;
+      }
+
+      // P2G at the new position (include/mpm_algorithm.cuh:1687-1792):
+      // A = C m - ndt V (D/2)^-1 tau, scaled here per unit mass and by dx.
+      AxisStencil st[2][3];
+      int lb[2][3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        st[0][a] = axis_stencil<-1>(xs[a]);
+        st[1][a] = axis_stencil<1>(xs[a]);
+        lb[0][a] = st[0][a].base - 4 * kk[a];
+        lb[1][a] = st[1][a].base - 4 * kk[a];
+      }
+      float D6[6], Di6[6], Di[9], DT[9];
+      d_matrix(st, dx, D6);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) D6[k] *= 0.5f;
+      inv_sym3(D6[0], D6[1], D6[2], D6[3], D6[4], D6[5], Di6);
+      sym_to_full(Di6, Di);
+      matmul3(Di, tau, DT);
+      float Ah[9];
+      bool finite = true;
+      const float sA = ndt * vol_over_mass;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        Ah[k] = (C[k] - sA * DT[k]) * dx;
+        finite &= fabsf(Ah[k]) < kFixMaxValue;
+      }
+#pragma unroll
+      for (int r = 0; r < 3; ++r) finite &= fabsf(v[r]) < kFixMaxValue;
+      if (!finite) {
+        set_status(scal, kStatusNumeric);
+        continue;
+      }
+      p2g_scatter(ptile, st, lb, v, Ah);
+    }
+    __syncthreads();
+
+    // Rebin epilogue (warp 0): group counts -> prefix, stable ranks, index list,
+    // next-step block totals.  Meanwhile warp 1 waits for lower colours.
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      const uint32_t c = lane < 28 ? sh.cnt[lane] : 0u;
+      const uint32_t cv = lane < 27 ? c : 0u;
+      uint32_t incl = cv;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (lane < 27) {
+        sh.pre[lane] = incl - cv;
+        sh.run[lane] = incl - cv;
+        cur.prefix28[item * 28 + lane] = incl - cv;
+        if (c > 0) {
+          const int x = key.x - (lane / 9 - 1), y = key.y - ((lane / 3) % 3 - 1), z = key.z - (lane % 3 - 1);
+          atomicAdd(md.dense_total + flat_block(sc, x, y, z), c);
+        }
+      }
+      if (lane == 26) cur.prefix28[item * 28 + 27] = incl;
+      if (lane == 27 && c > 0) atomicAdd(&scal->lost, c);
+      __syncwarp();
+      for (uint32_t b = 0; b < n; b += 32) {
+        const uint32_t q = b + lane;
+        const int code = q < n ? dcode[q] : 255;
+        const uint32_t mask = __match_any_sync(0xffffffffu, code);
+        const uint32_t lt = (1u << lane) - 1u;
+        uint32_t r = 0;
+        if (code < 27) r = sh.run[code] + __popc(mask & lt);
+        __syncwarp();
+        if (code < 27 && start + r < md.cap_particles) {
+          cur.idx[start + r] = static_cast<uint16_t>(q);
+          if (lane == 31 - __clz(mask)) sh.run[code] += __popc(mask);
+        }
+        __syncwarp();
+      }
+    }
+    flush_tile<NT>(sc, cur, md.done, item, key, ptile, md.mass * kFixInvScale, gout, stout, write_epoch, scal, sh.mode,
+                   threadIdx.x == 32);
+  }
+}
+
+// ------------------------------------------------------------------ initial rasterisation
+// Mass and momentum of the sorted initial particles into grid[0] with epoch 0
+// (include/mpm_algorithm.cuh:872-947, here with the same deterministic tile
+// flush as the substep).
+template <int NT>
+__global__ void __launch_bounds__(NT, 2) rasterize_kernel(SceneDev sc, ModelDev md, GridDev gd, Scalars* scal) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned long long* ptile = reinterpret_cast<unsigned long long*>(smem + kSmemVTile);
+  __shared__ SharedSmall sh;
+  const BlockListDev cur = md.bl[0];
+  const StateDev s0 = md.st[0];
+  const uint32_t nb = *cur.nblocks;
+  const float inv_dx = sc.inv_dx;
+  const float Z[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (;;) {
+    if (threadIdx.x == 0) sh.item = atomicAdd(md.ticket, 1u);
+    __syncthreads();
+    const uint32_t item = sh.item;
+    if (item >= nb) break;
+    const int4 key = cur.keys[item];
+    const uint32_t start = cur.start[item];
+    const uint32_t n = cur.count[item];
+    for (int i = threadIdx.x; i < kTileNodes * 4; i += NT) ptile[i] = 0ull;
+    __syncthreads();
+    const int kk[3] = {key.x, key.y, key.z};
+    for (uint32_t q = threadIdx.x; q < n; q += NT) {
+      const uint32_t i = start + q;
+      const float xs[3] = {s0.x[0][i] * inv_dx, s0.x[1][i] * inv_dx, s0.x[2][i] * inv_dx};
+      const float v[3] = {md.vel_in[3 * i], md.vel_in[3 * i + 1], md.vel_in[3 * i + 2]};
+      AxisStencil st[2][3];
+      int lb[2][3];
+      bool ok = true;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        st[0][a] = axis_stencil<-1>(xs[a]);
+        st[1][a] = axis_stencil<1>(xs[a]);
+        lb[0][a] = st[0][a].base - 4 * kk[a];
+        lb[1][a] = st[1][a].base - 4 * kk[a];
+        ok &= lb[0][a] >= 0 && lb[0][a] <= 6 && lb[1][a] >= 0 && lb[1][a] <= 6;
+      }
+      bool finite = fabsf(v[0]) < kFixMaxValue && fabsf(v[1]) < kFixMaxValue && fabsf(v[2]) < kFixMaxValue;
+      if (!ok) set_status(scal, kStatusOutsideBlock);
+      if (!finite) set_status(scal, kStatusNumeric);
+      if (ok && finite) p2g_scatter(ptile, st, lb, v, Z);
+    }
+    __syncthreads();
+    flush_tile<NT>(sc, cur, md.done, item, key, ptile, md.mass * kFixInvScale, gd.grid[0], gd.stamp[0], 0, scal,
+                   sh.mode, threadIdx.x == 32);
+  }
+}
+
+// ------------------------------------------------------------------ compaction
+// The next block list from the per-block totals: a scan over the domain in
+// colour-major order (colour class, then lexicographic key), so slots come out
+// grouped by colour and sorted by key within a colour.  Replaces
+// MarkActiveParticleBlocks + ExclusiveScan + InverseExclusiveScan +
+// UpdatePartition + UpdateBucket + ComputeBinCount
+// (include/mpm_algorithm.cuh:26-45,573-582,1868-1918, include/mpm_engine.cuh:659-787).
+__device__ __forceinline__ int4 traversal_key(const SceneDev& sc, uint32_t t) {
+  int c = 0;
+#pragma unroll
+  for (int k = 1; k < 8; ++k) c += (t >= sc.cbase[k]) ? 1 : 0;
+  const uint32_t loc = t - sc.cbase[c];
+  const uint32_t nz = sc.cdims[c][2], ny = sc.cdims[c][1];
+  const int k = loc % nz;
+  const int j = (loc / nz) % ny;
+  const int i = loc / (nz * ny);
+  return make_int4(2 * i + ((c >> 2) & 1), 2 * j + ((c >> 1) & 1), 2 * k + (c & 1), c);
+}
+
+__device__ __forceinline__ uint32_t block_reduce_sum(uint32_t v, uint32_t* scratch) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) scratch[w] = v;
+  __syncthreads();
+  uint32_t r = 0;
+  if (threadIdx.x < 32) {
+    r = threadIdx.x < (blockDim.x >> 5) ? scratch[threadIdx.x] : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    if (threadIdx.x == 0) scratch[0] = r;
+  }
+  __syncthreads();
+  r = scratch[0];
+  __syncthreads();
+  return r;
+}
+
+// Exclusive block scan of two values (blockDim = kCompactThreads).
+__device__ __forceinline__ void block_scan2(uint32_t a, uint32_t b, uint32_t& ea, uint32_t& eb, uint32_t* scratch) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t ia = a, ib = b;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t ta = __shfl_up_sync(0xffffffffu, ia, o);
+    const uint32_t tb = __shfl_up_sync(0xffffffffu, ib, o);
+    if (lane >= o) {
+      ia += ta;
+      ib += tb;
+    }
+  }
+  __syncthreads();
+  if (lane == 31) {
+    scratch[w] = ia;
+    scratch[32 + w] = ib;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int nw = blockDim.x >> 5;
+    uint32_t xa = lane < nw ? scratch[lane] : 0u, xb = lane < nw ? scratch[32 + lane] : 0u;
+    uint32_t ya = xa, yb = xb;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t ta = __shfl_up_sync(0xffffffffu, ya, o);
+      const uint32_t tb = __shfl_up_sync(0xffffffffu, yb, o);
+      if (lane >= o) {
+        ya += ta;
+        yb += tb;
+      }
+    }
+    scratch[64 + lane] = ya - xa;
+    scratch[96 + lane] = yb - xb;
+  }
+  __syncthreads();
+  ea = scratch[64 + w] + ia - a;
+  eb = scratch[96 + w] + ib - b;
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kCompactThreads) compact_reduce_kernel(SceneDev sc, const uint32_t* __restrict__ total,
+                                                                          uint32_t* __restrict__ tile_sums) {
+  __shared__ uint32_t scratch[128];
+  const uint32_t t0 = blockIdx.x * kCompactTile + threadIdx.x * kCompactPerThread;
+  uint32_t nblk = 0, npart = 0;
+  for (int k = 0; k < kCompactPerThread; ++k) {
+    const uint32_t t = t0 + k;
+    if (t >= sc.nblocks_domain) break;
+    const int4 key = traversal_key(sc, t);
+    const uint32_t c = total[flat_block(sc, key.x, key.y, key.z)];
+    nblk += c > 0 ? 1u : 0u;
+    npart += c;
+  }
+  nblk = block_reduce_sum(nblk, scratch);
+  npart = block_reduce_sum(npart, scratch);
+  if (threadIdx.x == 0) {
+    tile_sums[2 * blockIdx.x] = nblk;
+    tile_sums[2 * blockIdx.x + 1] = npart;
+  }
+}
+
+__global__ void __launch_bounds__(kCompactThreads)
+    compact_scatter_kernel(SceneDev sc, uint32_t* __restrict__ total, const uint32_t* __restrict__ tile_sums,
+                           BlockListDev out, uint32_t cap_slots, uint32_t* ticket, Scalars* scal) {
+  __shared__ uint32_t scratch[128];
+  uint32_t pb = 0, pp = 0;
+  for (uint32_t t = threadIdx.x; t < blockIdx.x; t += blockDim.x) {
+    pb += tile_sums[2 * t];
+    pp += tile_sums[2 * t + 1];
+  }
+  pb = block_reduce_sum(pb, scratch);
+  pp = block_reduce_sum(pp, scratch);
+  const uint32_t t0 = blockIdx.x * kCompactTile + threadIdx.x * kCompactPerThread;
+  uint32_t c[kCompactPerThread];
+  int64_t fb[kCompactPerThread];
+  int4 keys[kCompactPerThread];
+  uint32_t nblk = 0, npart = 0;
+#pragma unroll
+  for (int k = 0; k < kCompactPerThread; ++k) {
+    const uint32_t t = t0 + k;
+    c[k] = 0;
+    fb[k] = -1;
+    if (t < sc.nblocks_domain) {
+      keys[k] = traversal_key(sc, t);
+      fb[k] = flat_block(sc, keys[k].x, keys[k].y, keys[k].z);
+      c[k] = total[fb[k]];
+      nblk += c[k] > 0 ? 1u : 0u;
+      npart += c[k];
+    }
+  }
+  uint32_t eb, ep;
+  block_scan2(nblk, npart, eb, ep, scratch);
+  uint32_t slot = pb + eb, part = pp + ep;
+  bool overflow = false;
+#pragma unroll
+  for (int k = 0; k < kCompactPerThread; ++k) {
+    if (fb[k] < 0) continue;
+    if (c[k] > 0) {
+      if (slot < cap_slots) {
+        out.keys[slot] = keys[k];
+        out.start[slot] = part;
+        out.count[slot] = c[k];
+        out.table[fb[k]] = static_cast<int32_t>(slot);
+      } else {
+        out.table[fb[k]] = -1;
+        overflow = true;
+      }
+      ++slot;
+      part += c[k];
+      total[fb[k]] = 0;
+    } else {
+      out.table[fb[k]] = -1;
+    }
+  }
+  if (overflow) set_status(scal, kStatusCapacity);
+  if (blockIdx.x == gridDim.x - 1) {
+    const uint32_t tb = block_reduce_sum(nblk, scratch), tp = block_reduce_sum(npart, scratch);
+    if (threadIdx.x == 0) {
+      *out.nblocks = min(pb + tb, cap_slots);
+      *out.nparticles = pp + tp;
+      *ticket = 0;
+    }
+  }
+}
+
+// Advance the substep counter and roll the dt pair (include/mpm_engine.cuh:869-871).
+__global__ void end_substep_kernel(Scalars* scal) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    scal->step += 1;
+    scal->time += static_cast<double>(scal->cur_dt);
+    scal->cur_dt = scal->next_dt;
+  }
+}
+
+// ------------------------------------------------------------------ setup
+// Initial binning key of every particle: its colour-major traversal index
+// (0xFFFFFFFF outside the domain), and the per-block count.  Replaces
+// ActivateBlocksWithParticles + BuildParticleCellBucket
+// (include/mpm_algorithm.cuh:586-626,713-736).
+__global__ void setup_bin_kernel(SceneDev sc, uint32_t n, const float* __restrict__ x, uint32_t* __restrict__ keys,
+                                 uint32_t* __restrict__ vals, uint32_t* __restrict__ total) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
+  const int cx = static_cast<int>(px * sc.inv_dx + 0.25f), cy = static_cast<int>(py * sc.inv_dx + 0.25f),
+            cz = static_cast<int>(pz * sc.inv_dx + 0.25f);
+  const int bx = trunc_div4(cx - 2), by = trunc_div4(cy - 2), bz = trunc_div4(cz - 2);
+  uint32_t key = 0xFFFFFFFFu;
+  const bool finite = isfinite(px) && isfinite(py) && isfinite(pz) && px >= 0.f && py >= 0.f && pz >= 0.f;
+  if (finite && in_domain(sc, bx, by, bz)) {
+    const int c = colour_of(bx, by, bz);
+    const uint32_t nz = sc.cdims[c][2], ny = sc.cdims[c][1];
+    key = sc.cbase[c] + ((bx >> 1) * ny + (by >> 1)) * nz + (bz >> 1);
+    atomicAdd(total + flat_block(sc, bx, by, bz), 1u);
+  }
+  keys[i] = key;
+  vals[i] = i;
+}
+
+// Sorted initial state: x from the input, F = I, aux = logJp0 (0) or J0,
+// id = input index, velocities gathered for the rasterisation
+// (include/mpm_algorithm.cuh:974-1081).
+__global__ void setup_gather_kernel(ModelDev md, uint32_t n, const uint32_t* __restrict__ perm,
+                                    const float* __restrict__ x, const float* __restrict__ v, uint32_t nv, float aux0) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t s = perm[i];
+  StateDev st = md.st[0];
+  st.x[0][i] = x[3 * s];
+  st.x[1][i] = x[3 * s + 1];
+  st.x[2][i] = x[3 * s + 2];
+  if (st.F[0]) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) st.F[k][i] = (k & 3) ? 0.f : 1.f;
+  }
+  if (st.aux) st.aux[i] = aux0;
+  if (st.id) st.id[i] = s;
+  const uint32_t vs = nv == 1 ? 0u : s;
+  md.vel_in[3 * i] = v[3 * vs];
+  md.vel_in[3 * i + 1] = v[3 * vs + 1];
+  md.vel_in[3 * i + 2] = v[3 * vs + 2];
+}
+
+// Identity "previous step" for the first substep: every particle stays in
+// its block (direction 13), index list = in-block position
+// (include/mpm_algorithm.cuh:950-964 InitializeAdvectionBucket).
+__global__ void setup_identity_kernel(BlockListDev cur, BlockListDev prev) {
+  const uint32_t slot = blockIdx.x;
+  if (slot >= *cur.nblocks) return;
+  const uint32_t n = cur.count[slot], start = cur.start[slot];
+  if (threadIdx.x < 28) prev.prefix28[slot * 28 + threadIdx.x] = threadIdx.x <= 13 ? 0u : n;
+  for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) prev.idx[start + q] = static_cast<uint16_t>(q);
+}
+
+// ------------------------------------------------------------------ probe / export
+// Gathers the current state into block order (x, F, aux, id) and interpolates
+// v at each particle from the current grid with the grid update applied, as
+// the next G2P will (include/mpm_algorithm.cuh:1306-1331).
+template <int NT>
+__global__ void __launch_bounds__(NT) probe_kernel(SceneDev sc, ModelDev md, GridDev gd, Scalars* scal, float* ox,
+                                                  float* ov, float* oF, float* oaux, uint32_t* oid) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float4* vtile = reinterpret_cast<float4*>(smem);
+  __shared__ SharedSmall sh;
+  const int32_t step = scal->step;
+  const int parity = step & 1;
+  const BlockListDev cur = md.bl[parity];
+  const BlockListDev prev = md.bl[parity ^ 1];
+  const StateDev sin = md.st[parity];
+  const uint32_t nb = *cur.nblocks;
+  const float dt = scal->cur_dt;
+  for (uint32_t item = blockIdx.x; item < nb; item += gridDim.x) {
+    const int4 key = cur.keys[item];
+    const uint32_t start = cur.start[item];
+    const uint32_t n = cur.count[item];
+    if (threadIdx.x < 32) incoming_groups(sc, prev, key, sh.off, sh.idx, sh.src);
+    load_velocity_tile<NT>(sc, gd.grid[parity], gd.stamp[parity], step, key, dt, vtile);
+    __syncthreads();
+    const uint32_t nn = min(n, sh.off[27]);
+    for (uint32_t q = threadIdx.x; q < nn; q += NT) {
+      const int d = find_group(sh.off, q);
+      const uint32_t ii = sh.idx[d] + (q - sh.off[d]);
+      uint32_t iin = ii < md.cap_particles ? sh.src[d] + prev.idx[ii] : 0xFFFFFFFFu;
+      if (iin >= md.cap_particles) {
+        set_status(scal, kStatusConsistency);
+        iin = 0;
+      }
+      const uint32_t o = start + q;
+      const float x[3] = {sin.x[0][iin], sin.x[1][iin], sin.x[2][iin]};
+      if (ox) {
+        ox[3 * o] = x[0];
+        ox[3 * o + 1] = x[1];
+        ox[3 * o + 2] = x[2];
+      }
+      if (oF && sin.F[0]) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) oF[9 * o + k] = sin.F[k][iin];
+      }
+      if (oaux && sin.aux) oaux[o] = sin.aux[iin];
+      if (oid) oid[o] = sin.id ? sin.id[iin] : o;
+      if (ov) {
+        const float xs[3] = {x[0] * sc.inv_dx, x[1] * sc.inv_dx, x[2] * sc.inv_dx};
+        float v[3], C[9];
+        bool inside = true;
+        g2p(vtile, xs, key, sc.dx, v, C, inside);
+        ov[3 * o] = v[0];
+        ov[3 * o + 1] = v[1];
+        ov[3 * o + 2] = v[2];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ debug hook
+__global__ void debug_constitutive_kernel(MaterialParams mat, uint32_t n, const float* C, float dt, float* F,
+                                          float* aux, float* tau, float* U, float* S, float* V) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float c[9], f[9], t[9];
+  for (int k = 0; k < 9; ++k) c[k] = C[9 * i + k];
+  float a = aux ? aux[i] : 0.f;
+  if (mat.kind == kFluid) {
+    stress_fluid(mat.p[0], mat.p[1], mat.p[2], c, dt, a, t);
+  } else {
+    for (int k = 0; k < 9; ++k) f[k] = F[9 * i + k];
+    float dW[9];
+    for (int k = 0; k < 9; ++k) dW[k] = c[k] * dt + ((k & 3) ? 0.f : 1.f);
+    matmul3(dW, f, f);
+    if (U || S || V) {
+      float u[9], s[3], v[9];
+      svd3(f, u, s, v);
+      for (int k = 0; k < 9; ++k) {
+        if (U) U[9 * i + k] = u[k];
+        if (V) V[9 * i + k] = v[k];
+      }
+      if (S)
+        for (int k = 0; k < 3; ++k) S[3 * i + k] = s[k];
+    }
+    if (mat.kind == kFixedCorotated)
+      stress_fixed_corotated(mat.p[0], mat.p[1], f, t);
+    else
+      stress_drucker_prager(mat.p[0], mat.p[1], f, a, t);
+    for (int k = 0; k < 9; ++k) F[9 * i + k] = f[k];
+  }
+  if (aux) aux[i] = a;
+  for (int k = 0; k < 9; ++k) tau[9 * i + k] = t[k];
+}
+
+}  // namespace ckmpm

@@ -1,0 +1,280 @@
+// Device math for the CK-MPM substep: 3x3 helpers, the FP32 SVD, the compact
+// (CK) kernel weights and the three constitutive models on the hot path.
+//
+// Matrices are row-major float[9] like the reference's Matrix<float,3,3>
+// (AppledoreM/CKMPM include/data_type.cuh:32-425).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ckmpm {
+
+#define CKMPM_DEV __device__ __forceinline__
+
+CKMPM_DEV float det3(const float* a) {
+  return a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+         a[2] * (a[3] * a[7] - a[4] * a[6]);
+}
+
+// Adjugate inverse (include/data_type.cuh:369-386).
+CKMPM_DEV void inv3(const float* a, float* r) {
+  const float id = 1.0f / det3(a);
+  r[0] = id * (a[4] * a[8] - a[5] * a[7]);
+  r[1] = id * (a[2] * a[7] - a[1] * a[8]);
+  r[2] = id * (a[1] * a[5] - a[2] * a[4]);
+  r[3] = id * (a[5] * a[6] - a[3] * a[8]);
+  r[4] = id * (a[0] * a[8] - a[2] * a[6]);
+  r[5] = id * (a[2] * a[3] - a[0] * a[5]);
+  r[6] = id * (a[3] * a[7] - a[4] * a[6]);
+  r[7] = id * (a[1] * a[6] - a[0] * a[7]);
+  r[8] = id * (a[0] * a[4] - a[1] * a[3]);
+}
+
+// Inverse of a symmetric matrix given by its 6 unique entries
+// (d00, d11, d22, d01, d02, d12); writes the 6 unique entries of the inverse.
+CKMPM_DEV void inv_sym3(float d00, float d11, float d22, float d01, float d02, float d12, float* r) {
+  const float c00 = d11 * d22 - d12 * d12;
+  const float c01 = d02 * d12 - d01 * d22;
+  const float c02 = d01 * d12 - d02 * d11;
+  const float det = d00 * c00 + d01 * c01 + d02 * c02;
+  const float id = 1.0f / det;
+  r[0] = id * c00;
+  r[1] = id * (d00 * d22 - d02 * d02);
+  r[2] = id * (d00 * d11 - d01 * d01);
+  r[3] = id * c01;
+  r[4] = id * c02;
+  r[5] = id * (d01 * d02 - d00 * d12);
+}
+
+CKMPM_DEV void matmul3(const float* a, const float* b, float* r) {
+  float t[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) t[i * 3 + j] = a[i * 3] * b[j] + a[i * 3 + 1] * b[3 + j] + a[i * 3 + 2] * b[6 + j];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) r[k] = t[k];
+}
+
+// ------------------------------------------------------------------ SVD
+//
+// A = U diag(S) V^T with U, V proper rotations, |S0| >= |S1| >= |S2|, S0, S1 >= 0
+// and the sign of det(A) on S2 -- the convention of the method of
+// McAdams, Selle, Tamstorf, Teran, Sifakis, "Computing the Singular Value
+// Decomposition of 3x3 matrices with minimal branching and elementary floating
+// point operations", UW-Madison TR1690 (2011), which the reference vendors
+// (include/mpm_math.cuh:1-18).  Implemented here from the published outline:
+//   1. symmetric eigenproblem of A^T A by cyclic Jacobi (fixed sweep count,
+//      exact rotation angles from the 2x2 Schur form);
+//   2. B = A V, columns sorted by decreasing norm (sign flips keep det V = 1);
+//   3. Givens QR of B gives U and the diagonal S.
+
+CKMPM_DEV void jacobi_rotate(float& app, float& aqq, float& apq, float& arp, float& arq, float* V, int p, int q) {
+  // Zero apq.  t = tan(theta) of the smaller rotation solving
+  // t^2 + 2 tau t - 1 = 0 with tau = (aqq - app) / (2 apq).
+  const float d = aqq - app;
+  const float e = 2.0f * apq;
+  const float h = sqrtf(d * d + e * e);
+  const float den = d + copysignf(h, d);
+  float t = (fabsf(e) > 1e-30f && den != 0.0f) ? e / den : 0.0f;
+  const float c = rsqrtf(1.0f + t * t);
+  const float s = t * c;
+  app = app - t * apq;
+  aqq = aqq + t * apq;
+  apq = 0.0f;
+  const float rp = arp, rq = arq;
+  arp = c * rp - s * rq;
+  arq = s * rp + c * rq;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float vp = V[k * 3 + p], vq = V[k * 3 + q];
+    V[k * 3 + p] = c * vp - s * vq;
+    V[k * 3 + q] = s * vp + c * vq;
+  }
+}
+
+CKMPM_DEV void givens_qr_step(float* B, float* U, int p, int q, int col) {
+  const float a = B[p * 3 + col], b = B[q * 3 + col];
+  const float r2 = a * a + b * b;
+  float c = 1.0f, s = 0.0f;
+  if (r2 > 1e-38f) {
+    const float ir = rsqrtf(r2);
+    c = a * ir;
+    s = b * ir;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float bp = B[p * 3 + k], bq = B[q * 3 + k];
+    B[p * 3 + k] = c * bp + s * bq;
+    B[q * 3 + k] = -s * bp + c * bq;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float up = U[k * 3 + p], uq = U[k * 3 + q];
+    U[k * 3 + p] = c * up + s * uq;
+    U[k * 3 + q] = -s * up + c * uq;
+  }
+}
+
+CKMPM_DEV void swap_cols(float* V, float& la, float& lb, int a, int b) {
+  const float t = la;
+  la = lb;
+  lb = t;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float va = V[k * 3 + a];
+    V[k * 3 + a] = V[k * 3 + b];
+    V[k * 3 + b] = -va;
+  }
+}
+
+template <int kSweeps = 5>
+CKMPM_DEV void svd3(const float* A, float* U, float* S, float* V) {
+  // M = A^T A (symmetric; 6 unique entries)
+  float m00 = A[0] * A[0] + A[3] * A[3] + A[6] * A[6];
+  float m11 = A[1] * A[1] + A[4] * A[4] + A[7] * A[7];
+  float m22 = A[2] * A[2] + A[5] * A[5] + A[8] * A[8];
+  float m01 = A[0] * A[1] + A[3] * A[4] + A[6] * A[7];
+  float m02 = A[0] * A[2] + A[3] * A[5] + A[6] * A[8];
+  float m12 = A[1] * A[2] + A[4] * A[5] + A[7] * A[8];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) V[k] = (k & 3) ? 0.0f : 1.0f;
+#pragma unroll
+  for (int sweep = 0; sweep < kSweeps; ++sweep) {
+    jacobi_rotate(m00, m11, m01, m02, m12, V, 0, 1);  // r = 2: (m20, m21)
+    jacobi_rotate(m00, m22, m02, m01, m12, V, 0, 2);  // r = 1: (m10, m12)
+    jacobi_rotate(m11, m22, m12, m01, m02, V, 1, 2);  // r = 0: (m01, m02)
+  }
+  float l0 = m00, l1 = m11, l2 = m22;
+  if (l0 < l1) swap_cols(V, l0, l1, 0, 1);
+  if (l0 < l2) swap_cols(V, l0, l2, 0, 2);
+  if (l1 < l2) swap_cols(V, l1, l2, 1, 2);
+  float B[9];
+  matmul3(A, V, B);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) U[k] = (k & 3) ? 0.0f : 1.0f;
+  givens_qr_step(B, U, 0, 1, 0);
+  givens_qr_step(B, U, 0, 2, 0);
+  givens_qr_step(B, U, 1, 2, 1);
+  S[0] = B[0];
+  S[1] = B[4];
+  S[2] = B[8];
+}
+
+// ------------------------------------------------------------------ CK weights
+// w0 = 1 - o + sin(2 pi o) / (2 pi) for offset o in [0, 1); node weights are
+// w0 and 1 - w0 along each axis (include/mpm_kernel.cuh:91-114, which also
+// evaluates the sine with the __sinf intrinsic).
+CKMPM_DEV float ck_w0(float o) {
+  const float kTwoPi = 6.283185307179586f;
+  const float kInvTwoPi = 0.15915494309189535f;
+  return 1.0f - o + kInvTwoPi * __sinf(kTwoPi * o);
+}
+
+// ------------------------------------------------------------------ materials
+enum MaterialKind : int32_t {
+  kFixedCorotated = 0,
+  kDruckerPrager = 2,
+  kFluid = 3,
+};
+
+struct MaterialParams {
+  int32_t kind;
+  float p[4];  // FC / DP: lambda, mu.  Fluid: bulk, gamma, viscosity, J0.
+};
+
+// Fixed-corotated Kirchhoff stress, tau = U diag(2 mu s (s - 1) + lambda J (J - 1)) U^T
+// (include/mpm_material.cuh:320-357).
+CKMPM_DEV void stress_fixed_corotated(float lambda, float mu, const float* F, float* tau) {
+  float U[9], S[3], V[9];
+  svd3(F, U, S, V);
+  const float J = S[0] * S[1] * S[2];
+  const float lj = lambda * J * (J - 1.0f);
+  float sc[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) sc[i] = 2.0f * mu * S[i] * (S[i] - 1.0f) + lj;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = r; c < 3; ++c) {
+      const float v = U[r * 3] * sc[0] * U[c * 3] + U[r * 3 + 1] * sc[1] * U[c * 3 + 1] + U[r * 3 + 2] * sc[2] * U[c * 3 + 2];
+      tau[r * 3 + c] = v;
+      tau[c * 3 + r] = v;
+    }
+}
+
+// Drucker-Prager StVK-Hencky return map with the reference's constants:
+// zero cohesion, beta = 1, volume correction on, sin(phi) = 0.5
+// (include/mpm_material.cuh:362-464).  Updates F and logJp in place.
+CKMPM_DEV void stress_drucker_prager(float lambda, float mu, float* F, float& logJp, float* tau) {
+  const float kYs = 0.816496580927726f * 2.0f * 0.5f / (3.0f - 0.5f);
+  const float smu = 2.0f * mu;
+  float U[9], S[3], V[9];
+  svd3(F, U, S, V);
+  float eps[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) eps[i] = logf(fmaxf(fabsf(S[i]), 1e-4f));
+  const float esum = eps[0] + eps[1] + eps[2];
+  const float etr = esum + logJp;
+  float eh[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) eh[i] = eps[i] - etr / 3.0f;
+  const float ehn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2]);
+  float ns[3];
+  if (etr >= 0.0f) {
+    ns[0] = ns[1] = ns[2] = 1.0f;
+    logJp = esum + logJp;
+  } else {
+    logJp = 0.0f;
+    const float dg = ehn + (3.0f * lambda + smu) / smu * etr * kYs;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const float H = dg <= 0.0f ? eps[i] : eps[i] - (dg / ehn) * eh[i];
+      ns[i] = expf(H);
+    }
+  }
+  // F <- U diag(ns) V^T
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      F[r * 3 + c] = U[r * 3] * ns[0] * V[c * 3] + U[r * 3 + 1] * ns[1] * V[c * 3 + 1] + U[r * 3 + 2] * ns[2] * V[c * 3 + 2];
+  // tau = U diag((2 mu log s + lambda tr log s) / s) V^T F^T
+  float ls[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) ls[i] = logf(ns[i]);
+  const float tr = ls[0] + ls[1] + ls[2];
+  float ph[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) ph[i] = (smu * ls[i] + lambda * tr) / ns[i];
+  float P[9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      P[r * 3 + c] = U[r * 3] * ph[0] * V[c * 3] + U[r * 3 + 1] * ph[1] * V[c * 3 + 1] + U[r * 3 + 2] * ph[2] * V[c * 3 + 2];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      tau[r * 3 + c] = P[r * 3] * F[c * 3] + P[r * 3 + 1] * F[c * 3 + 1] + P[r * 3 + 2] * F[c * 3 + 2];
+}
+
+// J-fluid: J += tr(C) dt J; p = bulk (J^-gamma - 1); tau = J (visc (C + C^T) - p I)
+// (include/mpm_algorithm.cuh:528-569, include/mpm_material.cuh:468-477).
+CKMPM_DEV void stress_fluid(float bulk, float gamma, float visc, const float* C, float dt, float& J, float* tau) {
+  J += (C[0] + C[4] + C[8]) * dt * J;
+  const float p = bulk * (powf(J, -gamma) - 1.0f);
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) tau[r * 3 + c] = (C[r * 3 + c] + C[c * 3 + r]) * visc;
+  tau[0] -= p;
+  tau[4] -= p;
+  tau[8] -= p;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) tau[k] *= J;
+}
+
+}  // namespace ckmpm

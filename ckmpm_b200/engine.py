@@ -1,0 +1,374 @@
+"""Python host interface mirroring the reference's engine/material/model/config API.
+
+Names and call order follow AppledoreM/CKMPM:
+  * MPMConfig        <- MPMConfigBase<Derived> getters (include/mpm_config.h:12-124)
+                        plus the domain extent of MPMDomainRange (include/mpm_domain.h:17-30)
+  * MPMMaterial      <- MPMMaterial<k> and its MaterialParameter_ (include/mpm_material.cuh:20-175)
+  * MPMModel         <- MPMModel(mass, volume, x, v, material, freezeTime) (include/mpm_model.h:11-59)
+  * MPMEngine        <- MPMEngine<GridConfig>: Initialize, InitializeParticle,
+                        InitialSetup, Simulate (include/mpm_engine.cuh:29-974)
+
+Differences, all at the boundary: scene constants are run-time values instead
+of compile-time CRTP getters; the engine is an ordinary object (several per
+process) instead of a per-GridConfig singleton; failures raise CkmpmError
+instead of calling exit()/abort(); Simulate returns instead of ending the
+process.  All arithmetic runs in the CUDA library (ckmpm_b200/_lib).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Sequence
+
+import numpy as np
+
+from . import _capi as capi
+
+ConstitutiveModel = {"fixed_corotated": capi.FIXED_COROTATED, "drucker_prager": capi.DRUCKER_PRAGER,
+                     "fluid": capi.FLUID}
+
+
+def compute_lame_parameters(E: float, nu: float) -> tuple[float, float]:
+    """(lambda, mu) from Young's modulus and Poisson ratio (include/mpm_material.cuh:277-283)."""
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    return lam, mu
+
+
+def evaluate_sound_speed(E: float, nu: float, rho: float) -> float:
+    """include/mpm_test_base.h:15-19."""
+    return math.sqrt(E * (1 - nu) / ((1 + nu) * (1 - 2 * nu) * rho))
+
+
+def evaluate_timestep(dx: float, E: float, nu: float, rho: float, cfl: float = 0.5) -> float:
+    """cfl * dx / sound speed (include/mpm_test_base.h:21-24)."""
+    return cfl * dx / evaluate_sound_speed(E, nu, rho)
+
+
+@dataclass
+class MPMMaterial:
+    """One constitutive model and its parameters.
+
+    kind: 'fixed_corotated' | 'drucker_prager' (params lambda_, mu_) or
+    'fluid' (bulk_, gamma_, viscosity_, J0_), as MaterialParameter_ in
+    include/mpm_material.cuh:63-175.
+    """
+    kind: str
+    lambda_: float = 0.0
+    mu_: float = 0.0
+    bulk_: float = 0.0
+    gamma_: float = 0.0
+    viscosity_: float = 0.0
+    J0_: float = 1.0
+
+    @staticmethod
+    def fixed_corotated(lambda_: float, mu_: float) -> "MPMMaterial":
+        return MPMMaterial("fixed_corotated", lambda_=lambda_, mu_=mu_)
+
+    @staticmethod
+    def drucker_prager(lambda_: float, mu_: float) -> "MPMMaterial":
+        return MPMMaterial("drucker_prager", lambda_=lambda_, mu_=mu_)
+
+    @staticmethod
+    def fluid(bulk: float, gamma: float, viscosity: float, J0: float = 1.0) -> "MPMMaterial":
+        return MPMMaterial("fluid", bulk_=bulk, gamma_=gamma, viscosity_=viscosity, J0_=J0)
+
+    @property
+    def kind_code(self) -> int:
+        return ConstitutiveModel[self.kind]
+
+    def params(self) -> list[float]:
+        if self.kind == "fluid":
+            return [self.bulk_, self.gamma_, self.viscosity_, self.J0_]
+        return [self.lambda_, self.mu_, 0.0, 0.0]
+
+    def to_c(self) -> capi.Material:
+        m = capi.Material()
+        m.kind = self.kind_code
+        for i, v in enumerate(self.params()):
+            m.p[i] = float(v)
+        return m
+
+
+@dataclass
+class MPMModel:
+    """Particles of one material: MPMModel(mass, volume, x, v, material, freezeTime)."""
+    particle_mass: float
+    particle_volume: float
+    particle_position: np.ndarray
+    particle_velocity: np.ndarray
+    material: MPMMaterial
+    freeze_time: float = 0.0
+
+    def __post_init__(self):
+        self.particle_position = np.ascontiguousarray(self.particle_position, dtype=np.float32).reshape(-1, 3)
+        self.particle_velocity = np.ascontiguousarray(self.particle_velocity, dtype=np.float32).reshape(-1, 3)
+        n, nv = len(self.particle_position), len(self.particle_velocity)
+        if nv not in (1, n):
+            raise ValueError("particle_velocity must hold 1 or n velocities (include/mpm_model.h:31-32)")
+
+    def GetParticleMass(self) -> float:
+        return self.particle_mass
+
+    def GetParticleVolume(self) -> float:
+        return self.particle_volume
+
+    def GetParticleCount(self) -> int:
+        return len(self.particle_position)
+
+    def GetParticleMaterial(self) -> MPMMaterial:
+        return self.material
+
+    def IsFreezed(self, elapsed_seconds: float) -> bool:
+        return elapsed_seconds < self.freeze_time
+
+
+@dataclass
+class MPMConfig:
+    """Scene constants: the MPMConfigBase getters plus the domain extent in blocks."""
+    dx: float
+    domain_blocks: tuple[int, int, int]
+    gravity: float = -9.8
+    mass_clamp: float = 0.0
+    dt: float = 1e-4
+    cfl: float = 0.5
+    fps: int = 48
+    total_frames: int = 1
+    boundary: str = "sticky_blocks"
+    floor_cells: float = 8.0
+    max_particles_per_block: int = 4096
+    track_ids: bool = True
+    device: int = 0
+    block_size: int = 4
+    particles_per_cell_cap: int = 64
+
+    # MPMConfigBase getter names (include/mpm_config.h:17-123)
+    def GetDx(self) -> float:
+        return self.dx
+
+    def GetInvDx(self) -> float:
+        return 1.0 / self.dx
+
+    def GetBlockSize(self) -> int:
+        return self.block_size
+
+    def GetBlockVolume(self) -> int:
+        return self.block_size ** 3
+
+    def GetMaxParticleCountPerCell(self) -> int:
+        return self.particles_per_cell_cap
+
+    def GetMaxParticleCountPerBlock(self) -> int:
+        return self.max_particles_per_block
+
+    def GetFps(self) -> int:
+        return self.fps
+
+    def GetDt(self) -> float:
+        return self.dt
+
+    def GetCfl(self) -> float:
+        return self.cfl
+
+    def GetTotalSimulatedFrameCount(self) -> int:
+        return self.total_frames
+
+    def GetGravity(self) -> float:
+        return self.gravity
+
+    def GetMassClamp(self) -> float:
+        return self.mass_clamp
+
+    def to_c(self) -> capi.SceneDesc:
+        d = capi.SceneDesc()
+        d.dx = self.dx
+        for i in range(3):
+            d.domain_blocks[i] = int(self.domain_blocks[i])
+        d.gravity = self.gravity
+        d.mass_clamp = self.mass_clamp
+        d.boundary = {"sticky_blocks": capi.BOUNDARY_STICKY_BLOCKS, "slip_floor": capi.BOUNDARY_SLIP_FLOOR}[self.boundary]
+        d.floor_cells = self.floor_cells
+        d.max_particles_per_block = self.max_particles_per_block
+        d.device = self.device
+        d.flags = capi.FLAG_TRACK_IDS if self.track_ids else 0
+        return d
+
+
+@dataclass
+class ParticleState:
+    x: np.ndarray
+    v: np.ndarray
+    F: np.ndarray
+    aux: np.ndarray
+    id: np.ndarray
+
+
+class Scene:
+    """Owner of one ckmpm_scene handle (one simulation on one GPU)."""
+
+    def __init__(self, config: MPMConfig):
+        self.config = config
+        self._h = C.c_void_p()
+        L = capi.lib()
+        desc = config.to_c()
+        capi.check(L.ckmpm_create(C.byref(desc), C.byref(self._h)), "ckmpm_create", None)
+        self.models: list[MPMModel] = []
+
+    def add_model(self, model: MPMModel) -> int:
+        L = capi.lib()
+        mat = model.material.to_c()
+        idx = C.c_int32()
+        x, v = model.particle_position, model.particle_velocity
+        capi.check(L.ckmpm_add_model(self._h, C.byref(mat), len(x), capi.fptr(x), capi.fptr(v), len(v),
+                                     model.particle_mass, model.particle_volume, C.byref(idx)),
+                   "ckmpm_add_model", self._h)
+        self.models.append(model)
+        return idx.value
+
+    def setup(self) -> None:
+        capi.check(capi.lib().ckmpm_setup(self._h), "ckmpm_setup", self._h)
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        capi.check(capi.lib().ckmpm_set_stream(self._h, C.c_void_p(stream_handle or 0)), "ckmpm_set_stream", self._h)
+
+    def step(self, nsteps: int, dt: float) -> None:
+        capi.check(capi.lib().ckmpm_step(self._h, nsteps, dt), "ckmpm_step", self._h)
+
+    def step_async(self, nsteps: int, dt: float) -> None:
+        capi.check(capi.lib().ckmpm_step_async(self._h, nsteps, dt), "ckmpm_step_async", self._h)
+
+    def status_check(self) -> None:
+        capi.check(capi.lib().ckmpm_status_check(self._h), "ckmpm_status_check", self._h)
+
+    def step_profiled(self, nsteps: int, dt: float) -> tuple[float, float, int]:
+        out = (C.c_double * 3)()
+        capi.check(capi.lib().ckmpm_step_profiled(self._h, nsteps, dt, out), "ckmpm_step_profiled", self._h)
+        return out[0], out[1], int(out[2])
+
+    def count(self, model: int = 0) -> int:
+        n = C.c_uint32()
+        capi.check(capi.lib().ckmpm_get_count(self._h, model, C.byref(n)), "ckmpm_get_count", self._h)
+        return n.value
+
+    def state(self, model: int = 0) -> ParticleState:
+        n = self.count(model)
+        x = np.zeros((n, 3), np.float32)
+        v = np.zeros((n, 3), np.float32)
+        F = np.zeros((n, 3, 3), np.float32)
+        aux = np.zeros(n, np.float32)
+        ids = np.zeros(n, np.uint32)
+        nout = C.c_uint32()
+        capi.check(capi.lib().ckmpm_get_state(self._h, model, capi.fptr(x), capi.fptr(v), capi.fptr(F),
+                                              capi.fptr(aux), capi.uptr(ids), n, C.byref(nout)),
+                   "ckmpm_get_state", self._h)
+        return ParticleState(x, v, F, aux, ids)
+
+    def blocks(self, model: int = -1, which: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        n = C.c_uint32()
+        L = capi.lib()
+        code = L.ckmpm_get_blocks(self._h, model, which, None, None, 0, C.byref(n))
+        if code not in (capi.CKMPM_OK, 6):
+            capi.check(code, "ckmpm_get_blocks", self._h)
+        keys = np.zeros((n.value, 3), np.int32)
+        counts = np.zeros(n.value, np.uint32)
+        capi.check(L.ckmpm_get_blocks(self._h, model, which, capi.iptr(keys), capi.uptr(counts), n.value,
+                                      C.byref(n)), "ckmpm_get_blocks", self._h)
+        return keys, counts
+
+    def counters(self) -> dict:
+        out = (C.c_uint64 * 5)()
+        capi.check(capi.lib().ckmpm_get_counters(self._h, out), "ckmpm_get_counters", self._h)
+        return {"steps": int(out[0]), "lost": int(out[1]), "window_skips": int(out[2]), "status": int(out[3]),
+                "timeouts": int(out[4])}
+
+    def dt_pair(self) -> tuple[float, float]:
+        out = (C.c_float * 2)()
+        capi.check(capi.lib().ckmpm_get_dt(self._h, out), "ckmpm_get_dt", self._h)
+        return out[0], out[1]
+
+    def close(self) -> None:
+        if self._h:
+            capi.lib().ckmpm_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MPMEngine:
+    """Reference-shaped driver: Initialize -> InitializeParticle -> InitialSetup -> Simulate.
+
+    Mirrors MPMEngine<GridConfig> (include/mpm_engine.cuh:29-974): dt is
+    min(config dt, 1/fps) (:178) and shrunk by the initial CFL bound (:109-117);
+    Simulate runs frames of substeps.  With a fixed step size every substep
+    uses that dt; the first substep after InitialSetup advects with dt = 0, as
+    in the reference (:479-480).
+    """
+
+    def __init__(self):
+        self.scene: Scene | None = None
+        self.dt_ = 0.0
+        self.config: MPMConfig | None = None
+
+    def Initialize(self, config: MPMConfig) -> None:
+        self.config = config
+        self.scene = Scene(config)
+        self.dt_ = min(config.GetDt(), 1.0 / config.GetFps())
+
+    def InitializeParticle(self, config: MPMConfig, models: Sequence[MPMModel]) -> None:
+        assert self.scene is not None, "Initialize first"
+        for m in models:
+            vmax = float(np.max(np.linalg.norm(m.particle_velocity, axis=1))) if len(m.particle_velocity) else 0.0
+            if vmax > 0.0:
+                self.dt_ = min(self.dt_, config.GetDx() * config.GetCfl() / vmax)
+            self.scene.add_model(m)
+
+    def InitialSetup(self, config: MPMConfig) -> None:
+        assert self.scene is not None
+        self.scene.setup()
+
+    def Simulate(self, config: MPMConfig, export_callback=None, substeps_per_frame: int | None = None) -> int:
+        """Run GetTotalSimulatedFrameCount() frames at the fixed dt; returns substeps taken.
+
+        export_callback(frame_index, scene) is called after every frame (the
+        reference's ExportParticleToModel point, include/mpm_engine.cuh:880-883).
+        """
+        assert self.scene is not None
+        spf = substeps_per_frame or max(1, int(round((1.0 / config.GetFps()) / self.dt_)))
+        total = 0
+        for frame in range(config.GetTotalSimulatedFrameCount()):
+            self.scene.step(spf, self.dt_)
+            total += spf
+            if export_callback is not None:
+                export_callback(frame, self.scene)
+        return total
+
+
+def load_scene_json(path: str | Path) -> tuple[MPMConfig, list[MPMModel]]:
+    """JSON scene files (a project addition; the reference's importer at
+    include/mpm_io.h:168-199 is commented out).  Schema:
+      {"config": {MPMConfig fields}, "models": [{"material": {...}, "mass": m,
+       "volume": v, "positions": "file.npy" | [[x,y,z],...], "velocity": [[vx,vy,vz]]}]}
+    """
+    path = Path(path)
+    spec = json.loads(path.read_text())
+    cfgd = dict(spec["config"])
+    if "domain_blocks" in cfgd:
+        cfgd["domain_blocks"] = tuple(cfgd["domain_blocks"])
+    cfg = MPMConfig(**cfgd)
+    models = []
+    for md in spec["models"]:
+        mat = MPMMaterial(**md["material"])
+        pos = md["positions"]
+        if isinstance(pos, str):
+            pos = np.load(path.parent / pos)
+        models.append(MPMModel(md["mass"], md["volume"], np.asarray(pos, np.float32),
+                               np.asarray(md.get("velocity", [[0, 0, 0]]), np.float32), mat,
+                               md.get("freeze_time", 0.0)))
+    return cfg, models

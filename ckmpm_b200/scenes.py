@@ -1,0 +1,143 @@
+"""Seeded synthetic scenes with the shapes, sizes and materials of the benchmark configurations.
+
+Particles are seeded on a sub-cell lattice of spacing dx / ppc^(1/3) with a
+uniform jitter of one lattice spacing per particle (numpy PCG64, seed 0 unless
+given), kept when inside the shape.  Particle volume is dx^3 / ppc and mass
+rho * volume, as the reference's scenes do
+(tests/fluid_dam_break/test_fluid_dam_break.cuh:39-42).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .engine import MPMConfig, MPMMaterial, MPMModel, compute_lame_parameters
+
+
+def lattice(lo, hi, spacing: float, rng: np.random.Generator) -> np.ndarray:
+    """Jittered lattice points inside the box [lo, hi)."""
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    n = np.maximum(np.ceil((hi - lo) / spacing).astype(int), 0)
+    if n.min() <= 0:
+        return np.zeros((0, 3), np.float32)
+    idx = np.stack(np.meshgrid(*[np.arange(k) for k in n], indexing="ij"), -1).reshape(-1, 3).astype(np.float64)
+    pts = lo + (idx + rng.random(idx.shape)) * spacing
+    keep = np.all(pts < hi, axis=1)
+    return pts[keep]
+
+
+def box_particles(lo, hi, dx: float, ppc: int, rng) -> np.ndarray:
+    return lattice(lo, hi, dx / round(ppc ** (1 / 3)), rng).astype(np.float32)
+
+
+def sphere_particles(center, r: float, dx: float, ppc: int, rng) -> np.ndarray:
+    c = np.asarray(center, np.float64)
+    pts = lattice(c - r, c + r, dx / round(ppc ** (1 / 3)), rng)
+    keep = np.sum((pts - c) ** 2, axis=1) < r * r
+    return pts[keep].astype(np.float32)
+
+
+def cylinder_y_particles(center_xz, y0: float, r: float, h: float, dx: float, ppc: int, rng) -> np.ndarray:
+    cx, cz = center_xz
+    pts = lattice((cx - r, y0, cz - r), (cx + r, y0 + h, cz + r), dx / round(ppc ** (1 / 3)), rng)
+    keep = (pts[:, 0] - cx) ** 2 + (pts[:, 2] - cz) ** 2 < r * r
+    return pts[keep].astype(np.float32)
+
+
+def jelly_cube(seed: int = 0, dx: float = 1 / 64, lo=(0.4, 0.4, 0.4), hi=(0.6, 0.6, 0.6), ppc: int = 8,
+               E: float = 5e4, nu: float = 0.3, rho: float = 1000.0, v0=(0.0, -1.0, 0.0), gravity: float = -9.8,
+               dt: float = 1e-4, track_ids: bool = True) -> tuple[MPMConfig, list[MPMModel]]:
+    """Jelly cube, fixed-corotated: dx=1/64, cube [0.4,0.6]^3 at 8 ppc (~16.8k particles),
+    E=5e4, nu=0.3, rho=1000, v0=(0,-1,0), g=-9.8, dt=1e-4, sticky walls."""
+    rng = np.random.default_rng(seed)
+    x = box_particles(lo, hi, dx, ppc, rng)
+    n_cells = round(1.0 / dx)
+    cfg = MPMConfig(dx=dx, domain_blocks=(n_cells // 4,) * 3, gravity=gravity, dt=dt, track_ids=track_ids)
+    lam, mu = compute_lame_parameters(E, nu)
+    vol = dx ** 3 / ppc
+    return cfg, [MPMModel(rho * vol, vol, x, np.asarray([v0], np.float32), MPMMaterial.fixed_corotated(lam, mu))]
+
+
+def sand_column(seed: int = 0, dx: float = 1 / 256, r: float = 0.1, h: float = 0.4, ppc: int = 8,
+                E: float = 3.5e5, nu: float = 0.3, rho: float = 1600.0, gravity: float = -9.8,
+                dt: float = 5e-5, track_ids: bool = True) -> tuple[MPMConfig, list[MPMModel]]:
+    """Sand column collapse, Drucker-Prager (friction angle 30 deg): dx=1/256, cylinder r=0.1,
+    h=0.4 standing on y0 = 8 dx at (0.5, 0.5), 8 ppc (~1.69M particles), E=3.5e5, nu=0.3,
+    rho=1600, dt=5e-5, slip floor at 8 cells."""
+    rng = np.random.default_rng(seed)
+    y0 = 8 * dx
+    x = cylinder_y_particles((0.5, 0.5), y0, r, h, dx, ppc, rng)
+    n_cells = round(1.0 / dx)
+    cfg = MPMConfig(dx=dx, domain_blocks=(n_cells // 4,) * 3, gravity=gravity, dt=dt, boundary="slip_floor",
+                    floor_cells=8.0, track_ids=track_ids)
+    lam, mu = compute_lame_parameters(E, nu)
+    vol = dx ** 3 / ppc
+    return cfg, [MPMModel(rho * vol, vol, x, np.zeros((1, 3), np.float32), MPMMaterial.drucker_prager(lam, mu))]
+
+
+def dam_break_mixed(seed: int = 0, dx: float = 1 / 512, ppc: int = 8, n_spheres: int = 64, r: float = 0.03,
+                    fluid_hi=(0.4, 0.6, 1.0), bulk: float = 1e5, gamma: float = 7.15, viscosity: float = 0.1,
+                    E: float = 1e5, nu: float = 0.3, rho: float = 1000.0, dt: float = 2e-5,
+                    gravity: float = -9.8, track_ids: bool = False) -> tuple[MPMConfig, list[MPMModel]]:
+    """Mixed large scene: J-fluid dam-break block [0,0.4]x[0,0.6]x[0,1] clipped to the
+    two-block sticky margin (bulk 1e5, gamma 7.15 and viscosity 0.1 as the reference's
+    dam-break scene) plus 64 fixed-corotated spheres r=0.03 (E=1e5, nu=0.3) at seeded
+    positions with v0 ~ U(-2,2)^3; 8 ppc; dt=2e-5."""
+    rng = np.random.default_rng(seed)
+    margin = 8 * dx
+    lo = np.array([margin] * 3)
+    hi = np.minimum(np.asarray(fluid_hi), 1.0 - margin)
+    xf = box_particles(lo, hi, dx, ppc, rng)
+    spheres, vels = [], []
+    for _ in range(n_spheres):
+        c = rng.uniform(margin + r + 4 * dx, 1.0 - margin - r - 4 * dx, 3)
+        c[0] = rng.uniform(hi[0] + r + 4 * dx, 1.0 - margin - r - 4 * dx)
+        p = sphere_particles(c, r, dx, ppc, rng)
+        spheres.append(p)
+        vels.append(np.repeat(rng.uniform(-2, 2, (1, 3)).astype(np.float32), len(p), 0))
+    xs = np.concatenate(spheres) if spheres else np.zeros((0, 3), np.float32)
+    vs = np.concatenate(vels) if vels else np.zeros((1, 3), np.float32)
+    n_cells = round(1.0 / dx)
+    cfg = MPMConfig(dx=dx, domain_blocks=(n_cells // 4,) * 3, gravity=gravity, dt=dt, track_ids=track_ids)
+    vol = dx ** 3 / ppc
+    lam, mu = compute_lame_parameters(E, nu)
+    models = [MPMModel(rho * vol, vol, xf, np.zeros((1, 3), np.float32), MPMMaterial.fluid(bulk, gamma, viscosity))]
+    if len(xs):
+        models.append(MPMModel(rho * vol, vol, xs, vs, MPMMaterial.fixed_corotated(lam, mu)))
+    return cfg, models
+
+
+def fluid_box(seed: int = 0, dx: float = 1 / 64, lo=(0.3, 0.3, 0.3), hi=(0.5, 0.6, 0.5), ppc: int = 8,
+              bulk: float = 1e4, gamma: float = 7.15, viscosity: float = 0.1, rho: float = 1000.0,
+              gravity: float = -9.8, v0=(0.5, 0.0, -0.25), track_ids: bool = True) -> tuple[MPMConfig, list[MPMModel]]:
+    """Small J-fluid box for parity tests."""
+    rng = np.random.default_rng(seed)
+    x = box_particles(lo, hi, dx, ppc, rng)
+    n_cells = round(1.0 / dx)
+    cfg = MPMConfig(dx=dx, domain_blocks=(n_cells // 4,) * 3, gravity=gravity, track_ids=track_ids)
+    vol = dx ** 3 / ppc
+    return cfg, [MPMModel(rho * vol, vol, x, np.asarray([v0], np.float32), MPMMaterial.fluid(bulk, gamma, viscosity))]
+
+
+def small_sand(seed: int = 0, dx: float = 1 / 64, r: float = 0.1, h: float = 0.25, ppc: int = 8,
+               E: float = 3.5e5, nu: float = 0.3, rho: float = 1600.0, gravity: float = -9.8,
+               track_ids: bool = True) -> tuple[MPMConfig, list[MPMModel]]:
+    """Small Drucker-Prager column on the slip floor, for parity tests."""
+    rng = np.random.default_rng(seed)
+    y0 = 8 * dx
+    x = cylinder_y_particles((0.5, 0.5), y0, r, h, dx, ppc, rng)
+    n_cells = round(1.0 / dx)
+    cfg = MPMConfig(dx=dx, domain_blocks=(n_cells // 4,) * 3, gravity=gravity, boundary="slip_floor",
+                    floor_cells=8.0, track_ids=track_ids)
+    lam, mu = compute_lame_parameters(E, nu)
+    vol = dx ** 3 / ppc
+    return cfg, [MPMModel(rho * vol, vol, x, np.zeros((1, 3), np.float32), MPMMaterial.drucker_prager(lam, mu))]
+
+
+WORKLOADS = {
+    "jelly_cube": jelly_cube,
+    "sand_column": sand_column,
+    "dam_break_mixed": dam_break_mixed,
+}

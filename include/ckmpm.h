@@ -1,0 +1,182 @@
+/*
+ * ckmpm.h -- C ABI of the B200-native CK-MPM substep engine.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes.  No
+ * exit()/abort(); every failure is reported through the status and
+ * ckmpm_last_error().  One host thread per scene handle; all device memory is
+ * owned by the handle and released by ckmpm_destroy().
+ *
+ * The entry points replace the reference's header-only C++ API
+ * (AppledoreM/CKMPM, include/mpm_engine.cuh), which is a per-GridConfig
+ * singleton that owns its device memory, ends the process on errors and on
+ * completion, and takes its scene constants from compile-time CRTP classes
+ * (include/mpm_config.h:12-124).  Here the same constants travel in
+ * ckmpm_scene_desc at run time.
+ */
+#ifndef CKMPM_H_
+#define CKMPM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ckmpm_scene ckmpm_scene;
+
+typedef enum ckmpm_status {
+  CKMPM_OK = 0,
+  CKMPM_ERR_INVALID = 1,   /* bad argument or call order */
+  CKMPM_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+  CKMPM_ERR_CAPACITY = 3,  /* a block or the block table overflowed */
+  CKMPM_ERR_NUMERIC = 4,   /* non-finite or out-of-range values on the grid */
+  CKMPM_ERR_TIMEOUT = 5,   /* a bounded device-side wait gave up */
+  CKMPM_ERR_NOT_FOUND = 6  /* no such model / buffer too small */
+} ckmpm_status;
+
+/* Constitutive models; the numbering follows MPMConstitutiveModel
+ * (include/mpm_material.cuh:10-18). */
+typedef enum ckmpm_material_kind {
+  CKMPM_FIXED_COROTATED = 0,
+  CKMPM_DRUCKER_PRAGER = 2,
+  CKMPM_FLUID = 3
+} ckmpm_material_kind;
+
+/* Grid boundary rules.  STICKY_BLOCKS is the reference's built-in rule: every
+ * grid block within two blocks of the domain edge gets zero velocity
+ * (include/mpm_algorithm.cuh:765-768,802-805).  SLIP_FLOOR keeps sticky x/z
+ * walls and ceiling, and clamps v_y >= 0 for cells below floor_cells (the
+ * per-cell hook a scene installs through ProcessGridCellVelocity,
+ * include/mpm_config.h:108-117). */
+typedef enum ckmpm_boundary_kind {
+  CKMPM_BOUNDARY_STICKY_BLOCKS = 0,
+  CKMPM_BOUNDARY_SLIP_FLOOR = 1
+} ckmpm_boundary_kind;
+
+/* Scene constants: the getters of MPMConfigBase (include/mpm_config.h:17-123)
+ * and the block extent of MPMDomainRange (include/mpm_domain.h:17-30). */
+typedef struct ckmpm_scene_desc {
+  float dx;                  /* cell size; GetDx() */
+  int32_t domain_blocks[3];  /* domain extent in 4^3-cell blocks; MPMDomainRange<Bx,By,Bz> */
+  float gravity;             /* acceleration along y; GetGravity() */
+  float mass_clamp;          /* nodes with m <= mass_clamp get v = 0; GetMassClamp() */
+  int32_t boundary;          /* ckmpm_boundary_kind */
+  float floor_cells;         /* slip-floor height in cells (SLIP_FLOOR only) */
+  uint32_t max_particles_per_block; /* capacity per 4^3 block (reference: 64 per cell x 64 cells); <= 4096 */
+  int32_t device;            /* CUDA device ordinal */
+  uint32_t flags;            /* CKMPM_FLAG_* */
+} ckmpm_scene_desc;
+
+/* Keep a per-particle original index so state can be returned in input order. */
+#define CKMPM_FLAG_TRACK_IDS 1u
+
+/* Material parameters, MPMMaterial<k>::MaterialParameter_
+ * (include/mpm_material.cuh:63-175): FC / DP use p[0] = lambda, p[1] = mu;
+ * fluid uses p[0] = bulk, p[1] = gamma, p[2] = viscosity, p[3] = J0. */
+typedef struct ckmpm_material {
+  int32_t kind; /* ckmpm_material_kind */
+  float p[4];
+} ckmpm_material;
+
+/* Replaces MPMEngine<GridConfig>::GetInstance() + Initialize(config)
+ * (include/mpm_engine.cuh:80-84,171-191). */
+ckmpm_status ckmpm_create(const ckmpm_scene_desc* desc, ckmpm_scene** out);
+
+/* Replaces MPMModel(mass, volume, x, v, material) (include/mpm_model.h:19-33)
+ * plus the per-model part of MPMEngine::InitializeParticle
+ * (include/mpm_engine.cuh:92-168).  x: n float3 positions, v: nv float3
+ * velocities with nv == 1 (shared) or nv == n.  Host pointers. */
+ckmpm_status ckmpm_add_model(ckmpm_scene* s, const ckmpm_material* material, uint32_t n, const float* x,
+                             const float* v, uint32_t nv, float mass, float volume, int32_t* model_index);
+
+/* Replaces MPMEngine::InitialSetup (include/mpm_engine.cuh:216-383): first
+ * binning, block table, initial state (F = I, logJp = 0, J = J0) and the
+ * initial mass/momentum grid.  The next substep advects with dt = 0, as the
+ * reference's first Simulate step does (include/mpm_engine.cuh:479-480). */
+ckmpm_status ckmpm_setup(ckmpm_scene* s);
+
+/* Replaces the body of MPMEngine::Simulate's substep loop
+ * (include/mpm_engine.cuh:519-876) with the step size fixed: runs nsteps
+ * substeps where each advects with the previous substep's dt and deposits
+ * stress with `dt` (the reference's currentDt / nextDt pair).  Asynchronous on
+ * the scene's stream except for one status read at the end. */
+ckmpm_status ckmpm_step(ckmpm_scene* s, uint32_t nsteps, float dt);
+
+/* Same as ckmpm_step, but enqueues only: no synchronisation and no status
+ * read; call ckmpm_status_check() later. */
+ckmpm_status ckmpm_step_async(ckmpm_scene* s, uint32_t nsteps, float dt);
+
+/* Synchronise the scene's stream and turn the device status word into a code. */
+ckmpm_status ckmpm_status_check(ckmpm_scene* s);
+
+/* Adaptive step, the reference's CFL rule (include/mpm_engine.cuh:552-557):
+ * next dt = min(dt_max, frame_remaining, dx * cfl / max|v_grid|), computed on
+ * the device from the grid of the previous substep.  Advances nsteps substeps
+ * and returns the simulated time in *elapsed (may be NULL). */
+ckmpm_status ckmpm_step_adaptive(ckmpm_scene* s, uint32_t nsteps, float dt_max, float cfl, double frame_time,
+                                 double* elapsed);
+
+/* Use a caller-provided cudaStream_t (passed as void*) for all work of this
+ * scene; NULL selects the scene's own stream. */
+ckmpm_status ckmpm_set_stream(ckmpm_scene* s, void* cuda_stream);
+
+/* Number of live particles of a model (after losses to the domain edge). */
+ckmpm_status ckmpm_get_count(ckmpm_scene* s, int32_t model, uint32_t* n_live);
+
+/* Per-particle state, replacing the export path's RetrieveParticleBuffer +
+ * D2H (include/mpm_algorithm.cuh:1977-2020, include/mpm_engine.cuh:386-454).
+ * Arrays hold n_live entries (x, v: 3 floats; F: 9 floats row-major; aux:
+ * J for fluid, logJp for Drucker-Prager; id: input index).  With
+ * CKMPM_FLAG_TRACK_IDS the arrays are in input order and id is the identity
+ * over live particles; without it they are in block order.  v is the velocity
+ * the next G2P interpolates at each particle (the reference's conservation
+ * probe, include/mpm_algorithm.cuh:1306-1331).  Any pointer may be NULL.
+ * Host pointers; cap is the capacity in particles. */
+ckmpm_status ckmpm_get_state(ckmpm_scene* s, int32_t model, float* x, float* v, float* F, float* aux,
+                             uint32_t* id, uint32_t cap, uint32_t* n_out);
+
+/* Canonical block sets (what MPMPartition holds after a substep,
+ * include/mpm_partition.cuh:37-174 and include/mpm_engine.cuh:659-865):
+ * which = 0: blocks holding particles of `model` (all models if model < 0),
+ * lexicographically sorted, with per-block particle counts in `counts`;
+ * which = 1: plus their {0,1}^3 neighbours (Neighbor policy); which = 2: plus
+ * their {-1,0,1}^3 neighbours (Exterior policy).  keys: int32 triples. */
+ckmpm_status ckmpm_get_blocks(ckmpm_scene* s, int32_t model, int32_t which, int32_t* keys, uint32_t* counts,
+                              uint32_t cap, uint32_t* n_out);
+
+/* Device counters: [0] substeps taken, [1] particles lost at the domain edge,
+ * [2] P2G window escapes (particle skipped in P2G, include/mpm_algorithm.cuh:1670-1683),
+ * [3] status bits, [4] bounded-wait timeouts. */
+ckmpm_status ckmpm_get_counters(ckmpm_scene* s, uint64_t* out5);
+
+/* Current dt pair: [0] the dt the next substep advects with, [1] the dt it deposits stress with. */
+ckmpm_status ckmpm_get_dt(ckmpm_scene* s, float* out2);
+
+/* Run nsteps substeps without graphs, timing every kernel with CUDA events on
+ * the scene's stream.  ms_out[0]: total of the fused G2P2G launches, [1]: total
+ * of the rebinning launches, [2]: number of fused launches. */
+ckmpm_status ckmpm_step_profiled(ckmpm_scene* s, uint32_t nsteps, float dt, double* ms_out3);
+
+/* Device-math test hook: applies one constitutive update to n particles on
+ * the GPU exactly as the substep does (dW = I + dt C; F <- dW F; SVD; return
+ * map; stress).  F (9n), aux (n) are updated in place; tau (9n) receives the
+ * Kirchhoff stress; U, S, V (9n, 3n, 9n, may be NULL) receive the SVD of the
+ * trial F.  Host pointers. */
+ckmpm_status ckmpm_debug_constitutive(const ckmpm_material* material, uint32_t n, const float* C, float dt,
+                                      float* F, float* aux, float* tau, float* U, float* S, float* V);
+
+/* Replaces the process exit at the end of Simulate (include/mpm_engine.cuh:908). */
+ckmpm_status ckmpm_destroy(ckmpm_scene* s);
+
+/* Message of the last failure on this scene (or of the last failed create). */
+const char* ckmpm_last_error(const ckmpm_scene* s);
+
+/* Library version string. */
+const char* ckmpm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CKMPM_H_ */

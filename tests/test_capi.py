@@ -1,0 +1,51 @@
+"""The C-ABI library builds, loads and exports every symbol include/ckmpm.h declares.
+
+No compute calls: these run without a GPU.
+"""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+from ckmpm_b200 import _capi as capi
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols() -> set[str]:
+    text = (ROOT / "include" / "ckmpm.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"\b(ckmpm_[a-z_0-9]+)\s*\(", text))
+
+
+def test_header_declares_the_python_binding_surface():
+    assert declared_symbols() == set(capi.EXPORTED)
+
+
+def test_library_exports_every_declared_symbol(engine_lib):
+    nm = subprocess.run(["nm", "-D", "--defined-only", str(capi.LIB_PATH)], capture_output=True, text=True,
+                        check=True).stdout
+    exported = set(re.findall(r"\bT (ckmpm_[a-z_0-9]+)$", nm, flags=re.M))
+    missing = declared_symbols() - exported
+    assert not missing, missing
+    for name in declared_symbols():
+        assert hasattr(engine_lib, name)
+
+
+def test_version_string(engine_lib):
+    assert engine_lib.ckmpm_version().decode().startswith("ckmpm-b200")
+
+
+def test_null_arguments_are_rejected_without_a_device(engine_lib):
+    h = C.c_void_p()
+    assert engine_lib.ckmpm_create(None, C.byref(h)) == 1
+    assert engine_lib.ckmpm_setup(None) == 1
+    assert engine_lib.ckmpm_step(None, 1, C.c_float(1e-4)) == 1
+    assert engine_lib.ckmpm_destroy(None) == 0
+
+
+def test_header_compiles_as_c():
+    src = '#include "ckmpm.h"\nint main(void){ ckmpm_scene_desc d; (void)d; return (int)CKMPM_OK; }\n'
+    out = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", str(ROOT / "include"), "-x", "c", "-",
+                          "-fsyntax-only"], input=src, capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr

@@ -1,0 +1,211 @@
+"""Parity of the CUDA engine (through the C ABI) against the FP64 oracle.
+
+Tolerances (FP32 engine vs FP64 oracle on the same seeded inputs):
+  * one constitutive update: relative 2e-5 on tau and F (SVD and return map in FP32);
+  * after N substeps: positions within 2e-6 (absolute, domain [0,1]),
+    deformation gradients within 5e-5, velocities within 1e-4 x max|v| + 1e-6,
+    J / logJp within 5e-5;
+  * integer outputs (block sets, per-block counts, live counts): exact.
+"""
+import numpy as np
+import pytest
+
+from ckmpm_b200 import Scene, scenes
+from ckmpm_b200 import _capi as capi
+from ckmpm_b200.engine import MPMConfig, MPMMaterial, MPMModel
+
+pytestmark = pytest.mark.gpu
+
+X_TOL = 2e-6
+F_TOL = 5e-5
+V_REL = 1e-4
+AUX_TOL = 5e-5
+
+
+def run_engine(cfg, models, nsteps, dt):
+    s = Scene(cfg)
+    for m in models:
+        s.add_model(m)
+    s.setup()
+    if nsteps:
+        s.step(nsteps, dt)
+    return s
+
+
+def run_oracle(oracle_mod, cfg, models, nsteps, dt):
+    o = oracle_mod.OracleScene(cfg, models)
+    o.setup()
+    if nsteps:
+        o.step(nsteps, dt)
+    return o
+
+
+def compare(s, o, model=0, x_tol=X_TOL, f_tol=F_TOL, v_rel=V_REL, aux_tol=AUX_TOL, check_aux=False):
+    g = s.state(model)
+    r = o.state(model)
+    alive = np.nonzero(r["alive"])[0]
+    assert len(g.id) == len(alive), "live particle counts differ"
+    assert np.array_equal(g.id, alive.astype(np.uint32))
+    dx = np.abs(g.x - r["x"][alive]).max()
+    dF = np.abs(g.F - r["F"][alive]).max()
+    vmax = np.abs(r["v"][alive]).max()
+    dv = np.abs(g.v - r["v"][alive]).max()
+    daux = np.abs(g.aux - r["aux"][alive]).max() if check_aux else 0.0
+    print(f"max |dx|={dx:.3e} |dF|={dF:.3e} |dv|={dv:.3e} (vmax {vmax:.3e}) |daux|={daux:.3e}")
+    assert dx <= x_tol
+    assert dF <= f_tol
+    assert dv <= v_rel * vmax + 1e-6
+    assert daux <= aux_tol
+    return dx, dF, dv
+
+
+def test_constitutive_matches_oracle(engine_lib, oracle_mod):
+    rng = np.random.default_rng(7)
+    n = 512
+    for kind, params in [(0, [2.9e4, 1.9e4, 0, 0]), (2, [2.0e5, 1.35e5, 0, 0]), (3, [1e5, 7.15, 0.1, 1.0])]:
+        Cm = (0.5 * rng.normal(size=(n, 3, 3))).astype(np.float32)
+        F = (np.eye(3)[None] + 0.15 * rng.normal(size=(n, 3, 3))).astype(np.float32)
+        if kind == 2:
+            F[: n // 4] = np.eye(3) * 1.02  # expansion branch of the return map
+        aux = (np.full(n, 1.0) if kind == 3 else np.zeros(n)).astype(np.float32)
+        dt = 1e-3
+        mat = MPMMaterial(kind={0: "fixed_corotated", 2: "drucker_prager", 3: "fluid"}[kind])
+        cm = capi.Material()
+        cm.kind = kind
+        for i, p in enumerate(params):
+            cm.p[i] = p
+        Fg, ag, tg = F.copy(), aux.copy(), np.zeros_like(F)
+        S = np.zeros((n, 3), np.float32)
+        capi.check(engine_lib.ckmpm_debug_constitutive(cm, n, capi.fptr(Cm), dt, capi.fptr(Fg), capi.fptr(ag),
+                                                       capi.fptr(tg), None, capi.fptr(S), None), "debug")
+        for i in range(n):
+            Fo, ao, to = oracle_mod.constitutive(kind, params, Cm[i].astype(np.float64), dt,
+                                                 F[i].astype(np.float64), float(aux[i]))
+            scale = max(1.0, np.abs(to).max())
+            assert np.abs(tg[i] - to).max() <= 2e-5 * scale * (params[0] + params[1]) / max(params[0], 1) + 1e-3, (kind, i)
+            if kind != 3:
+                assert np.abs(Fg[i] - Fo).max() <= 2e-5 * max(1.0, np.abs(Fo).max()), (kind, i)
+            assert abs(ag[i] - ao) <= 2e-5 * max(1.0, abs(ao)), (kind, i)
+        if kind != 3:
+            # singular values of the trial F (before the return map) match the oracle's SVD
+            for i in range(0, n, 17):
+                Ft = (np.eye(3) + dt * Cm[i].astype(np.float64)) @ F[i].astype(np.float64)
+                _, So, _ = oracle_mod.svd3(Ft)
+                assert np.abs(S[i] - So).max() <= 3e-6 * max(1.0, So[0])
+
+
+def test_setup_binning_exact(engine_lib, oracle_mod):
+    cfg, models = scenes.jelly_cube()
+    s = run_engine(cfg, models, 0, 0.0)
+    o = oracle_mod.OracleScene(cfg, models)
+    for which in (0, 1, 2):
+        kg, cg = s.blocks(0, which)
+        ko, co = o.blocks(0, which)
+        assert np.array_equal(kg, ko)
+        assert np.array_equal(cg, co)
+    assert s.count(0) == len(models[0].particle_position)
+
+
+def test_jelly_parity(engine_lib, oracle_mod):
+    cfg, models = scenes.jelly_cube(lo=(0.42, 0.42, 0.42), hi=(0.58, 0.58, 0.58))
+    s = run_engine(cfg, models, 40, 1e-4)
+    o = run_oracle(oracle_mod, cfg, models, 40, 1e-4)
+    compare(s, o)
+    assert s.counters()["lost"] == 0
+
+
+def test_jelly_rebinning_tracks_positions(engine_lib, oracle_mod):
+    # Blocks after many substeps equal the blocks recomputed from the engine's own positions.
+    cfg, models = scenes.jelly_cube(lo=(0.40, 0.45, 0.40), hi=(0.56, 0.6, 0.52), v0=(1.5, -2.0, 0.7))
+    s = run_engine(cfg, models, 200, 1e-4)
+    st = s.state(0)
+    K = (np.floor(st.x.astype(np.float32) / np.float32(cfg.dx) + np.float32(0.25)).astype(int) - 2) // 4
+    uniq, cnt = np.unique(K, axis=0, return_counts=True)
+    kg, cg = s.blocks(0, 0)
+    assert np.array_equal(kg, uniq.astype(np.int32))
+    assert np.array_equal(cg, cnt.astype(np.uint32))
+    o = run_oracle(oracle_mod, cfg, models, 200, 1e-4)
+    compare(s, o, x_tol=1e-5, f_tol=2e-4, v_rel=5e-4)
+
+
+def test_sand_parity(engine_lib, oracle_mod):
+    cfg, models = scenes.small_sand()
+    s = run_engine(cfg, models, 30, 5e-5)
+    o = run_oracle(oracle_mod, cfg, models, 30, 5e-5)
+    compare(s, o, check_aux=True)
+
+
+def test_fluid_parity(engine_lib, oracle_mod):
+    cfg, models = scenes.fluid_box()
+    s = run_engine(cfg, models, 30, 5e-5)
+    o = run_oracle(oracle_mod, cfg, models, 30, 5e-5)
+    compare(s, o, check_aux=True)
+
+
+def test_two_models_share_the_grid(engine_lib, oracle_mod):
+    cfg, m1 = scenes.jelly_cube(lo=(0.3, 0.3, 0.3), hi=(0.42, 0.42, 0.42), v0=(1.0, 0.0, 0.0))
+    _, m2 = scenes.fluid_box(lo=(0.44, 0.3, 0.3), hi=(0.55, 0.4, 0.42), v0=(-1.0, 0.0, 0.0))
+    models = m1 + m2
+    s = run_engine(cfg, models, 60, 1e-4)
+    o = run_oracle(oracle_mod, cfg, models, 60, 1e-4)
+    compare(s, o, model=0)
+    compare(s, o, model=1, check_aux=True)
+    ku, cu = s.blocks(-1, 0)
+    ko, co = o.blocks(-1, 0)
+    assert np.array_equal(ku, ko) and np.array_equal(cu, co)
+
+
+def test_deterministic_bitwise(engine_lib):
+    cfg, models = scenes.jelly_cube(v0=(0.7, -1.3, 0.4))
+    a = run_engine(cfg, models, 50, 1e-4).state(0)
+    b = run_engine(cfg, models, 50, 1e-4).state(0)
+    assert np.array_equal(a.x.view(np.uint32), b.x.view(np.uint32))
+    assert np.array_equal(a.F.view(np.uint32), b.F.view(np.uint32))
+    assert np.array_equal(a.v.view(np.uint32), b.v.view(np.uint32))
+
+
+def test_first_substep_has_zero_advection(engine_lib):
+    cfg, models = scenes.jelly_cube()
+    s = run_engine(cfg, models, 1, 1e-4)
+    st = s.state(0)
+    assert np.array_equal(st.x, models[0].particle_position[st.id])
+    assert s.dt_pair() == (np.float32(1e-4), np.float32(1e-4))
+
+
+def test_particles_leaving_domain_are_counted(engine_lib, oracle_mod):
+    # Start outside the sticky layer moving out fast, with no walls in the way:
+    # a particle spawned in the last block leaves the domain.
+    cfg = MPMConfig(dx=1 / 64, domain_blocks=(16, 16, 16), gravity=0.0)
+    x = np.array([[0.5, 0.5, 0.5], [0.5, 0.5, 0.51], [1.2, 0.5, 0.5]], np.float32)
+    m = MPMModel(1e-4, 1e-7, x, np.zeros((1, 3), np.float32), MPMMaterial.fixed_corotated(1e2, 1e2))
+    s = run_engine(cfg, [m], 3, 1e-4)
+    assert s.count(0) == 2
+    assert s.counters()["lost"] == 1
+
+
+def test_capacity_overflow_is_reported(engine_lib):
+    cfg, models = scenes.jelly_cube()
+    cfg.max_particles_per_block = 64  # a full block holds 512 particles at 8 ppc
+    s = Scene(cfg)
+    s.add_model(models[0])
+    s.setup()
+    with pytest.raises(capi.CkmpmError) as ei:
+        s.step(1, 1e-4)
+    assert ei.value.code == 3
+
+
+def test_invalid_arguments(engine_lib):
+    cfg, models = scenes.jelly_cube()
+    with pytest.raises(capi.CkmpmError):
+        Scene(MPMConfig(dx=-1.0, domain_blocks=(4, 4, 4)))
+    s = Scene(cfg)
+    with pytest.raises(capi.CkmpmError):
+        s.setup()  # no models
+    with pytest.raises(capi.CkmpmError):
+        s.step(1, 1e-4)  # before setup
+    s.add_model(models[0])
+    s.setup()
+    with pytest.raises(capi.CkmpmError):
+        s.add_model(models[0])  # after setup
+    with pytest.raises(capi.CkmpmError):
+        s.step(1, -1.0)

@@ -1,0 +1,157 @@
+"""Self-checks of the FP64 oracle: the identities the reference's algorithm satisfies.
+
+The oracle (oracle/ckmpm_oracle.cpp) is the checker for the CUDA path; these
+tests pin its arithmetic independently of any GPU: SVD conventions, the CK
+weights, conservation of mass and momentum by P2G, exact transport of a
+uniform velocity field, the first-step dt = 0 rule and the block sets.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from ckmpm_b200 import scenes
+from ckmpm_b200.engine import MPMConfig, MPMMaterial, MPMModel
+
+
+def test_svd_conventions(oracle_mod):
+    rng = np.random.default_rng(0)
+    mats = [rng.normal(size=(3, 3)) for _ in range(50)]
+    mats += [np.eye(3), np.diag([2.0, 2.0, 2.0]), np.diag([1.0, 1.0, -1.0]), np.diag([3.0, 1e-7, 1e-7])]
+    mats += [np.diag([1.5, 1.5, 0.5]) @ np.linalg.qr(rng.normal(size=(3, 3)))[0]]
+    for A in mats:
+        U, S, V = oracle_mod.svd3(A)
+        assert np.allclose(U @ np.diag(S) @ V.T, A, atol=1e-12 * max(1.0, np.abs(A).max()))
+        assert np.allclose(U @ U.T, np.eye(3), atol=1e-12)
+        assert np.allclose(V @ V.T, np.eye(3), atol=1e-12)
+        assert np.linalg.det(U) > 0 and np.linalg.det(V) > 0
+        assert S[0] >= S[1] - 1e-12 >= abs(S[2]) - 2e-12
+        assert S[0] >= 0 and S[1] >= 0
+        if abs(np.linalg.det(A)) > 1e-9:
+            assert np.sign(S[2]) == np.sign(np.linalg.det(A))
+
+
+def test_ck_weight_partition_and_bounds(oracle_mod):
+    for o in np.linspace(0, 1, 101)[:-1]:
+        w0 = oracle_mod.ck_w0(o)
+        assert 0.0 <= w0 <= 1.0
+        assert math.isclose(w0, 1 - o + math.sin(2 * math.pi * o) / (2 * math.pi), abs_tol=1e-15)
+    # The two staggered grids' first moments cancel: sum_g (w1 - o_g) = 0
+    # for offsets half a cell apart (mpm_kernel.cuh:91-114 construction).
+    for s in np.linspace(0.3, 7.7, 37):
+        tot = 0.0
+        for g in (-1, 1):
+            base = int(s - 0.25 * g)
+            o = s - base - 0.25 * g
+            tot += (1 - oracle_mod.ck_w0(o)) - o
+        assert abs(tot) < 1e-12
+
+
+def _rigid_scene(v0, gravity=0.0):
+    cfg, models = scenes.jelly_cube(lo=(0.45, 0.45, 0.45), hi=(0.55, 0.55, 0.55), v0=v0, gravity=gravity)
+    # A "material" with negligible stiffness so the test isolates transport.
+    models[0].material = MPMMaterial.fixed_corotated(1e-6, 1e-6)
+    return cfg, models
+
+
+def test_uniform_translation_is_exact(oracle_mod):
+    v0 = (0.3, -0.2, 0.1)
+    cfg, models = _rigid_scene(v0)
+    o = oracle_mod.OracleScene(cfg, models)
+    o.setup()
+    dt = 1e-3
+    o.step(1, dt)  # first substep advects with dt = 0 (mpm_engine.cuh:479-480)
+    st = o.state(0)
+    assert np.allclose(st["x"], models[0].particle_position, atol=1e-12)
+    o.step(10, dt)
+    st = o.state(0)
+    expect = models[0].particle_position.astype(np.float64) + np.asarray(v0) * 10 * dt
+    assert np.allclose(st["x"], expect, atol=1e-10)
+    assert np.allclose(st["v"], np.asarray(v0)[None, :], atol=1e-10)
+    assert np.allclose(st["F"], np.eye(3)[None], atol=1e-9)
+
+
+def test_p2g_conserves_mass_and_momentum(oracle_mod):
+    cfg, models = scenes.jelly_cube(lo=(0.42, 0.44, 0.46), hi=(0.58, 0.57, 0.55), v0=(0.5, -1.0, 0.25),
+                                    gravity=0.0)
+    o = oracle_mod.OracleScene(cfg, models)
+    o.setup()
+    m = models[0]
+    _, g = o.grid()
+    # Each staggered grid carries the full mass (partition of unity per grid).
+    assert np.isclose(g[:, 0].sum(), 2 * m.particle_mass * m.GetParticleCount(), rtol=1e-12)
+    p0 = g[:, 1:4].sum(axis=(0, 2, 3))
+    o.step(3, 2e-4)
+    _, g = o.grid()
+    assert np.isclose(g[:, 0].sum(), 2 * m.particle_mass * m.GetParticleCount(), rtol=1e-12)
+    p1 = g[:, 1:4].sum(axis=(0, 2, 3))
+    assert np.allclose(p0, p1, rtol=1e-9, atol=1e-12)
+
+
+def test_block_sets(oracle_mod):
+    cfg, models = scenes.jelly_cube()
+    o = oracle_mod.OracleScene(cfg, models)
+    keys, counts = o.blocks(0, 0)
+    x = models[0].particle_position.astype(np.float64)
+    K = ((np.floor(x / cfg.dx + 0.25).astype(int) - 2) // 4)
+    uniq, cnt = np.unique(K, axis=0, return_counts=True)
+    assert np.array_equal(keys, uniq.astype(np.int32))
+    assert np.array_equal(counts, cnt.astype(np.uint32))
+    kn, _ = o.blocks(0, 1)
+    ke, _ = o.blocks(0, 2)
+    sa, sn, se = {tuple(k) for k in keys}, {tuple(k) for k in kn}, {tuple(k) for k in ke}
+    assert sa <= sn <= se
+    for (a, b, c) in sa:
+        for d in np.ndindex(2, 2, 2):
+            assert (a + d[0], b + d[1], c + d[2]) in sn
+        for d in np.ndindex(3, 3, 3):
+            assert (a + d[0] - 1, b + d[1] - 1, c + d[2] - 1) in se
+
+
+def test_sticky_walls_stop_particles(oracle_mod):
+    # Particles driven into the wall stop at the two-block sticky layer.
+    cfg, models = scenes.jelly_cube(lo=(0.2, 0.2, 0.45), hi=(0.3, 0.3, 0.55), v0=(-2.0, 0.0, 0.0), gravity=0.0)
+    o = oracle_mod.OracleScene(cfg, models)
+    o.setup()
+    o.step(400, 2e-4)
+    st = o.state(0)
+    assert st["alive"].all()
+    assert st["x"][:, 0].min() > 6 * cfg.dx
+
+
+def test_drucker_prager_return_map_projects(oracle_mod):
+    lam, mu = 1e4, 1e4
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        F = np.eye(3) + 0.2 * rng.normal(size=(3, 3))
+        if np.linalg.det(F) <= 0.1:
+            continue
+        Fn, logjp, tau = oracle_mod.constitutive(2, [lam, mu, 0, 0], np.zeros((3, 3)), 0.0, F, 0.0)
+        U, S, V = np.linalg.svd(Fn)
+        eps = np.log(np.maximum(np.abs(S), 1e-4))
+        tr = eps.sum()
+        dev = eps - tr / 3
+        ys = 0.816496580927726 * 2 * 0.5 / 2.5
+        # After projection: either expanded (tr >= 0, F -> rotation) or inside the cone.
+        if tr < -1e-12:
+            assert np.linalg.norm(dev) + (3 * lam + 2 * mu) / (2 * mu) * tr * ys <= 1e-6
+        assert np.allclose(tau, tau.T, atol=1e-8 * max(1, np.abs(tau).max()))
+
+
+def test_fluid_pressure(oracle_mod):
+    prm = [1e4, 7.0, 0.0, 1.0]
+    Cm = np.diag([0.1, 0.1, 0.1])
+    F, J, tau = oracle_mod.constitutive(3, prm, Cm, 1e-2, np.eye(3), 1.0)
+    J_expect = 1.0 + 0.3 * 1e-2
+    p = 1e4 * (J_expect ** -7.0 - 1.0)
+    assert math.isclose(J, J_expect, rel_tol=1e-12)
+    assert np.allclose(tau, -p * J_expect * np.eye(3), rtol=1e-12)
+
+
+def test_out_of_domain_particles_are_dropped(oracle_mod):
+    cfg = MPMConfig(dx=1 / 64, domain_blocks=(16, 16, 16), gravity=0.0)
+    x = np.array([[0.5, 0.5, 0.5], [1.5, 0.5, 0.5], [-0.2, 0.5, 0.5]], np.float32)
+    m = MPMModel(1e-3, 1e-6, x, np.zeros((1, 3), np.float32), MPMMaterial.fixed_corotated(1e3, 1e3))
+    o = oracle_mod.OracleScene(cfg, [m])
+    st = o.state(0)
+    assert st["alive"].tolist() == [True, False, False]
