@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--e2e-frame", type=int, default=100, help="substeps between position exports in the e2e run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="profiling driver: set up the workload, run warmup + steps substeps, no timing or baselines")
     return ap.parse_args()
 
 
@@ -326,6 +328,18 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.ncu_case:
+        from ckmpm_b200 import Scene, scenes
+        cfg, models = scenes.sand_column(track_ids=False)
+        cfg.device = local_rank
+        s = Scene(cfg)
+        for m in models:
+            s.add_model(m)
+        s.setup()
+        s.step(args.warmup, cfg.dt)
+        s.step(args.steps, cfg.dt)
+        print(json.dumps({"ncu_case": WORKLOAD, "particles": s.count(0), "substeps": args.warmup + args.steps}))
+        return
     if args.impl == "reference":
         if rank != 0:
             return

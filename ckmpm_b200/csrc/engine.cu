@@ -233,7 +233,9 @@ ckmpm_status ckmpm_create(const ckmpm_scene_desc* desc, ckmpm_scene** out) {
   cudaMemsetAsync(s->scal, 0, sizeof(Scalars), s->stream);
 
   auto set_attr = [&](const void* fn) {
-    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemFused));
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemFused));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   };
   if (set_attr(reinterpret_cast<const void*>(g2p2g_kernel<kFixedCorotated, kFusedThreads>)) != cudaSuccess ||
       set_attr(reinterpret_cast<const void*>(g2p2g_kernel<kDruckerPrager, kFusedThreads>)) != cudaSuccess ||

@@ -163,23 +163,56 @@ __device__ __forceinline__ float4 node_velocity(const SceneDev& sc, const float*
   return v;
 }
 
-// Loads the 2 x 8^3 velocity tile around particle block `key` from grid
-// buffer `gin`, applying the grid update on the fly.  Node (g, lx, ly, lz)
-// sits at tile index g*512 + lx*64 + ly*8 + lz.
+// Velocity tile around particle block `key`.  A particle of the block has its
+// grid -dx/4 base cell at local 2..5 and its grid +dx/4 base cell at local
+// 1..5 (block of a particle = (cell - 2) / 4), so G2P reaches only local nodes
+// 2..6 of grid 0 (5^3) and 1..6 of grid 1 (6^3): 341 nodes, stored as
+// g0: (lx-2)*25 + (ly-2)*5 + (lz-2) and g1: 125 + (lx-1)*36 + (ly-1)*6 + (lz-1).
+constexpr int kVelNodes = 125 + 216;
+
+__device__ __forceinline__ int vtile_index(int g, int lx, int ly, int lz) {
+  return g == 0 ? (lx - 2) * 25 + (ly - 2) * 5 + (lz - 2) : 125 + (lx - 1) * 36 + (ly - 1) * 6 + (lz - 1);
+}
+
+// s_blk[e] (e = 0..7 over the 2x2x2 window) holds the flat index of each
+// window block when it carries this epoch's grid, else -1; filled by
+// window_blocks() before the tile load.
+__device__ __forceinline__ void window_blocks(const SceneDev& sc, const int32_t* __restrict__ stin, int32_t read_epoch,
+                                              int4 key, int64_t* s_blk, int e) {
+  const int bx = key.x + (e >> 2), by = key.y + ((e >> 1) & 1), bz = key.z + (e & 1);
+  int64_t fb = -1;
+  if (in_domain(sc, bx, by, bz)) {
+    const int64_t f = flat_block(sc, bx, by, bz);
+    if (stin[f] == read_epoch) fb = f;
+  }
+  s_blk[e] = fb;
+}
+
+// Loads the velocity tile, applying the grid update on the fly.
 template <int NT>
-__device__ __forceinline__ void load_velocity_tile(const SceneDev& sc, const float* __restrict__ gin,
-                                                   const int32_t* __restrict__ stin, int32_t read_epoch, int4 key,
-                                                   float dt, float4* vtile) {
-  for (int i = threadIdx.x; i < kTileNodes; i += NT) {
-    const int gi = i >> 9, lx = (i >> 6) & 7, ly = (i >> 3) & 7, lz = i & 7;
-    const int bx = key.x + (lx >> 2), by = key.y + (ly >> 2), bz = key.z + (lz >> 2);
+__device__ __forceinline__ void load_velocity_tile(const SceneDev& sc, const float* __restrict__ gin, const int64_t* s_blk,
+                                                   int4 key, float dt, float4* vtile) {
+  for (int i = threadIdx.x; i < kVelNodes; i += NT) {
+    int g, lx, ly, lz;
+    if (i < 125) {
+      g = 0;
+      lx = 2 + i / 25;
+      ly = 2 + (i / 5) % 5;
+      lz = 2 + i % 5;
+    } else {
+      const int j = i - 125;
+      g = 1;
+      lx = 1 + j / 36;
+      ly = 1 + (j / 6) % 6;
+      lz = 1 + j % 6;
+    }
+    const int e = ((lx >> 2) << 2) | ((ly >> 2) << 1) | (lz >> 2);
+    const int64_t fb = s_blk[e];
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (in_domain(sc, bx, by, bz)) {
-      const int64_t fb = flat_block(sc, bx, by, bz);
-      if (stin[fb] == read_epoch) {
-        const int cell = gi * 64 + (lx & 3) * 16 + (ly & 3) * 4 + (lz & 3);
-        v = node_velocity(sc, gin + fb * 512, cell, bx, by, bz, by * 4 + (ly & 3), dt);
-      }
+    if (fb >= 0) {
+      const int cell = g * 64 + (lx & 3) * 16 + (ly & 3) * 4 + (lz & 3);
+      v = node_velocity(sc, gin + fb * 512, cell, key.x + (lx >> 2), key.y + (ly >> 2), key.z + (lz >> 2),
+                        (key.y + (ly >> 2)) * 4 + (ly & 3), dt);
     }
     vtile[i] = v;
   }
@@ -259,12 +292,13 @@ __device__ __forceinline__ void g2p(const float4* __restrict__ vtile, const floa
 #pragma unroll
   for (int g = 0; g < 2; ++g) {
     int l[3];
+    const int lo = g == 0 ? 2 : 1;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       l[a] = st[g][a].base - kb[a];
-      if (l[a] < 0 || l[a] > 6) {
+      if (l[a] < lo || l[a] > 5) {
         inside = false;
-        l[a] = min(max(l[a], 0), 6);
+        l[a] = min(max(l[a], lo), 5);
       }
     }
     const float wx[2] = {st[g][0].w0, 1.f - st[g][0].w0};
@@ -273,12 +307,13 @@ __device__ __forceinline__ void g2p(const float4* __restrict__ vtile, const floa
     float S[3] = {0.f, 0.f, 0.f}, T[3][3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) T[r][0] = T[r][1] = T[r][2] = 0.f;
-    const float4* base = vtile + g * 512 + l[0] * 64 + l[1] * 8 + l[2];
+    const int sx = g == 0 ? 25 : 36, sy = g == 0 ? 5 : 6;
+    const float4* base = vtile + vtile_index(g, l[0], l[1], l[2]);
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
       const int dxn = (n >> 2) & 1, dyn = (n >> 1) & 1, dzn = n & 1;
       const float w = wx[dxn] * wy[dyn] * wz[dzn];
-      const float4 vi = base[dxn * 64 + dyn * 8 + dzn];
+      const float4 vi = base[dxn * sx + dyn * sy + dzn];
       const float wv[3] = {w * vi.x, w * vi.y, w * vi.z};
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
@@ -302,6 +337,18 @@ __device__ __forceinline__ void g2p(const float4* __restrict__ vtile, const floa
   matmul3(B, Di, C);
 #pragma unroll
   for (int r = 0; r < 3; ++r) v[r] = 0.5f * vs[r];
+}
+
+// Exact 64-bit integer add into shared memory with two native 32-bit
+// atomics: the low word's returned old value gives the carry into the high
+// word.  Integer addition is associative, so the final 64-bit value is the
+// exact sum whatever order the adds arrive in (64-bit shared atomics are not
+// native on this part and measured 1.7x slower as a whole kernel).
+__device__ __forceinline__ void fixed_add(unsigned long long* p, long long v) {
+  unsigned* w = reinterpret_cast<unsigned*>(p);
+  const unsigned lo = static_cast<unsigned>(v);
+  const unsigned old = atomicAdd(w, lo);
+  atomicAdd(w + 1, static_cast<unsigned>(v >> 32) + ((old + lo < old) ? 1u : 0u));
 }
 
 // Scatter one particle's mass and momentum into the fixed-point tile.
@@ -333,10 +380,10 @@ __device__ __forceinline__ void p2g_scatter(unsigned long long* __restrict__ pti
         if (dzn) val[r] += Ah[r * 3 + 2];
       }
       unsigned long long* node = base + (dxn * 64 + dyn * 8 + dzn) * 4;
-      atomicAdd(node + 0, static_cast<unsigned long long>(__float2ll_rn(w)));
-      atomicAdd(node + 1, static_cast<unsigned long long>(__float2ll_rn(w * val[0])));
-      atomicAdd(node + 2, static_cast<unsigned long long>(__float2ll_rn(w * val[1])));
-      atomicAdd(node + 3, static_cast<unsigned long long>(__float2ll_rn(w * val[2])));
+      const long long fx[4] = {__float2ll_rn(w), __float2ll_rn(w * val[0]), __float2ll_rn(w * val[1]),
+                               __float2ll_rn(w * val[2])};
+#pragma unroll
+      for (int c = 0; c < 4; ++c) fixed_add(node + c, fx[c]);
     }
   }
 }
@@ -384,20 +431,36 @@ __device__ __forceinline__ void flush_tile(const SceneDev& sc, const BlockListDe
     s_mode[e] = mode;
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < 8 * 512; i += NT) {
-    const int e = i >> 9;
-    const int mode = s_mode[e];
-    if (mode == 2) continue;
-    const int w = i & 511;
-    const int ch = w >> 7, gi = (w >> 6) & 1, cell = w & 63;
-    const int lx = (e >> 2) * 4 + (cell >> 4), ly = ((e >> 1) & 1) * 4 + ((cell >> 2) & 3), lz = (e & 1) * 4 + (cell & 3);
-    const long long sv = static_cast<long long>(ptile[((gi * 8 + lx) * 64 + ly * 8 + lz) * 4 + ch]);
-    const float val = __ll2float_rn(sv) * unit;
-    float* dst = gout + flat_block(sc, key.x + (e >> 2), key.y + ((e >> 1) & 1), key.z + (e & 1)) * 512 + w;
-    if (mode == 0)
-      *dst = val;
-    else
-      *dst = __ldcg(dst) + val;
+  // Four entries per thread per round: all loads of a round issue before its stores.
+  constexpr int kRound = 4;
+  for (int i0 = threadIdx.x; i0 < 8 * 512; i0 += NT * kRound) {
+    float val[kRound], old[kRound];
+    float* dst[kRound];
+    int mode[kRound];
+#pragma unroll
+    for (int r = 0; r < kRound; ++r) {
+      const int i = i0 + r * NT;
+      mode[r] = 2;
+      dst[r] = nullptr;
+      old[r] = 0.f;
+      val[r] = 0.f;
+      if (i < 8 * 512) {
+        const int e = i >> 9;
+        mode[r] = s_mode[e];
+        const int w = i & 511;
+        const int ch = w >> 7, gi = (w >> 6) & 1, cell = w & 63;
+        const int lx = (e >> 2) * 4 + (cell >> 4), ly = ((e >> 1) & 1) * 4 + ((cell >> 2) & 3),
+                  lz = (e & 1) * 4 + (cell & 3);
+        const long long sv = static_cast<long long>(ptile[((gi * 8 + lx) * 64 + ly * 8 + lz) * 4 + ch]);
+        val[r] = __ll2float_rn(sv) * unit;
+        if (mode[r] != 2)
+          dst[r] = gout + flat_block(sc, key.x + (e >> 2), key.y + ((e >> 1) & 1), key.z + (e & 1)) * 512 + w;
+        if (mode[r] == 1) old[r] = __ldcg(dst[r]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kRound; ++r)
+      if (mode[r] != 2) *dst[r] = old[r] + val[r];
   }
   __syncthreads();
   if (threadIdx.x < 8 && s_mode[threadIdx.x] == 0) {
@@ -459,18 +522,17 @@ __device__ __forceinline__ int find_group(const uint32_t* s_off, uint32_t q) {
 }
 
 struct SharedSmall {
+  int64_t blk[8];
+  uint32_t wcnt[8][28];
   uint32_t item;
   uint32_t off[28];
   uint32_t idx[27];
   uint32_t src[27];
-  uint32_t cnt[28];
-  uint32_t pre[28];
-  uint32_t run[28];
   int mode[8];
   uint32_t nflag;
 };
 
-constexpr size_t kSmemVTile = sizeof(float4) * kTileNodes;               // 16 KB
+constexpr size_t kSmemVTile = sizeof(float4) * 344;                      // 5.5 KB (341 nodes)
 constexpr size_t kSmemPTile = sizeof(unsigned long long) * kTileNodes * 4;  // 32 KB
 constexpr size_t kSmemCodes = kMaxParticlesPerBlock;                     // 4 KB
 constexpr size_t kSmemFused = kSmemVTile + kSmemPTile + kSmemCodes;
@@ -483,8 +545,9 @@ constexpr size_t kSmemFused = kSmemVTile + kSmemPTile + kSmemCodes;
 // (:739-869), the advection record (mpm_particle.cuh:333-371) and the
 // per-block list build (:629-649, :1868-1918).
 template <int KIND, int NT>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, 3)
     g2p2g_kernel(SceneDev sc, ModelDev md, GridDev gd, Scalars* __restrict__ scal) {
+  static_assert(NT % 32 == 0 && NT / 32 <= 8 && NT >= 64, "block size");
   extern __shared__ __align__(16) unsigned char smem[];
   float4* vtile = reinterpret_cast<float4*>(smem);
   unsigned long long* ptile = reinterpret_cast<unsigned long long*>(smem + kSmemVTile);
@@ -517,12 +580,14 @@ __global__ void __launch_bounds__(NT, 2)
     const uint32_t start = cur.start[item];
     uint32_t n = cur.count[item];
 
-    if (threadIdx.x < 32) {
+    if (threadIdx.x < 32)
       incoming_groups(sc, prev, key, sh.off, sh.idx, sh.src);
-      if (threadIdx.x < 28) sh.cnt[threadIdx.x] = 0;
-    }
-    load_velocity_tile<NT>(sc, gin, stin, read_epoch, key, dt, vtile);
+    else if (threadIdx.x < 40)
+      window_blocks(sc, stin, read_epoch, key, sh.blk, threadIdx.x - 32);
+    for (int i = threadIdx.x; i < 8 * 28; i += NT) (&sh.wcnt[0][0])[i] = 0u;
     for (int i = threadIdx.x; i < kTileNodes * 4; i += NT) ptile[i] = 0ull;
+    __syncthreads();
+    load_velocity_tile<NT>(sc, gin, sh.blk, key, dt, vtile);
     __syncthreads();
     if (threadIdx.x == 0) {
       uint32_t flags = 0;
@@ -598,7 +663,6 @@ __global__ void __launch_bounds__(NT, 2)
       ok &= in_domain(sc, kk[0] - sh3[0], kk[1] - sh3[1], kk[2] - sh3[2]);
       const int code = ok ? (sh3[0] + 1) * 9 + (sh3[1] + 1) * 3 + (sh3[2] + 1) : 27;
       dcode[q] = static_cast<uint8_t>(code);
-      atomicAdd(&sh.cnt[code], 1u);
       if (!inside) set_status(scal, kStatusOutsideBlock);
       if (!win) {
         atomicAdd(&scal->window_skips, 1u);
@@ -641,42 +705,66 @@ __global__ void __launch_bounds__(NT, 2)
     }
     __syncthreads();
 
-    // Rebin epilogue (warp 0): group counts -> prefix, stable ranks, index list,
-    // next-step block totals.  Meanwhile warp 1 waits for lower colours.
-    if (threadIdx.x < 32) {
-      const int lane = threadIdx.x;
-      const uint32_t c = lane < 28 ? sh.cnt[lane] : 0u;
-      const uint32_t cv = lane < 27 ? c : 0u;
-      uint32_t incl = cv;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-      }
-      if (lane < 27) {
-        sh.pre[lane] = incl - cv;
-        sh.run[lane] = incl - cv;
-        cur.prefix28[item * 28 + lane] = incl - cv;
-        if (c > 0) {
-          const int x = key.x - (lane / 9 - 1), y = key.y - ((lane / 3) % 3 - 1), z = key.z - (lane % 3 - 1);
-          atomicAdd(md.dense_total + flat_block(sc, x, y, z), c);
-        }
-      }
-      if (lane == 26) cur.prefix28[item * 28 + 27] = incl;
-      if (lane == 27 && c > 0) atomicAdd(&scal->lost, c);
-      __syncwarp();
-      for (uint32_t b = 0; b < n; b += 32) {
+    // Rebin epilogue: stable ranks of the particles within their outgoing
+    // direction groups, in two passes over warp-contiguous ranges (per-warp
+    // group counts, then prefix over warps and directions, then ranks), the
+    // index list, this block's 28 group prefixes and the next step's per-block
+    // totals.
+    {
+      constexpr int kWarps = NT / 32;
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      const uint32_t span = ((n + kWarps * 32 - 1) / (kWarps * 32)) * 32;
+      const uint32_t q0 = wid * span, q1 = min(q0 + span, n);
+      const uint32_t lt = (1u << lane) - 1u;
+      for (uint32_t b = q0; b < q1; b += 32) {
         const uint32_t q = b + lane;
-        const int code = q < n ? dcode[q] : 255;
+        const int code = q < q1 ? dcode[q] : 255;
         const uint32_t mask = __match_any_sync(0xffffffffu, code);
-        const uint32_t lt = (1u << lane) - 1u;
-        uint32_t r = 0;
-        if (code < 27) r = sh.run[code] + __popc(mask & lt);
+        if (code < 28 && lane == 31 - __clz(mask)) sh.wcnt[wid][code] += __popc(mask);
         __syncwarp();
-        if (code < 27 && start + r < md.cap_particles) {
-          cur.idx[start + r] = static_cast<uint16_t>(q);
-          if (lane == 31 - __clz(mask)) sh.run[code] += __popc(mask);
+      }
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        uint32_t c = 0;
+        if (lane < 28) {
+#pragma unroll
+          for (int w = 0; w < kWarps; ++w) {
+            const uint32_t t = sh.wcnt[w][lane];
+            sh.wcnt[w][lane] = c;
+            c += t;
+          }
         }
+        const uint32_t cv = lane < 27 ? c : 0u;
+        uint32_t incl = cv;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        if (lane < 27) {
+          const uint32_t pre = incl - cv;
+#pragma unroll
+          for (int w = 0; w < kWarps; ++w) sh.wcnt[w][lane] += pre;
+          cur.prefix28[item * 28 + lane] = pre;
+          if (c > 0) {
+            const int x = key.x - (lane / 9 - 1), y = key.y - ((lane / 3) % 3 - 1), z = key.z - (lane % 3 - 1);
+            atomicAdd(md.dense_total + flat_block(sc, x, y, z), c);
+          }
+        }
+        if (lane == 26) cur.prefix28[item * 28 + 27] = incl;
+        if (lane == 27 && c > 0) atomicAdd(&scal->lost, c);
+      }
+      __syncthreads();
+      for (uint32_t b = q0; b < q1; b += 32) {
+        const uint32_t q = b + lane;
+        const int code = q < q1 ? dcode[q] : 255;
+        const uint32_t mask = __match_any_sync(0xffffffffu, code);
+        if (code < 27) {
+          const uint32_t r = sh.wcnt[wid][code] + __popc(mask & lt);
+          if (start + r < md.cap_particles) cur.idx[start + r] = static_cast<uint16_t>(q);
+        }
+        __syncwarp();
+        if (code < 27 && lane == 31 - __clz(mask)) sh.wcnt[wid][code] += __popc(mask);
         __syncwarp();
       }
     }
@@ -991,8 +1079,12 @@ __global__ void __launch_bounds__(NT) probe_kernel(SceneDev sc, ModelDev md, Gri
     const int4 key = cur.keys[item];
     const uint32_t start = cur.start[item];
     const uint32_t n = cur.count[item];
-    if (threadIdx.x < 32) incoming_groups(sc, prev, key, sh.off, sh.idx, sh.src);
-    load_velocity_tile<NT>(sc, gd.grid[parity], gd.stamp[parity], step, key, dt, vtile);
+    if (threadIdx.x < 32)
+      incoming_groups(sc, prev, key, sh.off, sh.idx, sh.src);
+    else if (threadIdx.x < 40)
+      window_blocks(sc, gd.stamp[parity], step, key, sh.blk, threadIdx.x - 32);
+    __syncthreads();
+    load_velocity_tile<NT>(sc, gd.grid[parity], sh.blk, key, dt, vtile);
     __syncthreads();
     const uint32_t nn = min(n, sh.off[27]);
     for (uint32_t q = threadIdx.x; q < nn; q += NT) {
