@@ -1,0 +1,163 @@
+// TEST INFRASTRUCTURE ONLY: driver of the reference CUDA build (AppledoreM/CKMPM).
+//
+// Compiled (oracle/Makefile, target `ref`) against the reference's own headers
+// where they lie; its output binaries go to oracle/_ref/ and are never part of
+// the product.  It drives the reference through its public API exactly as the
+// reference's scene executables do (tests/fluid_dam_break/test_fluid_dam_break.cu:5-18):
+// MPMEngine::Initialize -> InitializeParticle -> InitialSetup -> Simulate, with
+// a scene configuration class of our own (the reference takes scene constants
+// from compile-time CRTP classes, include/mpm_config.h:12-124).
+//
+// One binary per grid family (cell size, domain extent, gravity, boundary rule):
+//   CKMPM_HARNESS_SCENE_JELLY : dx = 1/64,  16^3 blocks, g = -9.8, sticky walls (the built-in rule)
+//   CKMPM_HARNESS_SCENE_SAND  : dx = 1/256, 64^3 blocks, g = -9.8, slip floor at 8 cells
+//   CKMPM_HARNESS_SCENE_SLIP  : dx = 1/64,  16^3 blocks, g = -9.8, slip floor at 8 cells
+// The slip floor is installed through the reference's irregular-boundary hook
+// (GetExistIrregularBoundary / ProcessGridCellVelocity, include/mpm_algorithm.cuh:795-799):
+// sticky x/z walls and ceiling two blocks deep, v_y >= 0 in cells below the floor.
+//
+// Usage: ref_<scene> <material> <params...4> <mass> <volume> <x.bin> <v.bin> <fps> <frames> <dt> <outdir> <mode>
+//   material: fc | dp | fluid; params: lambda mu 0 0 (fc/dp) or bulk gamma viscosity J0 (fluid)
+//   x.bin / v.bin: float32 xyz triples (v.bin holds 1 or n velocities)
+//   mode 0: export raw positions every frame (outdir/model_0_particle_frame_<k>.txt)
+//   mode 1: profile mode, no export; the reference prints its MPMBenchmark statistics
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <span>
+#include <string>
+#include <vector>
+
+#include "mpm_engine.cuh"
+
+namespace harness {
+
+#if defined(CKMPM_HARNESS_SCENE_SAND)
+constexpr float kDx = 1.f / 256.f;
+constexpr int kBlocks = 64;
+constexpr bool kSlipFloor = true;
+constexpr uint32_t kMaxBlocks = 60000;
+#elif defined(CKMPM_HARNESS_SCENE_SLIP)
+constexpr float kDx = 1.f / 64.f;
+constexpr int kBlocks = 16;
+constexpr bool kSlipFloor = true;
+constexpr uint32_t kMaxBlocks = 4096;
+#else
+constexpr float kDx = 1.f / 64.f;
+constexpr int kBlocks = 16;
+constexpr bool kSlipFloor = false;
+constexpr uint32_t kMaxBlocks = 4096;
+#endif
+constexpr float kGravity = -9.8f;
+constexpr float kFloorCells = 8.f;
+
+// Host-only run parameters (read by Initialize / Simulate on the host).
+inline uint32_t g_fps = 48;
+inline uint32_t g_frames = 1;
+inline float g_dt = 1e-4f;
+
+typedef mpm::MPMDomainRange<kBlocks, kBlocks, kBlocks> DomainRange;
+typedef mpm::MPMDomain<DomainRange, mpm::MPMDomainOffset<0, 0, 0>> Domain;
+typedef mpm::MPMGridConfig<Domain> GridConfig;
+
+class Config : public mpm::MPMConfigBase<Config> {
+ public:
+  friend class mpm::MPMConfigBase<Config>;
+  constexpr Config() = default;
+
+ protected:
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetDxImpl() const -> float { return kDx; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetBlockVolumeImpl() const -> uint32_t { return 64; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetBlockSizeImpl() const -> uint32_t { return 4; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetMaxParticleCountPerCellImpl() const -> uint32_t { return 64; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetMaxParticleCountPerBlockImpl() const -> uint32_t {
+    return GetBlockVolumeImpl() * GetMaxParticleCountPerCellImpl();
+  }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetMaxParticleCountPerBucketImpl() const -> uint32_t { return 32; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetMaxActiveBlockCountImpl() const -> uint32_t { return kMaxBlocks; }
+  MPM_FORCE_INLINE auto GetFpsImpl() const -> uint32_t { return g_fps; }
+  MPM_FORCE_INLINE auto GetDtImpl() const -> float { return g_dt; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetCflImpl() const -> float { return 0.5f; }
+  MPM_FORCE_INLINE auto GetTotalSimulatedFrameCountImpl() const -> uint32_t { return g_frames; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetGravityImpl() const -> float { return kGravity; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetMassClampImpl() const -> float { return 0.f; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetExistRigidParticleImpl() const -> bool { return false; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetRigidParticleCountImpl() const -> uint32_t { return 0; }
+  template <typename Scalar>
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetRigidParticleVelocityImpl(int) const -> mpm::Vector<Scalar, 3> {
+    return mpm::Vector<Scalar, 3>{0.f, 0.f, 0.f};
+  }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetExistIrregularBoundaryImpl() const -> bool { return kSlipFloor; }
+  MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto ProcessGridCellVelocityImpl(const mpm::Vector<int, 3>& cell,
+                                                                      mpm::Vector<float, 3>& velocity, int) const
+      -> void {
+    const int bx = cell[0] / 4, by = cell[1] / 4, bz = cell[2] / 4;
+    const bool wall = bx < 2 || bx + 2 >= kBlocks || bz < 2 || bz + 2 >= kBlocks || by + 2 >= kBlocks;
+    if (wall) {
+      velocity[0] = velocity[1] = velocity[2] = 0.f;
+    } else if (static_cast<float>(cell[1]) < kFloorCells) {
+      velocity[1] = velocity[1] > 0.f ? velocity[1] : 0.f;
+    }
+  }
+  MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto UpdateConfigImpl(float, int) -> void {}
+};
+
+std::vector<mpm::Vector<float, 3>> read_xyz(const char* path) {
+  std::ifstream f(path, std::ios::binary | std::ios::ate);
+  if (!f) {
+    std::fprintf(stderr, "cannot open %s\n", path);
+    std::exit(2);
+  }
+  const size_t bytes = static_cast<size_t>(f.tellg());
+  f.seekg(0);
+  std::vector<mpm::Vector<float, 3>> v(bytes / 12);
+  f.read(reinterpret_cast<char*>(v.data()), static_cast<std::streamsize>(v.size() * 12));
+  return v;
+}
+
+}  // namespace harness
+
+int main(int argc, char** argv) {
+  using namespace harness;
+  if (argc != 15) {
+    std::fprintf(stderr,
+                 "usage: %s fc|dp|fluid p0 p1 p2 p3 mass volume x.bin v.bin fps frames dt outdir mode\n", argv[0]);
+    return 2;
+  }
+  const std::string mat = argv[1];
+  const float p[4] = {std::strtof(argv[2], nullptr), std::strtof(argv[3], nullptr), std::strtof(argv[4], nullptr),
+                      std::strtof(argv[5], nullptr)};
+  const float mass = std::strtof(argv[6], nullptr), volume = std::strtof(argv[7], nullptr);
+  auto x = read_xyz(argv[8]);
+  auto v = read_xyz(argv[9]);
+  g_fps = static_cast<uint32_t>(std::strtoul(argv[10], nullptr, 10));
+  g_frames = static_cast<uint32_t>(std::strtoul(argv[11], nullptr, 10));
+  g_dt = std::strtof(argv[12], nullptr);
+  const std::string outdir = argv[13];
+  const int mode = std::atoi(argv[14]);
+
+  std::vector<mpm::MPMModelVariant> models;
+  using namespace mpm;
+  if (mat == "fc") {
+    using M = MPMMaterial<MPMConstitutiveModel::kFixedCorotated>;
+    models.emplace_back(MPMModel<M>{mass, volume, std::span<const Vector<float, 3>>(x),
+                                    std::span<const Vector<float, 3>>(v), M{M::MaterialParameter_{p[0], p[1]}}});
+  } else if (mat == "dp") {
+    using M = MPMMaterial<MPMConstitutiveModel::kDruckerPragerStvkhencky>;
+    models.emplace_back(MPMModel<M>{mass, volume, std::span<const Vector<float, 3>>(x),
+                                    std::span<const Vector<float, 3>>(v), M{M::MaterialParameter_{p[0], p[1]}}});
+  } else {
+    using M = MPMMaterial<MPMConstitutiveModel::kFluid>;
+    models.emplace_back(MPMModel<M>{mass, volume, std::span<const Vector<float, 3>>(x),
+                                    std::span<const Vector<float, 3>>(v),
+                                    M{M::MaterialParameter_{p[0], p[1], p[2], p[3]}}});
+  }
+  Config config;
+  auto* engine = MPMEngine<GridConfig>::GetInstance();
+  engine->Initialize(config);
+  engine->InitializeParticle(config, models);
+  engine->InitialSetup(config);
+  // Simulate ends the process itself (include/mpm_engine.cuh:908).
+  engine->Simulate(config, outdir, false, mode == 0, mode == 1);
+  return 0;
+}
