@@ -545,7 +545,7 @@ constexpr size_t kSmemFused = kSmemVTile + kSmemPTile + kSmemCodes;
 // (:739-869), the advection record (mpm_particle.cuh:333-371) and the
 // per-block list build (:629-649, :1868-1918).
 template <int KIND, int NT>
-__global__ void __launch_bounds__(NT, 3)
+__global__ void __launch_bounds__(NT, 4)
     g2p2g_kernel(SceneDev sc, ModelDev md, GridDev gd, Scalars* __restrict__ scal) {
   static_assert(NT % 32 == 0 && NT / 32 <= 8 && NT >= 64, "block size");
   extern __shared__ __align__(16) unsigned char smem[];

@@ -129,7 +129,7 @@ CKMPM_DEV void swap_cols(float* V, float& la, float& lb, int a, int b) {
   }
 }
 
-template <int kSweeps = 5>
+template <int kSweeps = 4>
 CKMPM_DEV void svd3(const float* A, float* U, float* S, float* V) {
   // M = A^T A (symmetric; 6 unique entries)
   float m00 = A[0] * A[0] + A[3] * A[3] + A[6] * A[6];
