@@ -1,0 +1,215 @@
+// ckmpm/mpm_engine.hpp -- header-only C++ shim over the C ABI (ckmpm.h) that
+// keeps the reference's engine/material/model/config names and call order, so
+// existing scene code of AppledoreM/CKMPM changes little to run on this engine:
+//
+//   reference (include/mpm_engine.cuh, include/mpm_model.h, ...)      this shim
+//   MPMEngine<GridConfig>::GetInstance()                      ->    ckmpm::MPMEngine (an ordinary object)
+//   Initialize(config)            (:171)                      ->    Initialize(config)
+//   InitializeParticle(config, models) (:92)                  ->    InitializeParticle(config, models)
+//   InitialSetup(config)          (:216)                      ->    InitialSetup(config)
+//   Simulate(config, dir, conservation, binary, profile) (:457) ->  Simulate(config, export_fn) -- returns
+//   MPMModel<MPMMaterial<k>>(mass, volume, x, v, material)    ->    ckmpm::MPMModel(mass, volume, x, v, material)
+//   MPMConfigBase<Derived> getters (include/mpm_config.h)     ->    ckmpm::MPMConfig (run-time fields, same getters)
+//
+// Differences are at the boundary only: scene constants are run-time values,
+// errors throw ckmpm::Error (the reference calls exit()/abort()), and Simulate
+// returns instead of ending the process.
+#pragma once
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <functional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../ckmpm.h"
+
+namespace ckmpm {
+
+struct Error : std::runtime_error {
+  ckmpm_status code;
+  Error(ckmpm_status c, const std::string& what) : std::runtime_error(what), code(c) {}
+};
+
+inline void check(ckmpm_status s, const ckmpm_scene* h, const char* where) {
+  if (s != CKMPM_OK) throw Error(s, std::string(where) + ": " + ckmpm_last_error(h));
+}
+
+using Vector3 = std::array<float, 3>;
+
+// ComputeLameParameters (include/mpm_material.cuh:277-283).
+inline std::array<float, 2> ComputeLameParameters(float E, float nu) {
+  return {E * nu / ((1 + nu) * (1 - 2 * nu)), E / (2 * (1 + nu))};
+}
+
+// MPMConstitutiveModel (include/mpm_material.cuh:10-18), the subset on this path.
+enum class MPMConstitutiveModel : int32_t {
+  kFixedCorotated = CKMPM_FIXED_COROTATED,
+  kDruckerPragerStvkhencky = CKMPM_DRUCKER_PRAGER,
+  kFluid = CKMPM_FLUID,
+};
+
+// MPMMaterial<k>::MaterialParameter_ collapsed into one run-time value type.
+struct MPMMaterial {
+  MPMConstitutiveModel kind = MPMConstitutiveModel::kFixedCorotated;
+  float p[4] = {0, 0, 0, 0};
+  static MPMMaterial FixedCorotated(float lambda, float mu) { return {MPMConstitutiveModel::kFixedCorotated, {lambda, mu, 0, 0}}; }
+  static MPMMaterial DruckerPrager(float lambda, float mu) {
+    return {MPMConstitutiveModel::kDruckerPragerStvkhencky, {lambda, mu, 0, 0}};
+  }
+  static MPMMaterial Fluid(float bulk, float gamma, float viscosity, float J0 = 1.0f) {
+    return {MPMConstitutiveModel::kFluid, {bulk, gamma, viscosity, J0}};
+  }
+  ckmpm_material c() const {
+    ckmpm_material m{};
+    m.kind = static_cast<int32_t>(kind);
+    for (int i = 0; i < 4; ++i) m.p[i] = p[i];
+    return m;
+  }
+};
+
+// MPMModel (include/mpm_model.h:11-59).
+class MPMModel {
+ public:
+  MPMModel(float particleMass, float particleVolume, std::vector<Vector3> particlePosition,
+           std::vector<Vector3> particleVelocity, MPMMaterial material, double freezeTime = 0.0)
+      : mass_(particleMass), volume_(particleVolume), x_(std::move(particlePosition)),
+        v_(std::move(particleVelocity)), material_(material), freeze_(freezeTime) {
+    if (v_.size() != 1 && v_.size() != x_.size())
+      throw Error(CKMPM_ERR_INVALID, "particle velocity must hold 1 or n entries");
+  }
+  float GetParticleMass() const { return mass_; }
+  float GetParticleVolume() const { return volume_; }
+  uint32_t GetParticleCount() const { return static_cast<uint32_t>(x_.size()); }
+  const MPMMaterial& GetParticleMaterial() const { return material_; }
+  const std::vector<Vector3>& GetParticlePosition() const { return x_; }
+  const std::vector<Vector3>& GetParticleVelocity() const { return v_; }
+  bool IsFreezed(double elapsedSeconds) const { return elapsedSeconds < freeze_; }
+
+ private:
+  float mass_, volume_;
+  std::vector<Vector3> x_, v_;
+  MPMMaterial material_;
+  double freeze_;
+};
+
+// MPMConfigBase getters as run-time fields (include/mpm_config.h:17-123).
+struct MPMConfig {
+  float dx = 1.f / 64.f;
+  std::array<int32_t, 3> domainBlocks = {16, 16, 16};  // MPMDomainRange<Bx, By, Bz>
+  float gravity = -9.8f;
+  float massClamp = 0.f;
+  float dt = 1e-4f;
+  float cfl = 0.5f;
+  uint32_t fps = 48;
+  uint32_t totalFrames = 1;
+  ckmpm_boundary_kind boundary = CKMPM_BOUNDARY_STICKY_BLOCKS;
+  float floorCells = 8.f;
+  uint32_t maxParticleCountPerBlock = 4096;
+  bool trackIds = true;
+  int32_t device = 0;
+
+  float GetDx() const { return dx; }
+  float GetInvDx() const { return 1.f / dx; }
+  uint32_t GetBlockSize() const { return 4; }
+  uint32_t GetBlockVolume() const { return 64; }
+  uint32_t GetMaxParticleCountPerBlock() const { return maxParticleCountPerBlock; }
+  uint32_t GetFps() const { return fps; }
+  float GetDt() const { return dt; }
+  float GetCfl() const { return cfl; }
+  uint32_t GetTotalSimulatedFrameCount() const { return totalFrames; }
+  float GetGravity() const { return gravity; }
+  float GetMassClamp() const { return massClamp; }
+
+  ckmpm_scene_desc c() const {
+    ckmpm_scene_desc d{};
+    d.dx = dx;
+    for (int i = 0; i < 3; ++i) d.domain_blocks[i] = domainBlocks[i];
+    d.gravity = gravity;
+    d.mass_clamp = massClamp;
+    d.boundary = boundary;
+    d.floor_cells = floorCells;
+    d.max_particles_per_block = maxParticleCountPerBlock;
+    d.device = device;
+    d.flags = trackIds ? CKMPM_FLAG_TRACK_IDS : 0u;
+    return d;
+  }
+};
+
+// MPMEngine (include/mpm_engine.cuh:29-974) with the same call order.
+class MPMEngine {
+ public:
+  MPMEngine() = default;
+  MPMEngine(const MPMEngine&) = delete;
+  MPMEngine& operator=(const MPMEngine&) = delete;
+  ~MPMEngine() {
+    if (scene_) ckmpm_destroy(scene_);
+  }
+
+  // Initialize: dt = min(config dt, 1 / fps) (include/mpm_engine.cuh:178).
+  void Initialize(const MPMConfig& config) {
+    const ckmpm_scene_desc d = config.c();
+    check(ckmpm_create(&d, &scene_), nullptr, "ckmpm_create");
+    dt_ = std::min(config.GetDt(), 1.0f / static_cast<float>(config.GetFps()));
+  }
+
+  // InitializeParticle: one engine model per MPMModel; dt shrinks by the CFL
+  // bound of the initial velocities (include/mpm_engine.cuh:109-117).
+  void InitializeParticle(const MPMConfig& config, const std::vector<MPMModel>& models) {
+    for (const auto& m : models) {
+      float vmax = 0.f;
+      for (const auto& v : m.GetParticleVelocity()) vmax = std::max(vmax, std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+      if (vmax > 0.f) dt_ = std::min(dt_, config.GetDx() * config.GetCfl() / vmax);
+      const ckmpm_material mat = m.GetParticleMaterial().c();
+      int32_t idx = 0;
+      check(ckmpm_add_model(scene_, &mat, m.GetParticleCount(), m.GetParticlePosition()[0].data(),
+                            m.GetParticleVelocity()[0].data(), static_cast<uint32_t>(m.GetParticleVelocity().size()),
+                            m.GetParticleMass(), m.GetParticleVolume(), &idx),
+            scene_, "ckmpm_add_model");
+      counts_.push_back(m.GetParticleCount());
+    }
+  }
+
+  void InitialSetup(const MPMConfig&) { check(ckmpm_setup(scene_), scene_, "ckmpm_setup"); }
+
+  // Simulate: GetTotalSimulatedFrameCount() frames of round((1/fps)/dt)
+  // substeps at the fixed dt; export(frame, engine) runs after every frame
+  // (the reference's ExportParticleToModel point, include/mpm_engine.cuh:880-883).
+  // Returns the number of substeps taken instead of ending the process.
+  uint64_t Simulate(const MPMConfig& config, const std::function<void(uint32_t, MPMEngine&)>& exportFrame = {}) {
+    const uint32_t perFrame = std::max<uint32_t>(
+        1u, static_cast<uint32_t>(std::lround((1.0 / config.GetFps()) / static_cast<double>(dt_))));
+    uint64_t total = 0;
+    for (uint32_t f = 0; f < config.GetTotalSimulatedFrameCount(); ++f) {
+      check(ckmpm_step(scene_, perFrame, dt_), scene_, "ckmpm_step");
+      total += perFrame;
+      if (exportFrame) exportFrame(f, *this);
+    }
+    return total;
+  }
+
+  // Positions of a model (input order when ids are tracked), the export path's
+  // RetrieveParticleBuffer + copy (include/mpm_engine.cuh:386-454).
+  std::vector<Vector3> GetParticlePosition(int32_t model) {
+    uint32_t n = 0;
+    check(ckmpm_get_count(scene_, model, &n), scene_, "ckmpm_get_count");
+    std::vector<Vector3> x(n);
+    uint32_t out = 0;
+    check(ckmpm_get_state(scene_, model, n ? x[0].data() : nullptr, nullptr, nullptr, nullptr, nullptr, n, &out),
+          scene_, "ckmpm_get_state");
+    return x;
+  }
+
+  float GetDt() const { return dt_; }
+  ckmpm_scene* Handle() { return scene_; }
+
+ private:
+  ckmpm_scene* scene_ = nullptr;
+  float dt_ = 0.f;
+  std::vector<uint32_t> counts_;
+};
+
+}  // namespace ckmpm

@@ -1,0 +1,79 @@
+"""Generate the golden fixtures: outputs of the reference CUDA build on seeded scenes.
+
+Run on a machine with a GPU and the reference harness built (make -C oracle ref):
+
+    python tests/golden/make_golden.py <outdir>
+
+For each scene below it runs the reference's stock MPMEngine::Simulate
+(oracle/_ref/ref_<family>, oracle/ref_harness.cu) twice and stores, per exported
+frame, the reference's particle positions (unordered, as the reference exports
+them), the largest nearest-neighbour distance between the two runs (the
+reference's own run-to-run spread, from its float atomics), and the inputs'
+checksum.  dt is a power of two and fps = 1 / (16 dt), so each frame is exactly
+16 substeps and the reference's frame clipping never changes dt; the first
+substep advects with dt = 0 as in the reference.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from ckmpm_b200 import scenes  # noqa: E402
+from oracle import ref_runner  # noqa: E402
+
+DT = 2.0 ** -14          # 6.103515625e-05, exact in float and double
+SUBSTEPS_PER_FRAME = 16
+FPS = 1024               # 1 / (16 * 2^-14)
+FRAMES = 8               # 128 substeps
+KEEP = (1, 7)            # frames stored: after 32 and 128 substeps
+
+
+def golden_scenes():
+    """(name, harness family, config, model) of every fixture."""
+    cfg, m = scenes.jelly_cube(lo=(0.44, 0.44, 0.44), hi=(0.56, 0.56, 0.56), v0=(0.3, -1.0, 0.2))
+    yield "jelly_fc", "jelly", cfg, m[0]
+    cfg, m = scenes.fluid_box(lo=(0.32, 0.3, 0.34), hi=(0.44, 0.42, 0.46), v0=(0.5, 0.0, -0.25))
+    yield "fluid", "jelly", cfg, m[0]
+    cfg, m = scenes.small_sand(r=0.06, h=0.15)
+    yield "sand_dp", "slip", cfg, m[0]
+
+
+def checksum(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()[:16]
+
+
+def main(outdir: str) -> None:
+    out = Path(outdir)
+    out.mkdir(parents=True, exist_ok=True)
+    meta = {}
+    for name, family, cfg, model in golden_scenes():
+        runs = []
+        for _ in range(2):
+            _, d = ref_runner.run(family, model, FPS, FRAMES, DT, 0)
+            runs.append(ref_runner.frames_out(d, FRAMES))
+        spread = []
+        for k in range(FRAMES):
+            _, dist = ref_runner.match_nn(runs[0][k], runs[1][k])
+            spread.append(float(dist.max()))
+        arrays = {f"frame{k}": runs[0][k] for k in KEEP}
+        np.savez_compressed(out / f"{name}.npz", **arrays)
+        meta[name] = {"family": family, "n": int(len(model.particle_position)),
+                      "input_sha": checksum(model.particle_position), "dt": DT, "fps": FPS, "frames": FRAMES,
+                      "substeps_per_frame": SUBSTEPS_PER_FRAME, "kept_frames": list(KEEP),
+                      "reference_run_to_run_spread": spread,
+                      "material": model.material.kind, "params": model.material.params(),
+                      "mass": model.particle_mass, "volume": model.particle_volume,
+                      "counts": [int(len(runs[0][k])) for k in range(FRAMES)]}
+        print(name, meta[name]["n"], "spread", max(spread), flush=True)
+    (out / "golden.json").write_text(json.dumps(meta, indent=1))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else str(Path(__file__).resolve().parent))
