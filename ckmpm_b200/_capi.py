@@ -39,7 +39,7 @@ EXPORTED = (
     "ckmpm_status_check", "ckmpm_step_adaptive", "ckmpm_set_stream", "ckmpm_get_count",
     "ckmpm_get_state", "ckmpm_get_blocks", "ckmpm_get_counters", "ckmpm_get_dt",
     "ckmpm_step_profiled", "ckmpm_debug_constitutive", "ckmpm_destroy", "ckmpm_last_error",
-    "ckmpm_version",
+    "ckmpm_version", "ckmpm_simulate_noalloc",
 )
 
 
@@ -100,6 +100,9 @@ def lib() -> C.CDLL:
         L.ckmpm_step_profiled.argtypes = [P, C.c_uint32, C.c_float, C.POINTER(C.c_double)]
         L.ckmpm_debug_constitutive.argtypes = [C.POINTER(Material), C.c_uint32, f32p, C.c_float, f32p, f32p, f32p,
                                                f32p, f32p, f32p]
+        L.ckmpm_simulate_noalloc.argtypes = [C.POINTER(SceneDesc), C.POINTER(Material), C.c_uint32, P, P, C.c_uint32,
+                                             C.c_float, C.c_float, C.c_uint32, C.c_float, P, P, P, P, P,
+                                             C.POINTER(C.c_uint32), C.POINTER(C.c_char_p)]
         L.ckmpm_destroy.argtypes = [P]
         L.ckmpm_last_error.argtypes = [P]
         L.ckmpm_last_error.restype = C.c_char_p

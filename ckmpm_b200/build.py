@@ -1,6 +1,6 @@
 """Build script for the native parts of ckmpm_b200.
 
-Compiles the CUDA engine (csrc/engine.cu) into ckmpm_b200/_lib/libckmpm_b200.so
+Compiles the CUDA engine (csrc/library.cu: engine.cu + noalloc.cu) into ckmpm_b200/_lib/libckmpm_b200.so
 for sm_100a with nvcc.  The .so is built in-tree so that it travels with the
 repository snapshot.
 """
@@ -16,8 +16,9 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libckmpm_b200.so"
-SOURCES = [PKG / "csrc" / "engine.cu"]
-DEPS = SOURCES + [PKG / "csrc" / "kernels.cuh", PKG / "csrc" / "mpm_math.cuh", ROOT / "include" / "ckmpm.h"]
+SOURCES = [PKG / "csrc" / "library.cu"]
+DEPS = SOURCES + [PKG / "csrc" / "engine.cu", PKG / "csrc" / "noalloc.cu", PKG / "csrc" / "kernels.cuh",
+                  PKG / "csrc" / "mpm_math.cuh", ROOT / "include" / "ckmpm.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

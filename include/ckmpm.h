@@ -166,6 +166,27 @@ ckmpm_status ckmpm_step_profiled(ckmpm_scene* s, uint32_t nsteps, float dt, doub
 ckmpm_status ckmpm_debug_constitutive(const ckmpm_material* material, uint32_t n, const float* C, float dt,
                                       float* F, float* aux, float* tau, float* U, float* S, float* V);
 
+/* No counterpart in the reference.  Runs one complete simulation of a single
+ * model -- setup and nsteps substeps, the same kernels in the same order as
+ * ckmpm_create / ckmpm_add_model / ckmpm_setup / ckmpm_step / ckmpm_get_state
+ * -- without allocating any memory, for callers that cannot call cudaMalloc:
+ * code running while another framework captures a CUDA graph on the stream,
+ * plugins whose host runtime owns the device memory budget, and real-time
+ * loops that cannot take the device-wide synchronisation of an allocation.
+ * All scratch lives in one fixed __device__ array of 34.7 MB that every GPU
+ * loading this library keeps until exit; limits: n <= 65536 particles and at
+ * most 4096 blocks in the domain (e.g. 16^3), else CKMPM_ERR_CAPACITY.  The
+ * first call on a device looks up the array's device address, so make that
+ * first call before any stream capture.  x, v (nv = 1 or n float3) and the
+ * outputs x_out, v_out (3n), F_out (9n), aux_out (n) are DEVICE pointers in
+ * input order (outputs may be NULL; particles lost at the domain edge read
+ * NaN).  Every call reuses the same array and clears what it needs: calls that
+ * overlap on the GPU race.  *message (may be NULL) receives a static string. */
+ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, const ckmpm_material* material, uint32_t n,
+                                    const float* x, const float* v, uint32_t nv, float mass, float volume,
+                                    uint32_t nsteps, float dt, void* cuda_stream, float* x_out, float* v_out,
+                                    float* F_out, float* aux_out, uint32_t* n_live, const char** message);
+
 /* Replaces the process exit at the end of Simulate (include/mpm_engine.cuh:908). */
 ckmpm_status ckmpm_destroy(ckmpm_scene* s);
 
