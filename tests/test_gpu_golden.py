@@ -1,0 +1,45 @@
+"""The CUDA engine against the reference CUDA build's own outputs (golden fixtures).
+
+Same fixtures and matching as tests/test_golden.py.  Both builds are FP32 and
+round the position update the same way, so the tolerance is the oracle test's
+(1e-6 + N * 2^-24 on positions, x 2 for Drucker-Prager), which bounds the
+reference's run-to-run spread too.
+"""
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from ckmpm_b200 import Scene
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def test_engine_matches_reference_build(engine_lib):
+    import sys
+    sys.path.insert(0, str(GOLDEN))
+    import make_golden
+    from test_golden import nn_error, tolerance
+    meta = json.loads((GOLDEN / "golden.json").read_text())
+    for name, family, cfg, model in make_golden.golden_scenes():
+        m = meta[name]
+        fx = np.load(GOLDEN / f"{name}.npz")
+        s = Scene(cfg)
+        s.add_model(model)
+        s.setup()
+        done = 0
+        for k in m["kept_frames"]:
+            target = (k + 1) * m["substeps_per_frame"]
+            s.step(target - done, m["dt"])
+            done = target
+            x = s.state(0).x
+            ref = fx[f"frame{k}"]
+            assert len(x) == len(ref) == m["counts"][k]
+            err = nn_error(x, ref)
+            print(f"{name} frame {k} ({target} substeps): engine vs reference {err:.3e}")
+            assert err <= tolerance(name, target), (name, k, err)
+        s.close()
