@@ -32,7 +32,15 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "particle-substeps/s"
-WORKLOAD = "sand_column_collapse: drucker-prager, dx=1/256 (64^3 blocks), cylinder r=0.1 h=0.4, 8 ppc, dt=5e-5, slip floor"
+WORKLOADS = {
+    "sand_column": "sand_column_collapse: drucker-prager, dx=1/256 (64^3 blocks), cylinder r=0.1 h=0.4, 8 ppc, "
+                   "dt=5e-5, slip floor",
+    "jelly_cube": "jelly_cube: fixed-corotated, dx=1/64 (16^3 blocks), cube [0.4,0.6]^3, 8 ppc, v0=(0,-1,0), "
+                  "dt=1e-4, sticky walls",
+    "dam_break_mixed": "dam_break_mixed: j-fluid block + 64 fixed-corotated spheres, dx=1/512 (128^3 blocks), 8 ppc, "
+                       "dt=2e-5, sticky walls",
+}
+REFERENCE_FAMILY = {"sand_column": "sand", "jelly_cube": "jelly"}
 STATE_BYTES = {0: 48, 2: 52, 3: 16}  # x + F (+ logJp) or x + J, read once and written once per substep
 
 
@@ -46,6 +54,7 @@ def parse():
     ap.add_argument("--e2e-frame", type=int, default=100, help="substeps between position exports in the e2e run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sand_column")
     ap.add_argument("--ncu-case", action="store_true",
                     help="profiling driver: set up the workload, run warmup + steps substeps, no timing or baselines")
     return ap.parse_args()
@@ -140,9 +149,23 @@ def committed_traffic() -> float | None:
 
 
 # ---------------------------------------------------------------- CPU baselines
-def cpu_baseline_oracle(cfg, models, seconds: float) -> dict:
-    """FP64 oracle (the reference algorithm restated serially) on the bench workload."""
+def cpu_baseline_oracle(cfg, models, seconds: float, max_particles: int = 2_000_000) -> dict:
+    """FP64 oracle (the reference algorithm restated serially) on the bench workload.
+
+    Scenes above max_particles are sampled: the first particles of each model in
+    seeding order (a contiguous slab of the lattice), up to the cap in total."""
+    import dataclasses
+
     from oracle import oracle as O
+    total = sum(len(m.particle_position) for m in models)
+    note = ""
+    if total > max_particles:
+        keep = max_particles / total
+        models = [dataclasses.replace(m, particle_position=m.particle_position[:max(1, int(len(m.particle_position) * keep))],
+                                      particle_velocity=m.particle_velocity[:1] if len(m.particle_velocity) == 1 else
+                                      m.particle_velocity[:max(1, int(len(m.particle_position) * keep))])
+                  for m in models]
+        note = f" (sample: first {keep:.2%} of each model's particles in seeding order)"
     o = O.OracleScene(cfg, models)
     o.setup()
     n = sum(len(m.particle_position) for m in models)
@@ -156,7 +179,7 @@ def cpu_baseline_oracle(cfg, models, seconds: float) -> dict:
     t = time.perf_counter() - t0
     o.close()
     return {"value": n * k / t, "unit": METRIC, "cores": 1, "kind": "port",
-            "sample": f"FP64 serial oracle (oracle/ckmpm_oracle.cpp), {k} substeps of the full {n}-particle scene "
+            "sample": f"FP64 serial oracle (oracle/ckmpm_oracle.cpp), {k} substeps of {n} particles{note} "
                       f"after one untimed substep, {t:.1f} s"}
 
 
@@ -189,15 +212,20 @@ def cpu_baseline_pic(seconds: float) -> dict:
 
 
 # ---------------------------------------------------------------- our arm
+def workload(name: str):
+    from ckmpm_b200 import scenes
+    return scenes.WORKLOADS[name](track_ids=False)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
-    from ckmpm_b200 import Scene, scenes
+    from ckmpm_b200 import Scene
 
     torch.cuda.set_device(local_rank)
     # A side stream: the legacy default stream cannot be captured into a CUDA graph.
     stream = torch.cuda.Stream()
-    cfg, models = scenes.sand_column(track_ids=False)
+    cfg, models = workload(args.workload)
     cfg.device = local_rank
     dt = cfg.dt
     n_total = sum(len(m.particle_position) for m in models)
@@ -238,14 +266,15 @@ def run_ours(args, rank, world, local_rank):
     fused_ms, other_ms, launches = s.step_profiled(args.profile_steps, dt)
     avg_fused = fused_ms / max(launches, 1)
     grid_blocks = len(s.blocks(-1, 1)[0])
-    S = STATE_BYTES[models[0].material.kind_code]
-    alg_bytes = n_live * (2 * S + 8) + 7168 * grid_blocks
+    alg_bytes = 7168 * grid_blocks
+    for i, m in enumerate(models):
+        alg_bytes += s.count(i) * (2 * STATE_BYTES[m.material.kind_code] + 8)
     peak, peak_kind = measured_peak()
     achieved = alg_bytes / (avg_fused / 1e3) / 1e9
-    tpp = committed_traffic()
+    tpp = committed_traffic() if args.workload == "sand_column" else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (tpp * n_live) if tpp else None,
-                "kernel": "g2p2g_kernel<DruckerPrager> (fused grid update + G2P + SVD/return map + rebin + P2G)",
+                "kernel": "g2p2g_kernel (fused grid update + G2P + SVD/return map + rebin + P2G), all models",
                 "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_fused,
                 "peak_source": f"{peak_kind} hbm_gbs", "fused_share": fused_ms / max(fused_ms + other_ms, 1e-9)}
     s.close()
@@ -269,8 +298,9 @@ def run_ours(args, rank, world, local_rank):
     for k in range(args.steps):
         s2.step(1, dt)  # one substep + device->host read of its status word
         if (k + 1) % args.e2e_frame == 0:
-            capi.check(L.ckmpm_get_state(s2._h, 0, capi.fptr(xbuf), None, None, None, None, n_total, C.byref(nout)),
-                       "ckmpm_get_state", s2._h)
+            for i in range(len(models)):
+                capi.check(L.ckmpm_get_state(s2._h, i, capi.fptr(xbuf), None, None, None, None, n_total,
+                                             C.byref(nout)), "ckmpm_get_state", s2._h)
             exports += 1
     e1.record(stream)
     e1.synchronize()
@@ -290,7 +320,7 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jittered lattice, numpy PCG64 seed 0)",
-        "config": {"workload": WORKLOAD, "particles": n_live, "grid_blocks": grid_blocks, "dt": dt,
+        "config": {"workload": WORKLOADS[args.workload], "particles": n_live, "grid_blocks": grid_blocks, "dt": dt,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "particle state ~190 MB > 126 MB L2: no flush"},
         "roofline": roofline, "e2e": e2e, "clocks": clocks,
@@ -303,12 +333,12 @@ def run_reference(args, rank, world):
     """Reference arm: the reference CUDA build driven through its own MPMEngine API
     (oracle/_ref, built from the reference's headers) when present, otherwise the
     FP64 port of its algorithm on a bounded sample."""
-    from ckmpm_b200 import scenes
-    cfg, models = scenes.sand_column(track_ids=False)
-    harness = ROOT / "oracle" / "_ref" / "ref_sand"
-    if harness.exists():
+    cfg, models = workload(args.workload)
+    family = REFERENCE_FAMILY.get(args.workload)
+    harness = ROOT / "oracle" / "_ref" / f"ref_{family}"
+    if family and harness.exists() and len(models) == 1:
         from oracle import ref_runner
-        res = ref_runner.time_reference("sand", cfg, models, args.steps, args.warmup)
+        res = ref_runner.time_reference(family, cfg, models, args.steps, args.warmup)
         value = res["value"]
         cpu = {"value": value, "unit": METRIC, "cores": 1, "kind": "reference", "sample": res["sample"]}
     else:
@@ -318,7 +348,7 @@ def run_reference(args, rank, world):
     return {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded jittered lattice, numpy PCG64 seed 0)",
-            "config": {"workload": WORKLOAD, "particles": sum(len(m.particle_position) for m in models)},
+            "config": {"workload": WORKLOADS[args.workload], "particles": sum(len(m.particle_position) for m in models)},
             "impl": "reference", "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -329,8 +359,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.ncu_case:
-        from ckmpm_b200 import Scene, scenes
-        cfg, models = scenes.sand_column(track_ids=False)
+        from ckmpm_b200 import Scene
+        cfg, models = workload(args.workload)
         cfg.device = local_rank
         s = Scene(cfg)
         for m in models:
@@ -338,7 +368,8 @@ def main():
         s.setup()
         s.step(args.warmup, cfg.dt)
         s.step(args.steps, cfg.dt)
-        print(json.dumps({"ncu_case": WORKLOAD, "particles": s.count(0), "substeps": args.warmup + args.steps}))
+        print(json.dumps({"ncu_case": WORKLOADS[args.workload], "particles": s.count(0),
+                          "substeps": args.warmup + args.steps}))
         return
     if args.impl == "reference":
         if rank != 0:
@@ -352,8 +383,7 @@ def main():
     line = run_ours(args, rank, world, local_rank)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            from ckmpm_b200 import scenes
-            cfg, models = scenes.sand_column(track_ids=False)
+            cfg, models = workload(args.workload)
             line["cpu_baseline"] = cpu_baseline_oracle(cfg, models, args.cpu_seconds)
             line["cpu_pic_baseline"] = cpu_baseline_pic(min(args.cpu_seconds, 10.0))
         print(json.dumps(line), flush=True)

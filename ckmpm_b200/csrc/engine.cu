@@ -117,7 +117,14 @@ cudaError_t launch_compact(ckmpm_scene* s, const ModelHost& m, const BlockListDe
 }
 
 __global__ void set_next_dt_kernel(Scalars* scal, float dt) {
-  if (threadIdx.x == 0) scal->next_dt = dt;
+  if (threadIdx.x == 0) {
+    scal->next_dt = dt;
+    scal->next_dt_d = static_cast<double>(dt);
+  }
+}
+
+__global__ void set_frame_end_kernel(Scalars* scal, double frame_time) {
+  if (threadIdx.x == 0) scal->frame_end = scal->time + frame_time;
 }
 
 // Enqueue one substep for every model.  The compaction of each model writes
@@ -456,8 +463,45 @@ ckmpm_status ckmpm_step(ckmpm_scene* s, uint32_t nsteps, float dt) {
   return ckmpm_status_check(s);
 }
 
-ckmpm_status ckmpm_step_adaptive(ckmpm_scene* s, uint32_t, float, float, double, double*) {
-  return fail(s, CKMPM_ERR_INVALID, "adaptive stepping is not available in this build");
+ckmpm_status ckmpm_step_adaptive(ckmpm_scene* s, uint32_t nsteps, float dt_max, float cfl, double frame_time,
+                                 double* elapsed) {
+  if (!s || !s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  if (!(dt_max > 0.f) || !(cfl > 0.f) || !(frame_time > 0.0))
+    return fail(s, CKMPM_ERR_INVALID, "dt_max, cfl and frame_time must be positive");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  Scalars h{};
+  CK_CUDA(s, cudaMemcpyAsync(&h, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  const double t0 = h.time, t_end = h.time + frame_time;
+  set_frame_end_kernel<<<1, 32, 0, s->stream>>>(s->scal, frame_time);
+  const int maxv_ctas = s->sm_count * 8;
+  float mass_floor = 0.f;
+  for (const auto& m : s->models) mass_floor = (mass_floor == 0.f) ? m.mass : std::min(mass_floor, m.mass);
+  mass_floor *= 1.52587890625e-05f;  // 2^-16
+  uint32_t taken = 0;
+  // Each substep advances by at most dt_max, so floor(remaining / dt_max)
+  // substeps never pass the frame end; the last one is clipped to it on the
+  // device, as the reference's frame loop does (include/mpm_engine.cuh:514-552).
+  for (;;) {
+    const double remaining = t_end - h.time;
+    if (!(remaining > 0.0) || taken >= nsteps) break;
+    uint32_t k = static_cast<uint32_t>(remaining / static_cast<double>(dt_max));
+    k = std::max<uint32_t>(1u, std::min<uint32_t>(k, nsteps - taken));
+    for (uint32_t i = 0; i < k; ++i) {
+      const int parity = static_cast<int>(s->host_step & 1);
+      grid_maxv_kernel<<<maxv_ctas, 256, 0, s->stream>>>(s->sc, s->grid, s->scal, mass_floor);
+      adaptive_dt_kernel<<<1, 32, 0, s->stream>>>(s->scal, s->sc.dx, cfl, dt_max);
+      CK_CUDA(s, enqueue_substep(s, parity));
+      ++s->host_step;
+    }
+    taken += k;
+    CK_CUDA(s, cudaMemcpyAsync(&h, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
+    CK_CUDA(s, cudaStreamSynchronize(s->stream));
+    ckmpm_status st = status_from(s, h);
+    if (st != CKMPM_OK) return st;
+  }
+  if (elapsed) *elapsed = h.time - t0;
+  return CKMPM_OK;
 }
 
 ckmpm_status ckmpm_get_count(ckmpm_scene* s, int32_t model, uint32_t* n_live) {

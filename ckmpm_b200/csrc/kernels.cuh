@@ -65,10 +65,10 @@ struct Scalars {
   uint32_t window_skips;
   uint32_t timeouts;
   uint32_t maxv2_bits; // max |v|^2 on the grid (float bits), adaptive dt
-  double time;         // simulated time, adaptive dt
+  double time;         // simulated time: sum of the dt each substep advanced with
   double frame_end;    // adaptive dt: end of the current frame
-  float dt_max, cfl;   // adaptive dt parameters
-  uint32_t pad[2];
+  double cur_dt_d;     // cur_dt / next_dt in double, as the reference keeps its clock
+  double next_dt_d;
 };
 
 struct BlockListDev {
@@ -991,13 +991,68 @@ __global__ void __launch_bounds__(kCompactThreads)
   }
 }
 
-// Advance the substep counter and roll the dt pair (include/mpm_engine.cuh:869-871).
+// Advance the substep counter and roll the dt pair: currentDt = nextDt, then
+// the clock advances by it (include/mpm_engine.cuh:869-871).
 __global__ void end_substep_kernel(Scalars* scal) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     scal->step += 1;
-    scal->time += static_cast<double>(scal->cur_dt);
     scal->cur_dt = scal->next_dt;
+    scal->cur_dt_d = scal->next_dt_d;
+    scal->time += scal->cur_dt_d;
   }
+}
+
+// Adaptive dt, part 1: max |v|^2 over every grid node the next substep reads,
+// after the grid update with the current dt (include/mpm_algorithm.cuh:739-869,
+// the max-velocity query of UpdateGridVelocityAndQueryMax).  One warp per
+// domain block; blocks whose stamp is stale are empty.  NaN counts as +inf.
+// Nodes lighter than mass_floor are left out: the grid sums are fixed point
+// with 2^-36 of a particle mass as unit, so at a few units v = mv / m is a
+// ratio of two rounded small integers (e.g. 8/1 where the field moves at 6).
+// Such a node's weight in G2P is of the same 2^-36 order, so it never moves
+// a particle, but it would set the CFL bound.  The host passes
+// mass_floor = 2^-16 x the lightest particle mass (>= 2^20 units, v to ~1e-6).
+__global__ void grid_maxv_kernel(SceneDev sc, GridDev gd, Scalars* scal, float mass_floor) {
+  sc.mass_clamp = fmaxf(sc.mass_clamp, mass_floor);
+  const int32_t step = scal->step;
+  const int parity = step & 1;
+  const float* g = gd.grid[parity];
+  const int32_t* stamp = gd.stamp[parity];
+  const float dt = scal->cur_dt;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  float vmax2 = 0.f;
+  for (uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < sc.nblocks_domain; b += warps) {
+    if (stamp[b] != step) continue;
+    const int bz = static_cast<int>(b % sc.dims[2]);
+    const int by = static_cast<int>((b / sc.dims[2]) % sc.dims[1]);
+    const int bx = static_cast<int>(b / (static_cast<uint32_t>(sc.dims[2]) * sc.dims[1]));
+    for (int node = lane; node < 128; node += 32) {
+      const float4 v = node_velocity(sc, g + static_cast<int64_t>(b) * 512, node, bx, by, bz, by * 4 + ((node >> 2) & 3), dt);
+      float n2 = v.x * v.x + v.y * v.y + v.z * v.z;
+      if (isnan(n2)) n2 = __int_as_float(0x7f800000);
+      vmax2 = fmaxf(vmax2, n2);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) vmax2 = fmaxf(vmax2, __shfl_xor_sync(0xffffffffu, vmax2, o));
+  if (lane == 0 && vmax2 > 0.f) atomicMax(&scal->maxv2_bits, __float_as_uint(vmax2));
+}
+
+// Adaptive dt, part 2 (one thread): nextDt = min(dt_max, frame end - time,
+// dx * cfl / max|v|) (include/mpm_engine.cuh:552-557).  An infinite max|v|
+// is the reference's "velocity reached infinity" stop: status NUMERIC.
+__global__ void adaptive_dt_kernel(Scalars* scal, float dx, float cfl, float dt_max) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double next = fmin(static_cast<double>(dt_max), scal->frame_end - scal->time);
+  const float v2 = __uint_as_float(scal->maxv2_bits);
+  scal->maxv2_bits = 0u;
+  if (isinf(v2)) scal->status |= kStatusNumeric;
+  const float vmax = sqrtf(v2);
+  if (vmax > 0.f) next = fmin(next, static_cast<double>(dx * cfl / vmax));
+  if (next < 0.0) next = 0.0;
+  scal->next_dt_d = next;
+  scal->next_dt = static_cast<float>(next);
 }
 
 // ------------------------------------------------------------------ setup

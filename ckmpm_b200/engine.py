@@ -243,6 +243,13 @@ class Scene:
     def status_check(self) -> None:
         capi.check(capi.lib().ckmpm_status_check(self._h), "ckmpm_status_check", self._h)
 
+    def step_adaptive(self, max_steps: int, dt_max: float, cfl: float, frame_time: float) -> float:
+        """Advance one frame of frame_time with the reference's dt rule; returns the time advanced."""
+        el = C.c_double()
+        capi.check(capi.lib().ckmpm_step_adaptive(self._h, max_steps, dt_max, cfl, frame_time, C.byref(el)),
+                   "ckmpm_step_adaptive", self._h)
+        return el.value
+
     def step_profiled(self, nsteps: int, dt: float) -> tuple[float, float, int]:
         out = (C.c_double * 3)()
         capi.check(capi.lib().ckmpm_step_profiled(self._h, nsteps, dt, out), "ckmpm_step_profiled", self._h)
@@ -333,21 +340,44 @@ class MPMEngine:
         assert self.scene is not None
         self.scene.setup()
 
-    def Simulate(self, config: MPMConfig, export_callback=None, substeps_per_frame: int | None = None) -> int:
-        """Run GetTotalSimulatedFrameCount() frames at the fixed dt; returns substeps taken.
+    def ExportParticleToModel(self, export_root: str | Path, frame: int) -> list[Path]:
+        """Raw binary export as the reference writes it with exportParticlePositionAsBinary
+        (include/mpm_engine.cuh:433-444): float32 xyz triples per model in
+        <root>/model_<i>_particle_frame_<frame>.txt."""
+        assert self.scene is not None
+        root = Path(export_root)
+        root.mkdir(parents=True, exist_ok=True)
+        out = []
+        for i in range(len(self.scene.models)):
+            x = self.scene.state(i).x
+            f = root / f"model_{i}_particle_frame_{frame}.txt"
+            np.ascontiguousarray(x, np.float32).tofile(f)
+            out.append(f)
+        return out
 
-        export_callback(frame_index, scene) is called after every frame (the
-        reference's ExportParticleToModel point, include/mpm_engine.cuh:880-883).
+    def Simulate(self, config: MPMConfig, export_callback=None, fixed_substeps_per_frame: int | None = None,
+                 export_root: str | Path | None = None) -> int:
+        """Run GetTotalSimulatedFrameCount() frames; returns the substeps taken.
+
+        As the reference's Simulate (include/mpm_engine.cuh:457-909): every
+        substep takes nextDt = min(dt_, time left in the frame, dx cfl / max|v|)
+        on the device, the first substep advects with 0, and each frame ends
+        exactly on its boundary.  With fixed_substeps_per_frame every substep
+        uses dt_ instead.  export_callback(frame_index, scene) runs after every
+        frame (the reference's ExportParticleToModel point, :880-883).
         """
         assert self.scene is not None
-        spf = substeps_per_frame or max(1, int(round((1.0 / config.GetFps()) / self.dt_)))
-        total = 0
+        start = self.scene.counters()["steps"]
         for frame in range(config.GetTotalSimulatedFrameCount()):
-            self.scene.step(spf, self.dt_)
-            total += spf
+            if fixed_substeps_per_frame:
+                self.scene.step(fixed_substeps_per_frame, self.dt_)
+            else:
+                self.scene.step_adaptive(1 << 30, self.dt_, config.GetCfl(), 1.0 / config.GetFps())
+            if export_root is not None:
+                self.ExportParticleToModel(export_root, frame)
             if export_callback is not None:
                 export_callback(frame, self.scene)
-        return total
+        return self.scene.counters()["steps"] - start
 
 
 def load_scene_json(path: str | Path) -> tuple[MPMConfig, list[MPMModel]]:

@@ -175,17 +175,18 @@ class MPMEngine {
 
   void InitialSetup(const MPMConfig&) { check(ckmpm_setup(scene_), scene_, "ckmpm_setup"); }
 
-  // Simulate: GetTotalSimulatedFrameCount() frames of round((1/fps)/dt)
-  // substeps at the fixed dt; export(frame, engine) runs after every frame
-  // (the reference's ExportParticleToModel point, include/mpm_engine.cuh:880-883).
-  // Returns the number of substeps taken instead of ending the process.
-  uint64_t Simulate(const MPMConfig& config, const std::function<void(uint32_t, MPMEngine&)>& exportFrame = {}) {
-    const uint32_t perFrame = std::max<uint32_t>(
-        1u, static_cast<uint32_t>(std::lround((1.0 / config.GetFps()) / static_cast<double>(dt_))));
-    uint64_t total = 0;
+  // Simulate: GetTotalSimulatedFrameCount() frames; every substep takes
+  // nextDt = min(dt_, time left in the frame, dx cfl / max|v|) on the device
+  // (include/mpm_engine.cuh:514-557); export(frame, engine) runs after every
+  // frame (the ExportParticleToModel point, :880-883).  Returns the simulated
+  // time instead of ending the process.
+  double Simulate(const MPMConfig& config, const std::function<void(uint32_t, MPMEngine&)>& exportFrame = {}) {
+    double total = 0.0;
     for (uint32_t f = 0; f < config.GetTotalSimulatedFrameCount(); ++f) {
-      check(ckmpm_step(scene_, perFrame, dt_), scene_, "ckmpm_step");
-      total += perFrame;
+      double elapsed = 0.0;
+      check(ckmpm_step_adaptive(scene_, 1u << 30, dt_, config.GetCfl(), 1.0 / config.GetFps(), &elapsed), scene_,
+            "ckmpm_step_adaptive");
+      total += elapsed;
       if (exportFrame) exportFrame(f, *this);
     }
     return total;

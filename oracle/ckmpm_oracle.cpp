@@ -72,6 +72,7 @@ struct Scene {
   double current_dt = 0.0;
   int64_t steps = 0;
   int64_t lost = 0, window_skips = 0;
+  std::vector<double> dt_log;
 };
 
 inline int64_t flat_key(const Scene& s, int bx, int by, int bz) {
@@ -556,6 +557,48 @@ int oracle_setup(void* h) {
   s->current_dt = 0.0;
   s->steps = 0;
   return 0;
+}
+
+// One frame with the reference's adaptive rule (include/mpm_engine.cuh:514-557):
+// every substep takes next = min(dt_max, frame end - time, dx cfl / max|v|),
+// max|v| over all grid nodes after the grid update with the current dt.
+// Returns the number of substeps taken.
+int oracle_step_frame(void* h, double dt_max, double cfl, double frame_time, double* time) {
+  Scene* s = static_cast<Scene*>(h);
+  const double end = *time + frame_time;
+  int taken = 0;
+  while (*time < end) {
+    double vmax2 = 0.0;
+    for (auto& kv : s->grid) {
+      const int64_t k = kv.first;
+      const int bz = static_cast<int>(k % s->d.dims[2]);
+      const int by = static_cast<int>((k / s->d.dims[2]) % s->d.dims[1]);
+      const int bx = static_cast<int>(k / (static_cast<int64_t>(s->d.dims[2]) * s->d.dims[1]));
+      for (int gi = 0; gi < 2; ++gi)
+        for (int cell = 0; cell < 64; ++cell) {
+          const int c[3] = {bx * 4 + (cell >> 4), by * 4 + ((cell >> 2) & 3), bz * 4 + (cell & 3)};
+          double v[3];
+          node_velocity(*s, gi, c, s->current_dt, v);
+          vmax2 = std::max(vmax2, v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        }
+    }
+    double next = std::min(dt_max, end - *time);
+    const double vmax = std::sqrt(vmax2);
+    if (vmax > 0.0) next = std::min(next, s->d.dx * cfl / vmax);
+    substep(*s, next);
+    *time += next;
+    ++taken;
+    s->dt_log.push_back(next);
+  }
+  return taken;
+}
+
+// The dt of every adaptive substep taken so far (up to cap entries); returns the count.
+int oracle_dt_log(void* h, double* out, int cap) {
+  Scene* s = static_cast<Scene*>(h);
+  const int n = static_cast<int>(s->dt_log.size());
+  for (int i = 0; i < n && i < cap; ++i) out[i] = s->dt_log[i];
+  return n;
 }
 
 int oracle_step(void* h, int nsteps, double dt) {

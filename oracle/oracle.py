@@ -36,6 +36,7 @@ def lib() -> C.CDLL:
         L.oracle_add_model.argtypes = [C.c_void_p, C.c_int, d, C.c_int, f, f, C.c_int, C.c_double, C.c_double]
         L.oracle_setup.argtypes = [C.c_void_p]
         L.oracle_step.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.oracle_step_frame.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]
         L.oracle_get_state.argtypes = [C.c_void_p, C.c_int, d, d, d, d, C.POINTER(C.c_uint8)]
         L.oracle_set_state.argtypes = [C.c_void_p, C.c_int, d, d, d]
         L.oracle_counter.argtypes = [C.c_void_p, C.c_int]
@@ -88,6 +89,13 @@ class OracleScene:
 
     def step(self, nsteps: int, dt: float):
         lib().oracle_step(self._h, nsteps, dt)
+
+    def step_frame(self, dt_max: float, cfl: float, frame_time: float) -> int:
+        """One frame with the reference's adaptive dt rule; returns the substeps taken."""
+        t = C.c_double(getattr(self, "_time", 0.0))
+        k = lib().oracle_step_frame(self._h, dt_max, cfl, frame_time, C.byref(t))
+        self._time = t.value
+        return k
 
     def state(self, model: int = 0):
         n = self.n[model]

@@ -45,6 +45,17 @@ def golden_scenes():
     yield "sand_dp", "slip", cfg, m[0]
 
 
+# Adaptive-dt fixture: the reference's own Simulate picks every dt (CFL on the
+# grid's max |v| binds, and each frame ends on a clipped substep).
+ADAPTIVE = {"name": "jelly_adaptive", "family": "jelly", "dt": 2e-3, "fps": 48, "frames": 2}
+
+
+def adaptive_scene():
+    cfg, m = scenes.jelly_cube(lo=(0.44, 0.44, 0.44), hi=(0.56, 0.56, 0.56), v0=(6.0, 0.0, 0.0), E=2e4, gravity=-9.8)
+    cfg.dt, cfg.fps, cfg.total_frames, cfg.cfl = ADAPTIVE["dt"], ADAPTIVE["fps"], ADAPTIVE["frames"], 0.5
+    return cfg, m[0]
+
+
 def checksum(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()[:16]
 
@@ -72,6 +83,19 @@ def main(outdir: str) -> None:
                       "mass": model.particle_mass, "volume": model.particle_volume,
                       "counts": [int(len(runs[0][k])) for k in range(FRAMES)]}
         print(name, meta[name]["n"], "spread", max(spread), flush=True)
+    cfg, model = adaptive_scene()
+    a = ADAPTIVE
+    runs = []
+    for _ in range(2):
+        text, d = ref_runner.run(a["family"], model, a["fps"], a["frames"], a["dt"], 0)
+        runs.append(ref_runner.frames_out(d, a["frames"]))
+    spread = [float(ref_runner.match_nn(runs[0][k], runs[1][k])[1].max()) for k in range(a["frames"])]
+    np.savez_compressed(out / f"{a['name']}.npz", **{f"frame{k}": runs[0][k] for k in range(a["frames"])})
+    meta[a["name"]] = {"family": a["family"], "n": int(len(model.particle_position)),
+                       "input_sha": checksum(model.particle_position), "dt": a["dt"], "fps": a["fps"],
+                       "frames": a["frames"], "kept_frames": list(range(a["frames"])), "adaptive": True,
+                       "reference_run_to_run_spread": spread, "counts": [int(len(r)) for r in runs[0]]}
+    print(a["name"], meta[a["name"]]["n"], "spread", max(spread), flush=True)
     (out / "golden.json").write_text(json.dumps(meta, indent=1))
 
 

@@ -42,7 +42,9 @@ def tolerance(name: str, nsub: int) -> float:
 def nn_error(x: np.ndarray, ref: np.ndarray) -> float:
     from oracle import ref_runner
     i, d = ref_runner.match_nn(x, ref)
-    assert len(set(i.tolist())) == len(ref), "nearest-neighbour matching is not one-to-one"
+    assert len(set(i.tolist())) == len(ref), (
+        f"nearest-neighbour matching is not one-to-one (max distance {d.max():.3e}, "
+        f"mean offset {(ref[i] - x).mean(axis=0)})")
     return float(d.max())
 
 
@@ -55,6 +57,33 @@ def test_fixtures_match_the_seeded_inputs():
         assert m["n"] == len(model.particle_position)
         spread = max(m["reference_run_to_run_spread"])
         assert spread <= tolerance(name, 128), (name, spread)
+
+
+def adaptive_dt(cfg, model) -> float:
+    """dt_ of the reference's Initialize + InitializeParticle (include/mpm_engine.cuh:109-117,178)."""
+    dt = np.float32(min(np.float32(cfg.dt), np.float32(1.0) / np.float32(cfg.fps)))
+    vmax = float(np.max(np.linalg.norm(model.particle_velocity.astype(np.float64), axis=1)))
+    if vmax > 0:
+        dt = min(dt, np.float32(cfg.dx * cfg.cfl / vmax))
+    return float(dt)
+
+
+def test_oracle_matches_reference_adaptive(oracle_mod):
+    _, mg = golden_cases()
+    meta = load_meta()["jelly_adaptive"]
+    cfg, model = mg.adaptive_scene()
+    assert meta["input_sha"] == mg.checksum(model.particle_position)
+    fx = np.load(GOLDEN / "jelly_adaptive.npz")
+    o = oracle_mod.OracleScene(cfg, [model])
+    o.setup()
+    dt = adaptive_dt(cfg, model)
+    total = 0
+    for k in meta["kept_frames"]:
+        total += o.step_frame(dt, cfg.cfl, 1.0 / cfg.fps)
+        x = o.state(0)["x"]
+        err = nn_error(x, fx[f"frame{k}"])
+        print(f"jelly_adaptive frame {k} ({total} substeps): oracle vs reference {err:.3e}")
+        assert err <= tolerance("jelly_adaptive", total), (k, err)
 
 
 def test_oracle_matches_reference_build(oracle_mod):

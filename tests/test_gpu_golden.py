@@ -43,3 +43,25 @@ def test_engine_matches_reference_build(engine_lib):
             print(f"{name} frame {k} ({target} substeps): engine vs reference {err:.3e}")
             assert err <= tolerance(name, target), (name, k, err)
         s.close()
+
+
+def test_engine_simulate_matches_reference_adaptive(engine_lib):
+    """The reference-shaped MPMEngine.Simulate (adaptive CFL dt, frame clipping)
+    against the reference's own Simulate on the same scene."""
+    sys.path.insert(0, str(GOLDEN))
+    import make_golden
+    from test_golden import nn_error, tolerance
+    from ckmpm_b200 import MPMEngine
+    meta = json.loads((GOLDEN / "golden.json").read_text())["jelly_adaptive"]
+    cfg, model = make_golden.adaptive_scene()
+    fx = np.load(GOLDEN / "jelly_adaptive.npz")
+    frames = {}
+    eng = MPMEngine()
+    eng.Initialize(cfg)
+    eng.InitializeParticle(cfg, [model])
+    eng.InitialSetup(cfg)
+    n = eng.Simulate(cfg, export_callback=lambda f, scene: frames.__setitem__(f, scene.state(0).x.copy()))
+    for k in meta["kept_frames"]:
+        err = nn_error(frames[k], fx[f"frame{k}"])
+        print(f"jelly_adaptive frame {k}: engine vs reference {err:.3e} ({n} substeps in total)")
+        assert err <= tolerance("jelly_adaptive", n), (k, err)
