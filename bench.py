@@ -39,8 +39,10 @@ WORKLOADS = {
                   "dt=1e-4, sticky walls",
     "dam_break_mixed": "dam_break_mixed: j-fluid block + 64 fixed-corotated spheres, dx=1/512 (128^3 blocks), 8 ppc, "
                        "dt=2e-5, sticky walls",
+    "batched_256": "batched_256: 256 independent scenes, dx=1/64 (16^3 blocks each), 2k-200k particles log-uniform, "
+                   "fixed-corotated/j-fluid/drucker-prager, box or sphere, v0~U(-1,1)^3, 8 ppc, dt=1e-4, sticky walls",
 }
-REFERENCE_FAMILY = {"sand_column": "sand", "jelly_cube": "jelly"}
+REFERENCE_FAMILY = {"sand_column": "sand", "jelly_cube": "jelly", "dam_break_mixed": "dam", "batched_256": "jelly"}
 STATE_BYTES = {0: 48, 2: 52, 3: 16}  # x + F (+ logJp) or x + J, read once and written once per substep
 
 
@@ -183,6 +185,33 @@ def cpu_baseline_oracle(cfg, models, seconds: float, max_particles: int = 2_000_
                       f"after one untimed substep, {t:.1f} s"}
 
 
+def cpu_baseline_batched(cfg, models, seconds: float) -> dict:
+    """FP64 oracle on a sample of the batch: one scene of each material (the
+    first in scene order), run one after another; aggregate rate."""
+    from oracle import oracle as O
+    picked = {}
+    for m in models:
+        picked.setdefault(m.material.kind, m)
+    work, secs, kdone = 0, 0.0, []
+    for m in picked.values():
+        o = O.OracleScene(cfg, [m])
+        o.setup()
+        o.step(1, cfg.dt)
+        t0 = time.perf_counter()
+        o.step(1, cfg.dt)
+        t1 = time.perf_counter() - t0
+        k = int(max(1, min(64, seconds / len(picked) / max(t1, 1e-6))))
+        t0 = time.perf_counter()
+        o.step(k, cfg.dt)
+        secs += time.perf_counter() - t0
+        work += len(m.particle_position) * k
+        kdone.append(f"{m.material.kind} {len(m.particle_position)} particles x {k} substeps")
+        o.close()
+    return {"value": work / secs, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": "FP64 serial oracle (oracle/ckmpm_oracle.cpp), one scene per material from the batch: "
+                      + "; ".join(kdone)}
+
+
 def cpu_baseline_pic(seconds: float) -> dict:
     """python-src PIC demo restated in C++/OpenMP on the jelly cube, all host threads."""
     import ctypes as C
@@ -214,7 +243,141 @@ def cpu_baseline_pic(seconds: float) -> dict:
 # ---------------------------------------------------------------- our arm
 def workload(name: str):
     from ckmpm_b200 import scenes
+    if name == "batched_256":
+        return scenes.batched_scenes()
     return scenes.WORKLOADS[name](track_ids=False)
+
+
+def run_batched(args, rank, world, local_rank):
+    """Batched form: this rank's shard of the 256 scenes in one SceneBatch
+    (one persistent fused launch + rebinning per substep, CUDA graphs), launch
+    shape from the autotuner; beside it, at N = 1, the same scenes looped
+    through the plain single-scene path on one stream."""
+    import torch
+
+    from ckmpm_b200 import Scene
+    from ckmpm_b200.batch import SceneBatch, reduce_over_ranks, shard_scenes
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.Stream()
+    cfg, models = workload(args.workload)
+    cfg.device = local_rank
+    dt = cfg.dt
+    counts = [len(m.particle_position) for m in models]
+    mine = shard_scenes(counts, world)[rank]
+    sub = [models[i] for i in mine]
+
+    b = SceneBatch(cfg, sub)
+    b.set_stream(stream.cuda_stream)
+    b.setup()
+    best, tried = b.autotune(16, dt)
+    b.step(args.warmup, dt)
+    n_live = b.count(0)
+    sampler = ClockSampler(device_uuid(local_rank))
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    b.step_async(args.steps, dt)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    b.status_check()
+    ms = ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    ms, total_live = reduce_over_ranks(ms, float(n_live))
+    value = total_live * args.steps / (ms / 1e3)
+
+    fused_ms, other_ms, launches = b.step_profiled(min(args.profile_steps, 100), dt)
+    avg_fused = fused_ms / max(launches, 1)
+    grid_blocks = sum(len(b.blocks_in(i, 1)[0]) for i in range(len(sub)))
+    st = b.state()
+    kinds = np.array([m.material.kind_code for m in sub])[b.scene_of(st.id)]
+    alg_bytes = 7168 * grid_blocks + sum(int((kinds == k).sum()) * (2 * STATE_BYTES[k] + 8) for k in STATE_BYTES)
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / (avg_fused / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "g2p2g_kernel<kMixed> (all scenes of the shard in one launch)",
+                "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_fused,
+                "peak_source": f"{peak_kind} hbm_gbs", "fused_share": fused_ms / max(fused_ms + other_ms, 1e-9)}
+    b.close()
+
+    looped = None
+    if world == 1:
+        # The plain path over the same scenes, one after another on one stream.
+        loop_steps = min(args.steps, 64)
+        plain = []
+        for m in sub:
+            s = Scene(cfg)
+            s.set_stream(stream.cuda_stream)
+            s.add_model(m)
+            s.setup()
+            s.step(8, dt)
+            plain.append(s)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for s in plain:
+            s.step_async(loop_steps, dt)
+        ev1.record(stream)
+        ev1.synchronize()
+        lms = ev0.elapsed_time(ev1)
+        n_plain = 0
+        for s in plain:
+            s.status_check()
+            n_plain += s.count(0)
+            s.close()
+        lv = n_plain * loop_steps / (lms / 1e3)
+        looped = {"value": lv, "unit": METRIC, "steps": loop_steps, "ms_per_step": lms / loop_steps,
+                  "speedup_of_batched": value / lv,
+                  "how": "each scene through ckmpm_create/ckmpm_step_async (graphs of 8 substeps), scenes in turn "
+                         "on one stream, device time of the whole loop"}
+
+    # End to end through the public API with host buffers.
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b2 = SceneBatch(cfg, sub)
+    b2.set_stream(stream.cuda_stream)
+    b2.setup()
+    exports = 0
+    for k in range(args.steps):
+        b2.step(1, dt)
+        if (k + 1) % args.e2e_frame == 0:
+            b2.state()
+            exports += 1
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms, _ = reduce_over_ranks(e0.elapsed_time(e1), 0.0)
+    b2.close()
+    n_in = sum(len(m.particle_position) for m in sub)
+    e2e = {"value": total_live * args.steps / (e2e_ms / 1e3), "unit": METRIC,
+           "h2d_bytes_per_step": n_in * 24 / args.steps,
+           "d2h_bytes_per_step": 64 + exports * n_live * (12 + 12 + 36 + 4 + 4) / args.steps,
+           "includes": "batch construction and setup (upload of x, v; binning; initial grid), every substep's "
+                       f"status read, a full state export every {args.e2e_frame} substeps"}
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes, numpy PCG64 seed 0)",
+        "config": {"workload": WORKLOADS[args.workload], "scenes": len(models), "scenes_this_rank": len(sub),
+                   "particles": int(total_live), "grid_blocks_rank0": grid_blocks, "dt": dt,
+                   "parallelism": f"scenes sharded over {world} GPUs (longest-first bin-pack), no collective"
+                   if world > 1 else "single GPU",
+                   "tuning": best, "tuning_candidates": len(tried),
+                   "l2": "particle state ~560 MB > 126 MB L2: no flush"},
+        "roofline": roofline, "e2e": e2e, "clocks": clocks,
+        "gpu_launches": 1 + args.steps * 4,
+    }
+    if looped:
+        line["looped_plain"] = looped
+    return line
 
 
 def run_ours(args, rank, world, local_rank):
@@ -336,7 +499,21 @@ def run_reference(args, rank, world):
     cfg, models = workload(args.workload)
     family = REFERENCE_FAMILY.get(args.workload)
     harness = ROOT / "oracle" / "_ref" / f"ref_{family}"
-    if family and harness.exists() and len(models) == 1:
+    if family and harness.exists() and args.workload == "batched_256":
+        # The reference runs one scene per process: loop it over every 8th scene.
+        from oracle import ref_runner
+        work, secs = 0, 0.0
+        sample = models[::8]
+        for m in sample:
+            r = ref_runner.time_reference(family, cfg, [m], args.steps, args.warmup)
+            work += r["particles"] * r["substeps"]
+            secs += r["seconds"]
+        value = work / secs
+        cpu = {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
+               "sample": f"reference CUDA build (oracle/_ref/ref_{family}) via MPMEngine::Simulate in profile mode, "
+                         f"one process per scene, every 8th scene ({len(sample)} of {len(models)}), "
+                         f"{args.warmup + args.steps} substeps each; host timer around each frame loop, summed"}
+    elif family and harness.exists():
         from oracle import ref_runner
         res = ref_runner.time_reference(family, cfg, models, args.steps, args.warmup)
         value = res["value"]
@@ -380,11 +557,17 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    line = run_ours(args, rank, world, local_rank)
+    if args.workload == "batched_256":
+        line = run_batched(args, rank, world, local_rank)
+    else:
+        line = run_ours(args, rank, world, local_rank)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             cfg, models = workload(args.workload)
-            line["cpu_baseline"] = cpu_baseline_oracle(cfg, models, args.cpu_seconds)
+            if args.workload == "batched_256":
+                line["cpu_baseline"] = cpu_baseline_batched(cfg, models, args.cpu_seconds)
+            else:
+                line["cpu_baseline"] = cpu_baseline_oracle(cfg, models, args.cpu_seconds)
             line["cpu_pic_baseline"] = cpu_baseline_pic(min(args.cpu_seconds, 10.0))
         print(json.dumps(line), flush=True)
     if world > 1:

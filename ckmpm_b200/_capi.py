@@ -39,8 +39,12 @@ EXPORTED = (
     "ckmpm_status_check", "ckmpm_step_adaptive", "ckmpm_set_stream", "ckmpm_get_count",
     "ckmpm_get_state", "ckmpm_get_blocks", "ckmpm_get_counters", "ckmpm_get_dt",
     "ckmpm_step_profiled", "ckmpm_debug_constitutive", "ckmpm_destroy", "ckmpm_last_error",
-    "ckmpm_version", "ckmpm_simulate_noalloc",
+    "ckmpm_version", "ckmpm_simulate_noalloc", "ckmpm_create_batch", "ckmpm_add_batch", "ckmpm_get_blocks_in",
+    "ckmpm_set_tuning", "ckmpm_get_tuning", "ckmpm_autotune", "ckmpm_checkpoint_bytes", "ckmpm_checkpoint_save",
+    "ckmpm_checkpoint_restore",
 )
+
+MAX_BATCH_SCENES = 65536
 
 
 class SceneDesc(C.Structure):
@@ -59,6 +63,19 @@ class SceneDesc(C.Structure):
 
 class Material(C.Structure):
     _fields_ = [("kind", C.c_int32), ("p", C.c_float * 4)]
+
+
+class BatchScene(C.Structure):
+    _fields_ = [("material", Material), ("mass", C.c_float), ("volume", C.c_float), ("n", C.c_uint32)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("threads", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("graph_chunk", C.c_uint32),
+                ("probe_ms", C.c_float)]
+
+    def as_dict(self) -> dict:
+        return {"threads": int(self.threads), "ctas_per_sm": int(self.ctas_per_sm),
+                "graph_chunk": int(self.graph_chunk), "probe_ms": float(self.probe_ms)}
 
 
 class CkmpmError(RuntimeError):
@@ -103,6 +120,16 @@ def lib() -> C.CDLL:
         L.ckmpm_simulate_noalloc.argtypes = [C.POINTER(SceneDesc), C.POINTER(Material), C.c_uint32, P, P, C.c_uint32,
                                              C.c_float, C.c_float, C.c_uint32, C.c_float, P, P, P, P, P,
                                              C.POINTER(C.c_uint32), C.POINTER(C.c_char_p)]
+        L.ckmpm_create_batch.argtypes = [C.POINTER(SceneDesc), C.c_uint32, C.POINTER(P)]
+        L.ckmpm_add_batch.argtypes = [P, C.c_uint32, C.POINTER(BatchScene), f32p, f32p]
+        L.ckmpm_get_blocks_in.argtypes = [P, C.c_uint32, C.c_int32, C.c_int32, i32p, u32p, C.c_uint32, u32p]
+        L.ckmpm_set_tuning.argtypes = [P, C.POINTER(Tuning)]
+        L.ckmpm_get_tuning.argtypes = [P, C.POINTER(Tuning), u32p]
+        L.ckmpm_autotune.argtypes = [P, C.c_uint32, C.c_float, C.POINTER(Tuning), C.c_uint32, u32p,
+                                     C.POINTER(Tuning)]
+        L.ckmpm_checkpoint_bytes.argtypes = [P, C.POINTER(C.c_uint64)]
+        L.ckmpm_checkpoint_save.argtypes = [P, P]
+        L.ckmpm_checkpoint_restore.argtypes = [P, P]
         L.ckmpm_destroy.argtypes = [P]
         L.ckmpm_last_error.argtypes = [P]
         L.ckmpm_last_error.restype = C.c_char_p

@@ -20,7 +20,9 @@ namespace {
 constexpr int kFusedThreads = 256;
 constexpr int kProbeThreads = 256;
 constexpr int kGraphChunk = 8;
-constexpr const char* kVersion = "ckmpm-b200 0.1.0";
+constexpr int kMaxGraphChunk = 64;
+constexpr int kMixedKind = 7;  // ModelHost::mat.kind of a batch's single model (per-scene materials)
+constexpr const char* kVersion = "ckmpm-b200 0.2.0";
 
 thread_local std::string g_create_error;
 
@@ -41,6 +43,10 @@ struct ModelHost {
   uint32_t* oid = nullptr;
   std::vector<float> hx, hv, hF, ha;
   std::vector<uint32_t> hid;
+  // Batch: per-scene materials and input offsets (host copies and device arrays).
+  std::vector<SceneMat> smat;
+  std::vector<uint32_t> sstart;
+  std::vector<int32_t> skind;
 };
 
 }  // namespace
@@ -57,7 +63,13 @@ struct ckmpm_scene {
   std::string err;
   int sm_count = 0;
   int fused_ctas = 0;
-  std::vector<void*> allocs;
+  int occ[2] = {0, 0};     // resident fused CTAs per SM at 128 / 256 threads
+  uint32_t nstack = 1;     // stacked domains: 1, or the scene count of a batch
+  ckmpm_tuning tune{};
+  // Every device allocation with its size; the first n_state_allocs hold the
+  // simulation state (what a checkpoint copies), later ones are export buffers.
+  std::vector<std::pair<void*, size_t>> allocs;
+  size_t n_state_allocs = 0;
   cudaGraphExec_t graph_chunk = nullptr;
   cudaGraphExec_t graph_one = nullptr;
   uint64_t host_step = 0;
@@ -81,8 +93,9 @@ ckmpm_status fail(ckmpm_scene* s, ckmpm_status code, const std::string& msg) {
 template <typename T>
 cudaError_t dalloc(ckmpm_scene* s, T** p, size_t count) {
   void* q = nullptr;
-  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
-  if (e == cudaSuccess) s->allocs.push_back(q);
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e == cudaSuccess) s->allocs.emplace_back(q, bytes);
   *p = static_cast<T*>(q);
   return e;
 }
@@ -93,19 +106,45 @@ void free_graphs(ckmpm_scene* s) {
   s->graph_chunk = s->graph_one = nullptr;
 }
 
-template <int KIND>
+template <int KIND, int NT>
 cudaError_t launch_fused(ckmpm_scene* s, const ModelHost& m) {
-  g2p2g_kernel<KIND, kFusedThreads><<<s->fused_ctas, kFusedThreads, kSmemFused, s->stream>>>(s->sc, m.dev, s->grid,
-                                                                                             s->scal);
+  g2p2g_kernel<KIND, NT><<<s->fused_ctas, NT, kSmemFused, s->stream>>>(s->sc, m.dev, s->grid, s->scal);
   return cudaGetLastError();
 }
 
-cudaError_t launch_fused_any(ckmpm_scene* s, const ModelHost& m) {
+template <int NT>
+cudaError_t launch_fused_nt(ckmpm_scene* s, const ModelHost& m) {
   switch (m.mat.kind) {
-    case CKMPM_FIXED_COROTATED: return launch_fused<kFixedCorotated>(s, m);
-    case CKMPM_DRUCKER_PRAGER: return launch_fused<kDruckerPrager>(s, m);
-    default: return launch_fused<kFluid>(s, m);
+    case CKMPM_FIXED_COROTATED: return launch_fused<kFixedCorotated, NT>(s, m);
+    case CKMPM_DRUCKER_PRAGER: return launch_fused<kDruckerPrager, NT>(s, m);
+    case kMixedKind: return launch_fused<kMixed, NT>(s, m);
+    default: return launch_fused<kFluid, NT>(s, m);
   }
+}
+
+cudaError_t launch_fused_any(ckmpm_scene* s, const ModelHost& m) {
+  return s->tune.threads == 128 ? launch_fused_nt<128>(s, m) : launch_fused_nt<256>(s, m);
+}
+
+template <int NT>
+cudaError_t set_fused_attributes(int* occ) {
+  const void* fns[4] = {reinterpret_cast<const void*>(g2p2g_kernel<kFixedCorotated, NT>),
+                        reinterpret_cast<const void*>(g2p2g_kernel<kDruckerPrager, NT>),
+                        reinterpret_cast<const void*>(g2p2g_kernel<kFluid, NT>),
+                        reinterpret_cast<const void*>(g2p2g_kernel<kMixed, NT>)};
+  int lowest = 1 << 30;
+  for (const void* fn : fns) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemFused));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    int o = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, NT, kSmemFused);
+    if (e != cudaSuccess) return e;
+    lowest = std::min(lowest, o);
+  }
+  *occ = std::max(1, lowest);
+  return cudaSuccess;
 }
 
 // Compaction of one model's next block list into list `out`.
@@ -171,23 +210,16 @@ ckmpm_status status_from(ckmpm_scene* s, const Scalars& h) {
   return CKMPM_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-const char* ckmpm_version(void) { return kVersion; }
-
-const char* ckmpm_last_error(const ckmpm_scene* s) { return s ? s->err.c_str() : g_create_error.c_str(); }
-
-ckmpm_status ckmpm_create(const ckmpm_scene_desc* desc, ckmpm_scene** out) {
+ckmpm_status create_impl(const ckmpm_scene_desc* desc, uint32_t nstack, ckmpm_scene** out) {
   if (!desc || !out) return fail(nullptr, CKMPM_ERR_INVALID, "null argument");
   *out = nullptr;
+  if (nstack < 1 || nstack > CKMPM_MAX_BATCH_SCENES) return fail(nullptr, CKMPM_ERR_INVALID, "scene count out of range");
   if (!(desc->dx > 0.f)) return fail(nullptr, CKMPM_ERR_INVALID, "dx must be positive");
   for (int a = 0; a < 3; ++a)
     if (desc->domain_blocks[a] < 1 || desc->domain_blocks[a] > 4096)
       return fail(nullptr, CKMPM_ERR_INVALID, "domain_blocks out of range");
   const uint64_t nbd = static_cast<uint64_t>(desc->domain_blocks[0]) * desc->domain_blocks[1] * desc->domain_blocks[2];
-  if (nbd > (1ull << 28)) return fail(nullptr, CKMPM_ERR_INVALID, "domain too large for the dense block table");
+  if (nbd * nstack > (1ull << 28)) return fail(nullptr, CKMPM_ERR_INVALID, "domain too large for the dense block table");
   if (desc->boundary != CKMPM_BOUNDARY_STICKY_BLOCKS && desc->boundary != CKMPM_BOUNDARY_SLIP_FLOOR)
     return fail(nullptr, CKMPM_ERR_INVALID, "unknown boundary kind");
   if (desc->max_particles_per_block > static_cast<uint32_t>(kMaxParticlesPerBlock))
@@ -199,6 +231,7 @@ ckmpm_status ckmpm_create(const ckmpm_scene_desc* desc, ckmpm_scene** out) {
 
   ckmpm_scene* s = new ckmpm_scene();
   s->desc = *desc;
+  s->nstack = nstack;
   if (s->desc.max_particles_per_block == 0) s->desc.max_particles_per_block = kMaxParticlesPerBlock;
   auto bail = [&](ckmpm_status st) {
     g_create_error = s->err;
@@ -219,49 +252,169 @@ ckmpm_status ckmpm_create(const ckmpm_scene_desc* desc, ckmpm_scene** out) {
   sc.mass_clamp = desc->mass_clamp;
   sc.boundary = desc->boundary;
   sc.floor_cells = desc->floor_cells;
-  sc.nblocks_domain = static_cast<uint32_t>(nbd);
-  uint32_t base = 0;
-  for (int c = 0; c < 8; ++c) {
-    const int par[3] = {(c >> 2) & 1, (c >> 1) & 1, c & 1};
-    for (int a = 0; a < 3; ++a) sc.cdims[c][a] = (sc.dims[a] - par[a] + 1) / 2;
-    sc.cbase[c] = base;
-    base += static_cast<uint32_t>(sc.cdims[c][0]) * sc.cdims[c][1] * sc.cdims[c][2];
-  }
-  sc.cbase[8] = base;
+  init_colour_classes(sc, nstack);
+  const uint64_t nbt = sc.nblocks_domain;
 
   // Dense grids and stamps.
   for (int b = 0; b < 2; ++b) {
-    if (dalloc(s, &s->grid.grid[b], static_cast<size_t>(nbd) * 512) != cudaSuccess ||
-        dalloc(s, &s->grid.stamp[b], nbd) != cudaSuccess)
+    if (dalloc(s, &s->grid.grid[b], static_cast<size_t>(nbt) * 512) != cudaSuccess ||
+        dalloc(s, &s->grid.stamp[b], nbt) != cudaSuccess)
       return bail(fail(s, CKMPM_ERR_CUDA, "grid allocation failed"));
-    cudaMemsetAsync(s->grid.stamp[b], 0xFF, sizeof(int32_t) * nbd, s->stream);
+    cudaMemsetAsync(s->grid.stamp[b], 0xFF, sizeof(int32_t) * nbt, s->stream);
   }
   if (dalloc(s, &s->scal, 1) != cudaSuccess) return bail(fail(s, CKMPM_ERR_CUDA, "scalar allocation failed"));
   cudaMemsetAsync(s->scal, 0, sizeof(Scalars), s->stream);
 
-  auto set_attr = [&](const void* fn) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemFused));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-  };
-  if (set_attr(reinterpret_cast<const void*>(g2p2g_kernel<kFixedCorotated, kFusedThreads>)) != cudaSuccess ||
-      set_attr(reinterpret_cast<const void*>(g2p2g_kernel<kDruckerPrager, kFusedThreads>)) != cudaSuccess ||
-      set_attr(reinterpret_cast<const void*>(g2p2g_kernel<kFluid, kFusedThreads>)) != cudaSuccess ||
-      set_attr(reinterpret_cast<const void*>(rasterize_kernel<kFusedThreads>)) != cudaSuccess)
+  if (set_fused_attributes<128>(&s->occ[0]) != cudaSuccess || set_fused_attributes<256>(&s->occ[1]) != cudaSuccess ||
+      cudaFuncSetAttribute(reinterpret_cast<const void*>(rasterize_kernel<kFusedThreads>),
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemFused)) != cudaSuccess)
     return bail(fail(s, CKMPM_ERR_CUDA, "cudaFuncSetAttribute failed"));
-  int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, g2p2g_kernel<kFixedCorotated, kFusedThreads>, kFusedThreads,
-                                                kSmemFused);
-  int occ2 = 0, occ3 = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, g2p2g_kernel<kDruckerPrager, kFusedThreads>, kFusedThreads,
-                                                kSmemFused);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, g2p2g_kernel<kFluid, kFusedThreads>, kFusedThreads, kSmemFused);
-  occ = std::max(1, std::min(occ, std::min(occ2, occ3)));
-  s->fused_ctas = occ * s->sm_count;
+  // Default launch shape: 256 threads, as many resident CTAs as fit, graphs of 8.
+  s->tune.threads = kFusedThreads;
+  s->tune.ctas_per_sm = static_cast<uint32_t>(s->occ[1]);
+  s->tune.graph_chunk = kGraphChunk;
+  s->tune.probe_ms = 0.f;
+  s->fused_ctas = s->occ[1] * s->sm_count;
   if (cudaStreamSynchronize(s->stream) != cudaSuccess) return bail(fail(s, CKMPM_ERR_CUDA, "init sync failed"));
   *out = s;
   return CKMPM_OK;
 }
+
+ckmpm_status apply_tuning(ckmpm_scene* s, const ckmpm_tuning& t) {
+  if (t.threads != 128 && t.threads != 256) return fail(s, CKMPM_ERR_INVALID, "threads must be 128 or 256");
+  const int occ = s->occ[t.threads == 128 ? 0 : 1];
+  if (t.ctas_per_sm < 1 || t.ctas_per_sm > static_cast<uint32_t>(occ))
+    return fail(s, CKMPM_ERR_INVALID, "ctas_per_sm must be between 1 and the kernel's occupancy");
+  if (t.graph_chunk < 2 || t.graph_chunk > kMaxGraphChunk || (t.graph_chunk & 1))
+    return fail(s, CKMPM_ERR_INVALID, "graph_chunk must be even, 2..64");
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  free_graphs(s);
+  s->tune = t;
+  s->fused_ctas = static_cast<int>(t.ctas_per_sm) * s->sm_count;
+  return CKMPM_OK;
+}
+
+// Checkpoint: the state allocations back to back, each at a 256-byte offset.
+size_t checkpoint_bytes(const ckmpm_scene* s) {
+  size_t total = 0;
+  for (size_t i = 0; i < s->n_state_allocs; ++i) total += (s->allocs[i].second + 255) & ~static_cast<size_t>(255);
+  return total;
+}
+
+cudaError_t checkpoint_copy(ckmpm_scene* s, unsigned char* buf, bool save) {
+  size_t off = 0;
+  for (size_t i = 0; i < s->n_state_allocs; ++i) {
+    void* p = s->allocs[i].first;
+    const size_t b = s->allocs[i].second;
+    cudaError_t e = save ? cudaMemcpyAsync(buf + off, p, b, cudaMemcpyDeviceToDevice, s->stream)
+                         : cudaMemcpyAsync(p, buf + off, b, cudaMemcpyDeviceToDevice, s->stream);
+    if (e != cudaSuccess) return e;
+    off += (b + 255) & ~static_cast<size_t>(255);
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ckmpm_version(void) { return kVersion; }
+
+ckmpm_status ckmpm_create(const ckmpm_scene_desc* desc, ckmpm_scene** out) { return create_impl(desc, 1, out); }
+
+ckmpm_status ckmpm_create_batch(const ckmpm_scene_desc* desc, uint32_t nscenes, ckmpm_scene** out) {
+  return create_impl(desc, nscenes, out);
+}
+
+ckmpm_status ckmpm_add_batch(ckmpm_scene* s, uint32_t nscenes, const ckmpm_batch_scene* scenes, const float* x,
+                             const float* v) {
+  if (!s || !scenes || !x || !v) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  if (s->setup_done) return fail(s, CKMPM_ERR_INVALID, "scenes must be added before ckmpm_setup");
+  if (!s->models.empty()) return fail(s, CKMPM_ERR_INVALID, "a batch holds exactly one ckmpm_add_batch call");
+  if (nscenes != s->nstack) return fail(s, CKMPM_ERR_INVALID, "nscenes differs from ckmpm_create_batch");
+  ModelHost m;
+  m.mat.kind = kMixedKind;
+  m.smat.resize(nscenes);
+  m.skind.resize(nscenes);
+  m.sstart.assign(nscenes + 1, 0u);
+  uint64_t total = 0;
+  float lightest = 0.f;
+  for (uint32_t i = 0; i < nscenes; ++i) {
+    const ckmpm_batch_scene& b = scenes[i];
+    const int k = b.material.kind;
+    if (k != CKMPM_FIXED_COROTATED && k != CKMPM_DRUCKER_PRAGER && k != CKMPM_FLUID)
+      return fail(s, CKMPM_ERR_INVALID, "unsupported material kind in scene " + std::to_string(i));
+    if (!(b.mass > 0.f) || !(b.volume > 0.f))
+      return fail(s, CKMPM_ERR_INVALID, "mass and volume must be positive (scene " + std::to_string(i) + ")");
+    if (k != CKMPM_FLUID && !(b.material.p[1] > 0.f))
+      return fail(s, CKMPM_ERR_INVALID, "mu must be positive (scene " + std::to_string(i) + ")");
+    SceneMat& sm = m.smat[i];
+    sm.kind = k;
+    for (int j = 0; j < 4; ++j) sm.p[j] = b.material.p[j];
+    sm.vol_over_mass = b.volume / b.mass;
+    sm.unit = b.mass * kFixInvScale;
+    sm.aux0 = k == CKMPM_FLUID ? b.material.p[3] : 0.f;
+    m.skind[i] = k;
+    m.sstart[i] = static_cast<uint32_t>(total);
+    total += b.n;
+    lightest = (i == 0) ? b.mass : std::min(lightest, b.mass);
+  }
+  if (total == 0 || total > 0xFFFFFFF0ull) return fail(s, CKMPM_ERR_INVALID, "batch particle count out of range");
+  m.sstart[nscenes] = static_cast<uint32_t>(total);
+  m.n = static_cast<uint32_t>(total);
+  m.nv = m.n;
+  m.mass = lightest;  // only the adaptive-dt mass floor reads it for a batch
+  m.vol = 1.f;
+  m.x.assign(x, x + 3 * static_cast<size_t>(total));
+  m.v.assign(v, v + 3 * static_cast<size_t>(total));
+  s->models.push_back(std::move(m));
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_set_tuning(ckmpm_scene* s, const ckmpm_tuning* t) {
+  if (!s || !t) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  return apply_tuning(s, *t);
+}
+
+ckmpm_status ckmpm_get_tuning(ckmpm_scene* s, ckmpm_tuning* t, uint32_t* max_ctas_per_sm2) {
+  if (!s || !t) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  *t = s->tune;
+  if (max_ctas_per_sm2) {
+    max_ctas_per_sm2[0] = static_cast<uint32_t>(s->occ[0]);
+    max_ctas_per_sm2[1] = static_cast<uint32_t>(s->occ[1]);
+  }
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_checkpoint_bytes(ckmpm_scene* s, uint64_t* bytes) {
+  if (!s || !bytes) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  if (!s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  *bytes = checkpoint_bytes(s);
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_checkpoint_save(ckmpm_scene* s, void* device_dst) {
+  if (!s || !device_dst) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  if (!s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  CK_CUDA(s, checkpoint_copy(s, static_cast<unsigned char*>(device_dst), true));
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_checkpoint_restore(ckmpm_scene* s, const void* device_src) {
+  if (!s || !device_src) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  if (!s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  CK_CUDA(s, checkpoint_copy(s, static_cast<unsigned char*>(const_cast<void*>(device_src)), false));
+  Scalars h{};
+  CK_CUDA(s, cudaMemcpyAsync(&h, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  s->host_step = static_cast<uint64_t>(h.step);
+  return CKMPM_OK;
+}
+
+const char* ckmpm_last_error(const ckmpm_scene* s) { return s ? s->err.c_str() : g_create_error.c_str(); }
 
 ckmpm_status ckmpm_add_model(ckmpm_scene* s, const ckmpm_material* material, uint32_t n, const float* x,
                              const float* v, uint32_t nv, float mass, float volume, int32_t* model_index) {
@@ -293,11 +446,13 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
   if (s->models.empty()) return fail(s, CKMPM_ERR_INVALID, "no models");
   CK_CUDA(s, cudaSetDevice(s->desc.device));
   const uint32_t nbd = s->sc.nblocks_domain;
-  const bool track = (s->desc.flags & CKMPM_FLAG_TRACK_IDS) != 0;
   uint32_t lost_at_setup = 0;
   for (auto& m : s->models) {
     ModelDev& d = m.dev;
     const uint32_t n = m.n;
+    const bool batch = m.mat.kind == kMixedKind;
+    // A batch always tracks ids: they map each particle back to its scene.
+    const bool track = batch || (s->desc.flags & CKMPM_FLAG_TRACK_IDS) != 0;
     d.cap_particles = n;
     d.cap_slots = std::max<uint32_t>(1, std::min<uint32_t>(nbd, n));
     d.max_per_block = s->desc.max_particles_per_block;
@@ -340,6 +495,19 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     CK_CUDA(s, dalloc(s, &d.done, d.cap_slots));
     CK_CUDA(s, cudaMemsetAsync(d.done, 0xFF, sizeof(int32_t) * d.cap_slots, s->stream));
     CK_CUDA(s, dalloc(s, &d.vel_in, 3 * static_cast<size_t>(n)));
+    d.smat = nullptr;
+    d.sstart = nullptr;
+    if (batch) {
+      SceneMat* sm = nullptr;
+      uint32_t* ss = nullptr;
+      CK_CUDA(s, dalloc(s, &sm, m.smat.size()));
+      CK_CUDA(s, dalloc(s, &ss, m.sstart.size()));
+      CK_CUDA(s, cudaMemcpyAsync(sm, m.smat.data(), sizeof(SceneMat) * m.smat.size(), cudaMemcpyHostToDevice, s->stream));
+      CK_CUDA(s, cudaMemcpyAsync(ss, m.sstart.data(), sizeof(uint32_t) * m.sstart.size(), cudaMemcpyHostToDevice,
+                                 s->stream));
+      d.smat = sm;
+      d.sstart = ss;
+    }
 
     // Upload, bin, radix-sort by colour-major block index, compact.
     float *dx_in = nullptr, *dv_in = nullptr;
@@ -352,7 +520,7 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     CK_CUDA(s, cudaMalloc(&v_out, sizeof(uint32_t) * n));
     CK_CUDA(s, cudaMemcpyAsync(dx_in, m.x.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->stream));
     CK_CUDA(s, cudaMemcpyAsync(dv_in, m.v.data(), sizeof(float) * 3 * m.nv, cudaMemcpyHostToDevice, s->stream));
-    setup_bin_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(s->sc, n, dx_in, k_in, v_in, d.dense_total);
+    setup_bin_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(s->sc, n, dx_in, d.sstart, k_in, v_in, d.dense_total);
     size_t temp_bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, k_in, k_out, v_in, v_out, static_cast<int>(n), 0, 32,
                                     s->stream);
@@ -369,8 +537,8 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     lost_at_setup += n - m.n_valid;
     const float aux0 = m.mat.kind == CKMPM_FLUID ? m.mat.p[3] : 0.f;
     if (m.n_valid > 0)
-      setup_gather_kernel<<<(m.n_valid + 255) / 256, 256, 0, s->stream>>>(d, m.n_valid, v_out, dx_in, dv_in, m.nv,
-                                                                           aux0);
+      setup_gather_kernel<<<(m.n_valid + 255) / 256, 256, 0, s->stream>>>(d, s->nstack, m.n_valid, v_out, dx_in,
+                                                                           dv_in, m.nv, aux0);
     // Identity previous-step structures in list 1.
     CK_CUDA(s, cudaMemcpyAsync(d.bl[1].table, d.bl[0].table, sizeof(int32_t) * nbd, cudaMemcpyDeviceToDevice,
                                s->stream));
@@ -411,6 +579,7 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
   CK_CUDA(s, cudaStreamSynchronize(s->stream));
   s->setup_done = true;
   s->host_step = 0;
+  s->n_state_allocs = s->allocs.size();
   Scalars r{};
   CK_CUDA(s, cudaMemcpy(&r, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost));
   return status_from(s, r);
@@ -435,11 +604,12 @@ ckmpm_status ckmpm_step_async(ckmpm_scene* s, uint32_t nsteps, float dt) {
   uint32_t done = 0;
   while (done < nsteps) {
     const int parity = static_cast<int>(s->host_step & 1);
-    if (parity == 0 && nsteps - done >= static_cast<uint32_t>(kGraphChunk)) {
-      if (!s->graph_chunk) CK_CUDA(s, build_graph(s, kGraphChunk, 0, &s->graph_chunk));
+    const uint32_t chunk = s->tune.graph_chunk;
+    if (parity == 0 && nsteps - done >= chunk) {
+      if (!s->graph_chunk) CK_CUDA(s, build_graph(s, static_cast<int>(chunk), 0, &s->graph_chunk));
       CK_CUDA(s, cudaGraphLaunch(s->graph_chunk, s->stream));
-      done += kGraphChunk;
-      s->host_step += kGraphChunk;
+      done += chunk;
+      s->host_step += chunk;
     } else {
       CK_CUDA(s, enqueue_substep(s, parity));
       ++done;
@@ -565,6 +735,12 @@ ckmpm_status ckmpm_get_state(ckmpm_scene* s, int32_t model, float* x, float* v, 
     for (uint32_t j = 0; j < n; ++j)
       for (int k = 0; k < 9; ++k) F[9 * j + k] = (k & 3) ? 0.f : 1.f;
   if (aux && m.mat.kind == CKMPM_FIXED_COROTATED) std::fill(aux, aux + n, 0.f);
+  // Batch: a fluid scene's particles carry no F (reported as I) and a
+  // fixed-corotated scene's no aux (reported as 0).
+  auto scene_kind = [&](uint32_t pid) {
+    const auto it = std::upper_bound(m.sstart.begin(), m.sstart.end(), pid);
+    return m.skind[static_cast<size_t>(it - m.sstart.begin()) - 1];
+  };
   if (sorted) {
     std::vector<uint32_t> order(n);
     for (uint32_t i = 0; i < n; ++i) order[i] = i;
@@ -576,6 +752,12 @@ ckmpm_status ckmpm_get_state(ckmpm_scene* s, int32_t model, float* x, float* v, 
       if (F && m.mat.kind != CKMPM_FLUID) std::memcpy(F + 9 * j, &m.hF[9 * i], sizeof(float) * 9);
       if (aux && m.mat.kind != CKMPM_FIXED_COROTATED) aux[j] = m.ha[i];
       if (id) id[j] = m.hid[i];
+      if (m.mat.kind == kMixedKind) {
+        const int32_t k = scene_kind(m.hid[i]);
+        if (F && k == CKMPM_FLUID)
+          for (int c = 0; c < 9; ++c) F[9 * j + c] = (c & 3) ? 0.f : 1.f;
+        if (aux && k == CKMPM_FIXED_COROTATED) aux[j] = 0.f;
+      }
     }
   } else if (id) {
     std::memcpy(id, m.hid.data(), sizeof(uint32_t) * n);
@@ -585,7 +767,13 @@ ckmpm_status ckmpm_get_state(ckmpm_scene* s, int32_t model, float* x, float* v, 
 
 ckmpm_status ckmpm_get_blocks(ckmpm_scene* s, int32_t model, int32_t which, int32_t* keys, uint32_t* counts,
                               uint32_t cap, uint32_t* n_out) {
+  return ckmpm_get_blocks_in(s, 0, model, which, keys, counts, cap, n_out);
+}
+
+ckmpm_status ckmpm_get_blocks_in(ckmpm_scene* s, uint32_t scene, int32_t model, int32_t which, int32_t* keys,
+                                 uint32_t* counts, uint32_t cap, uint32_t* n_out) {
   if (!s) return fail(s, CKMPM_ERR_INVALID, "null scene");
+  if (scene >= s->nstack) return fail(s, CKMPM_ERR_NOT_FOUND, "no such scene in the batch");
   if (!s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
   if (which < 0 || which > 2) return fail(s, CKMPM_ERR_INVALID, "which must be 0, 1 or 2");
   if (model >= static_cast<int32_t>(s->models.size())) return fail(s, CKMPM_ERR_NOT_FOUND, "no such model");
@@ -603,7 +791,8 @@ ckmpm_status ckmpm_get_blocks(ckmpm_scene* s, int32_t model, int32_t which, int3
       CK_CUDA(s, cudaMemcpy(hk.data(), cur.keys, sizeof(int4) * nb, cudaMemcpyDeviceToHost));
       CK_CUDA(s, cudaMemcpy(hc.data(), cur.count, sizeof(uint32_t) * nb, cudaMemcpyDeviceToHost));
     }
-    for (uint32_t i = 0; i < nb; ++i) set[std::make_tuple(hk[i].x, hk[i].y, hk[i].z)] += hc[i];
+    for (uint32_t i = 0; i < nb; ++i)
+      if (static_cast<uint32_t>(hk[i].w) == scene) set[std::make_tuple(hk[i].x, hk[i].y, hk[i].z)] += hc[i];
   }
   if (which >= 1) {
     const int lo = which == 1 ? 0 : -1;
@@ -634,6 +823,73 @@ ckmpm_status ckmpm_get_blocks(ckmpm_scene* s, int32_t model, int32_t which, int3
     ++i;
   }
   return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_autotune(ckmpm_scene* s, uint32_t probe_steps, float dt, ckmpm_tuning* results, uint32_t cap,
+                            uint32_t* n_results, ckmpm_tuning* best) {
+  if (!s || !best) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  if (!s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  if (probe_steps < 2 || probe_steps > 4096) return fail(s, CKMPM_ERR_INVALID, "probe_steps must be 2..4096");
+  if (!(dt >= 0.f)) return fail(s, CKMPM_ERR_INVALID, "dt must be non-negative");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  // The probes advance the simulation; the state is saved first and put back
+  // after every candidate, so tuning leaves the scene exactly as it found it.
+  const size_t bytes = checkpoint_bytes(s);
+  void* saved = nullptr;
+  CK_CUDA(s, cudaMalloc(&saved, bytes));
+  struct Guard {
+    void* p;
+    ~Guard() { cudaFree(p); }
+  } guard{saved};
+  CK_CUDA(s, checkpoint_copy(s, static_cast<unsigned char*>(saved), true));
+  const ckmpm_tuning before = s->tune;
+  std::vector<ckmpm_tuning> cands;
+  for (uint32_t nt : {256u, 128u}) {
+    const int occ = s->occ[nt == 128 ? 0 : 1];
+    for (int c = occ; c >= 1; --c)
+      for (uint32_t chunk : {8u, 32u}) cands.push_back(ckmpm_tuning{nt, static_cast<uint32_t>(c), chunk, 0.f});
+  }
+  cudaEvent_t e0, e1;
+  CK_CUDA(s, cudaEventCreate(&e0));
+  CK_CUDA(s, cudaEventCreate(&e1));
+  ckmpm_status result = CKMPM_OK;
+  for (auto& c : cands) {
+    ckmpm_status st = CKMPM_OK;
+    if ((st = ckmpm_checkpoint_restore(s, saved)) != CKMPM_OK || (st = apply_tuning(s, c)) != CKMPM_OK ||
+        (st = ckmpm_step_async(s, c.graph_chunk, dt)) != CKMPM_OK) {  // warm-up; captures this shape's graph
+      result = st;
+      break;
+    }
+    const uint32_t k = ((probe_steps + c.graph_chunk - 1) / c.graph_chunk) * c.graph_chunk;
+    cudaEventRecord(e0, s->stream);
+    st = ckmpm_step_async(s, k, dt);
+    cudaEventRecord(e1, s->stream);
+    if (st == CKMPM_OK) st = ckmpm_status_check(s);
+    if (st != CKMPM_OK) {
+      result = st;
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    c.probe_ms = ms / static_cast<float>(k);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ckmpm_status rs = ckmpm_checkpoint_restore(s, saved);
+  if (result != CKMPM_OK) {
+    apply_tuning(s, before);
+    return result;
+  }
+  if (rs != CKMPM_OK) return rs;
+  const ckmpm_tuning* pick = &cands[0];
+  for (const auto& c : cands)
+    if (c.probe_ms < pick->probe_ms) pick = &c;
+  *best = *pick;
+  if (n_results) *n_results = static_cast<uint32_t>(cands.size());
+  if (results)
+    for (uint32_t i = 0; i < std::min<uint32_t>(cap, static_cast<uint32_t>(cands.size())); ++i) results[i] = cands[i];
+  return apply_tuning(s, *pick);
 }
 
 ckmpm_status ckmpm_get_counters(ckmpm_scene* s, uint64_t* out5) {
@@ -742,7 +998,7 @@ ckmpm_status ckmpm_destroy(ckmpm_scene* s) {
   cudaSetDevice(s->desc.device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   free_graphs(s);
-  for (void* p : s->allocs) cudaFree(p);
+  for (auto& p : s->allocs) cudaFree(p.first);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
   delete s;
   return CKMPM_OK;

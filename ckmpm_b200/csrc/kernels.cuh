@@ -1,6 +1,8 @@
 // Device kernels of the CK-MPM substep.
 //
-// Data layout (per scene):
+// Data layout (per scene; a batch stacks `nstack` identical domains, scene w
+// owning table entries [w * blocks, (w + 1) * blocks), and no stencil, wait or
+// rebin ever crosses from one stacked domain into another):
 //  * grid[2]: dense over every 4^3 block of the domain, 2 KB per block:
 //    [m, mvx, mvy, mvz][grid -dx/4, +dx/4][cell i*16 + j*4 + k], the per-block
 //    SoA of the reference's MPMGridBlock (include/mpm_grid.cuh:18-67) but
@@ -47,14 +49,27 @@ enum StatusBits : uint32_t {
 
 struct SceneDev {
   float dx, inv_dx;
-  int32_t dims[3];
+  int32_t dims[3];       // blocks per axis of one domain
   float gravity, mass_clamp;
   int32_t boundary;
   float floor_cells;
-  uint32_t cbase[9];     // colour-major traversal: first index of each colour class
-  int32_t cdims[8][3];   // sub-lattice extent of each colour class
-  uint32_t nblocks_domain;
+  uint32_t cbase[9];     // colour-major traversal: first index of each colour class (all stacked domains)
+  int32_t cdims[8][3];   // sub-lattice extent of each colour class in one domain
+  uint32_t ccount[8];    // blocks of each colour class in one domain
+  uint32_t nstack;       // stacked domains (1 for a single scene, the scene count for a batch)
+  uint32_t nblocks_domain;  // table entries over all stacked domains
 };
+
+// Per-scene material of a batch (one model per stacked domain).
+struct SceneMat {
+  int32_t kind;
+  float p[4];
+  float vol_over_mass;  // V_p / m_p
+  float unit;           // m_p * 2^-36: value of one fixed-point unit of the P2G tile
+  float aux0;           // initial logJp (0) or J
+};
+
+constexpr int kMixed = 7;  // material kind read per work item from the scene's SceneMat
 
 struct Scalars {
   int32_t step;        // substeps taken; epoch of the grid that the next substep reads
@@ -103,6 +118,8 @@ struct ModelDev {
   int32_t track_ids;
   MaterialParams mat;
   float mass, vol;
+  const SceneMat* smat;     // batch: per stacked domain; null for a single scene
+  const uint32_t* sstart;   // batch setup: first input particle of each scene (nstack + 1)
 };
 
 struct GridDev {
@@ -110,13 +127,42 @@ struct GridDev {
   int32_t* stamp[2];
 };
 
+// Colour classes of the traversal over `nstack` stacked domains of sc.dims
+// blocks: class c holds the blocks whose coordinate parities are the bits of c.
+inline void init_colour_classes(SceneDev& sc, uint32_t nstack) {
+  sc.nstack = nstack;
+  sc.nblocks_domain = nstack * static_cast<uint32_t>(sc.dims[0]) * sc.dims[1] * sc.dims[2];
+  uint32_t base = 0;
+  for (int c = 0; c < 8; ++c) {
+    const int par[3] = {(c >> 2) & 1, (c >> 1) & 1, c & 1};
+    for (int a = 0; a < 3; ++a) sc.cdims[c][a] = (sc.dims[a] - par[a] + 1) / 2;
+    sc.ccount[c] = static_cast<uint32_t>(sc.cdims[c][0]) * sc.cdims[c][1] * sc.cdims[c][2];
+    sc.cbase[c] = base;
+    base += nstack * sc.ccount[c];
+  }
+  sc.cbase[8] = base;
+}
+
 // ------------------------------------------------------------------ helpers
 __device__ __forceinline__ bool in_domain(const SceneDev& sc, int x, int y, int z) {
   return (unsigned)x < (unsigned)sc.dims[0] && (unsigned)y < (unsigned)sc.dims[1] && (unsigned)z < (unsigned)sc.dims[2];
 }
 
-__device__ __forceinline__ int64_t flat_block(const SceneDev& sc, int x, int y, int z) {
-  return (static_cast<int64_t>(x) * sc.dims[1] + y) * sc.dims[2] + z;
+__device__ __forceinline__ int64_t flat_block(const SceneDev& sc, int w, int x, int y, int z) {
+  return ((static_cast<int64_t>(w) * sc.dims[0] + x) * sc.dims[1] + y) * sc.dims[2] + z;
+}
+
+// Scene of input particle i from the batch's scene offsets (binary search).
+__device__ __forceinline__ int scene_of(const uint32_t* sstart, uint32_t nstack, uint32_t i) {
+  int lo = 0, hi = static_cast<int>(nstack);
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (sstart[mid] <= i)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
 }
 
 __device__ __forceinline__ int colour_of(int x, int y, int z) { return ((x & 1) << 2) | ((y & 1) << 1) | (z & 1); }
@@ -182,7 +228,7 @@ __device__ __forceinline__ void window_blocks(const SceneDev& sc, const int32_t*
   const int bx = key.x + (e >> 2), by = key.y + ((e >> 1) & 1), bz = key.z + (e & 1);
   int64_t fb = -1;
   if (in_domain(sc, bx, by, bz)) {
-    const int64_t f = flat_block(sc, bx, by, bz);
+    const int64_t f = flat_block(sc, key.w, bx, by, bz);
     if (stin[f] == read_epoch) fb = f;
   }
   s_blk[e] = fb;
@@ -405,14 +451,14 @@ __device__ __forceinline__ void flush_tile(const SceneDev& sc, const BlockListDe
   if (waiter) {
     // One spin budget for all waits of this flush; once any wait in the launch
     // has given up (status bit set), later waits do not spin at all.
-    const int c0 = key.w;
+    const int c0 = colour_of(key.x, key.y, key.z);
     bool give_up = (*reinterpret_cast<volatile uint32_t*>(&scal->status) & kStatusTimeout) != 0;
     uint32_t spins = 0;
     for (int nb = 0; nb < 27 && !give_up; ++nb) {
       if (nb == 13) continue;
       const int x = key.x + nb / 9 - 1, y = key.y + (nb / 3) % 3 - 1, z = key.z + nb % 3 - 1;
       if (!in_domain(sc, x, y, z) || colour_of(x, y, z) >= c0) continue;
-      const int32_t slot = cur.table[flat_block(sc, x, y, z)];
+      const int32_t slot = cur.table[flat_block(sc, key.w, x, y, z)];
       if (slot < 0) continue;
       while (ld_acquire(done + slot) != epoch) {
         if (++spins > kSpinLimit) {
@@ -430,7 +476,7 @@ __device__ __forceinline__ void flush_tile(const SceneDev& sc, const BlockListDe
     const int e = threadIdx.x;
     const int x = key.x + (e >> 2), y = key.y + ((e >> 1) & 1), z = key.z + (e & 1);
     int mode = 2;
-    if (in_domain(sc, x, y, z)) mode = (ld_acquire(stout + flat_block(sc, x, y, z)) == epoch) ? 1 : 0;
+    if (in_domain(sc, x, y, z)) mode = (ld_acquire(stout + flat_block(sc, key.w, x, y, z)) == epoch) ? 1 : 0;
     s_mode[e] = mode;
   }
   __syncthreads();
@@ -446,7 +492,8 @@ __device__ __forceinline__ void flush_tile(const SceneDev& sc, const BlockListDe
     const unsigned long long* src = ptile + ((gi * 8 + lx) * 64 + ly * 8 + lz);
     const unsigned long long s0 = src[0], s1 = src[kTileNodes], s2 = src[2 * kTileNodes], s3 = src[3 * kTileNodes];
     if (mode == 1 && (s0 | s1 | s2 | s3) == 0ull) continue;
-    float* dst = gout + flat_block(sc, key.x + (e >> 2), key.y + ((e >> 1) & 1), key.z + (e & 1)) * 512 + gi * 64 + cell;
+    float* dst =
+        gout + flat_block(sc, key.w, key.x + (e >> 2), key.y + ((e >> 1) & 1), key.z + (e & 1)) * 512 + gi * 64 + cell;
     const float v0 = __ll2float_rn(static_cast<long long>(s0)) * unit;
     const float v1 = __ll2float_rn(static_cast<long long>(s1)) * unit;
     const float v2 = __ll2float_rn(static_cast<long long>(s2)) * unit;
@@ -467,7 +514,7 @@ __device__ __forceinline__ void flush_tile(const SceneDev& sc, const BlockListDe
   __syncthreads();
   if (threadIdx.x < 8 && s_mode[threadIdx.x] == 0) {
     const int e = threadIdx.x;
-    stout[flat_block(sc, key.x + (e >> 2), key.y + ((e >> 1) & 1), key.z + (e & 1))] = epoch;
+    stout[flat_block(sc, key.w, key.x + (e >> 2), key.y + ((e >> 1) & 1), key.z + (e & 1))] = epoch;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -488,7 +535,7 @@ __device__ __forceinline__ void incoming_groups(const SceneDev& sc, const BlockL
   if (lane < 27) {
     const int x = key.x + lane / 9 - 1, y = key.y + (lane / 3) % 3 - 1, z = key.z + lane % 3 - 1;
     if (in_domain(sc, x, y, z)) {
-      const int32_t s = prev.table[flat_block(sc, x, y, z)];
+      const int32_t s = prev.table[flat_block(sc, key.w, x, y, z)];
       if (s >= 0) {
         const uint32_t a = prev.prefix28[s * 28 + lane], b = prev.prefix28[s * 28 + lane + 1];
         c = b - a;
@@ -545,9 +592,16 @@ constexpr size_t kSmemFused = kSmemVTile + kSmemPTile + kSmemCodes;
 // colour-major order).  Replaces the reference's G2P2G
 // (include/mpm_algorithm.cuh:1367-1845) together with the grid update
 // (:739-869), the advection record (mpm_particle.cuh:333-371) and the
-// per-block list build (:629-649, :1868-1918).
+// per-block list build (:629-649, :1868-1918).  KIND is the material, or
+// kMixed for a batch, where each work item reads its scene's material (one
+// scene per stacked domain, so the kind is uniform across the CTA).  Register
+// budget: 64 per thread at 256 threads (4 CTAs per SM); at 128 threads the
+// shared-memory footprint allows 5 CTAs per SM, so up to 102 registers.
+template <int NT>
+constexpr int fused_min_ctas() { return NT == 128 ? 5 : 1024 / NT; }
+
 template <int KIND, int NT>
-__global__ void __launch_bounds__(NT, 4)
+__global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
     g2p2g_kernel(SceneDev sc, ModelDev md, GridDev gd, Scalars* __restrict__ scal) {
   static_assert(NT % 32 == 0 && NT / 32 <= 8 && NT >= 64, "block size");
   extern __shared__ __align__(16) unsigned char smem[];
@@ -570,7 +624,6 @@ __global__ void __launch_bounds__(NT, 4)
   int32_t* __restrict__ stout = gd.stamp[parity ^ 1];
   const uint32_t nb = *cur.nblocks;
   const float dx = sc.dx, inv_dx = sc.inv_dx;
-  const float vol_over_mass = md.vol / md.mass;
   const uint32_t maxp = min(md.max_per_block, static_cast<uint32_t>(kMaxParticlesPerBlock));
 
   for (;;) {
@@ -581,6 +634,18 @@ __global__ void __launch_bounds__(NT, 4)
     const int4 key = cur.keys[item];
     const uint32_t start = cur.start[item];
     uint32_t n = cur.count[item];
+    int kind = KIND;
+    float mp0 = md.mat.p[0], mp1 = md.mat.p[1], mp2 = md.mat.p[2];
+    float vol_over_mass = md.vol / md.mass, unit = md.mass * kFixInvScale;
+    if (KIND == kMixed) {
+      const SceneMat& sm = md.smat[key.w];
+      kind = sm.kind;
+      mp0 = sm.p[0];
+      mp1 = sm.p[1];
+      mp2 = sm.p[2];
+      vol_over_mass = sm.vol_over_mass;
+      unit = sm.unit;
+    }
 
     if (threadIdx.x < 32)
       incoming_groups(sc, prev, key, sh.off, sh.idx, sh.src);
@@ -610,11 +675,11 @@ __global__ void __launch_bounds__(NT, 4)
       float x[3] = {sin.x[0][iin], sin.x[1][iin], sin.x[2][iin]};
       float F[9];
       float aux = 0.f;
-      if (KIND != kFluid) {
+      if (kind != kFluid) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) F[k] = sin.F[k][iin];
       }
-      if (KIND != kFixedCorotated) aux = sin.aux[iin];
+      if (kind != kFixedCorotated) aux = sin.aux[iin];
       float xs[3] = {x[0] * inv_dx, x[1] * inv_dx, x[2] * inv_dx};
       bool inside = true;
       float v[3], C[9];
@@ -623,28 +688,28 @@ __global__ void __launch_bounds__(NT, 4)
       for (int a = 0; a < 3; ++a) x[a] += dt * v[a];
 
       float tau[9];
-      if (KIND == kFluid) {
-        stress_fluid(md.mat.p[0], md.mat.p[1], md.mat.p[2], C, dt, aux, tau);
+      if (kind == kFluid) {
+        stress_fluid(mp0, mp1, mp2, C, dt, aux, tau);
       } else {
         float dW[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) dW[k] = C[k] * dt + ((k & 3) ? 0.f : 1.f);
         matmul3(dW, F, F);
-        if (KIND == kFixedCorotated)
-          stress_fixed_corotated(md.mat.p[0], md.mat.p[1], F, tau);
+        if (kind == kFixedCorotated)
+          stress_fixed_corotated(mp0, mp1, F, tau);
         else
-          stress_drucker_prager(md.mat.p[0], md.mat.p[1], F, aux, tau);
+          stress_drucker_prager(mp0, mp1, F, aux, tau);
       }
 
       const uint32_t o = start + q;
       sout.x[0][o] = x[0];
       sout.x[1][o] = x[1];
       sout.x[2][o] = x[2];
-      if (KIND != kFluid) {
+      if (kind != kFluid) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) sout.F[k][o] = F[k];
       }
-      if (KIND != kFixedCorotated) sout.aux[o] = aux;
+      if (kind != kFixedCorotated) sout.aux[o] = aux;
       if (md.track_ids) sout.id[o] = sin.id[iin];
 
       // Rebin record: direction code of (old block - new block), 27 = lost.
@@ -750,7 +815,7 @@ __global__ void __launch_bounds__(NT, 4)
           cur.prefix28[item * 28 + lane] = pre;
           if (c > 0) {
             const int x = key.x - (lane / 9 - 1), y = key.y - ((lane / 3) % 3 - 1), z = key.z - (lane % 3 - 1);
-            atomicAdd(md.dense_total + flat_block(sc, x, y, z), c);
+            atomicAdd(md.dense_total + flat_block(sc, key.w, x, y, z), c);
           }
         }
         if (lane == 26) cur.prefix28[item * 28 + 27] = incl;
@@ -770,7 +835,7 @@ __global__ void __launch_bounds__(NT, 4)
         __syncwarp();
       }
     }
-    flush_tile<NT>(sc, cur, md.done, item, key, ptile, md.mass * kFixInvScale, gout, stout, write_epoch, scal, sh.mode,
+    flush_tile<NT>(sc, cur, md.done, item, key, ptile, unit, gout, stout, write_epoch, scal, sh.mode,
                    threadIdx.x == 32);
   }
 }
@@ -821,8 +886,9 @@ __global__ void __launch_bounds__(NT, 2) rasterize_kernel(SceneDev sc, ModelDev 
       if (ok && finite) p2g_scatter(ptile, st, lb, v, Z);
     }
     __syncthreads();
-    flush_tile<NT>(sc, cur, md.done, item, key, ptile, md.mass * kFixInvScale, gd.grid[0], gd.stamp[0], 0, scal,
-                   sh.mode, threadIdx.x == 32);
+    const float unit = md.smat ? md.smat[key.w].unit : md.mass * kFixInvScale;
+    flush_tile<NT>(sc, cur, md.done, item, key, ptile, unit, gd.grid[0], gd.stamp[0], 0, scal, sh.mode,
+                   threadIdx.x == 32);
   }
 }
 
@@ -833,16 +899,20 @@ __global__ void __launch_bounds__(NT, 2) rasterize_kernel(SceneDev sc, ModelDev 
 // MarkActiveParticleBlocks + ExclusiveScan + InverseExclusiveScan +
 // UpdatePartition + UpdateBucket + ComputeBinCount
 // (include/mpm_algorithm.cuh:26-45,573-582,1868-1918, include/mpm_engine.cuh:659-787).
+// Traversal index -> block key (x, y, z, stacked domain).  Order: colour
+// class, then stacked domain, then lexicographic within the class.
 __device__ __forceinline__ int4 traversal_key(const SceneDev& sc, uint32_t t) {
   int c = 0;
 #pragma unroll
   for (int k = 1; k < 8; ++k) c += (t >= sc.cbase[k]) ? 1 : 0;
-  const uint32_t loc = t - sc.cbase[c];
+  uint32_t loc = t - sc.cbase[c];
+  const uint32_t w = loc / sc.ccount[c];
+  loc -= w * sc.ccount[c];
   const uint32_t nz = sc.cdims[c][2], ny = sc.cdims[c][1];
   const int k = loc % nz;
   const int j = (loc / nz) % ny;
   const int i = loc / (nz * ny);
-  return make_int4(2 * i + ((c >> 2) & 1), 2 * j + ((c >> 1) & 1), 2 * k + (c & 1), c);
+  return make_int4(2 * i + ((c >> 2) & 1), 2 * j + ((c >> 1) & 1), 2 * k + (c & 1), static_cast<int>(w));
 }
 
 __device__ __forceinline__ uint32_t block_reduce_sum(uint32_t v, uint32_t* scratch) {
@@ -915,7 +985,7 @@ __global__ void __launch_bounds__(kCompactThreads) compact_reduce_kernel(SceneDe
     const uint32_t t = t0 + k;
     if (t >= sc.nblocks_domain) break;
     const int4 key = traversal_key(sc, t);
-    const uint32_t c = total[flat_block(sc, key.x, key.y, key.z)];
+    const uint32_t c = total[flat_block(sc, key.w, key.x, key.y, key.z)];
     nblk += c > 0 ? 1u : 0u;
     npart += c;
   }
@@ -950,7 +1020,7 @@ __global__ void __launch_bounds__(kCompactThreads)
     fb[k] = -1;
     if (t < sc.nblocks_domain) {
       keys[k] = traversal_key(sc, t);
-      fb[k] = flat_block(sc, keys[k].x, keys[k].y, keys[k].z);
+      fb[k] = flat_block(sc, keys[k].w, keys[k].x, keys[k].y, keys[k].z);
       c[k] = total[fb[k]];
       nblk += c[k] > 0 ? 1u : 0u;
       npart += c[k];
@@ -1026,7 +1096,7 @@ __global__ void grid_maxv_kernel(SceneDev sc, GridDev gd, Scalars* scal, float m
     if (stamp[b] != step) continue;
     const int bz = static_cast<int>(b % sc.dims[2]);
     const int by = static_cast<int>((b / sc.dims[2]) % sc.dims[1]);
-    const int bx = static_cast<int>(b / (static_cast<uint32_t>(sc.dims[2]) * sc.dims[1]));
+    const int bx = static_cast<int>((b / (static_cast<uint32_t>(sc.dims[2]) * sc.dims[1])) % sc.dims[0]);
     for (int node = lane; node < 128; node += 32) {
       const float4 v = node_velocity(sc, g + static_cast<int64_t>(b) * 512, node, bx, by, bz, by * 4 + ((node >> 2) & 3), dt);
       float n2 = v.x * v.x + v.y * v.y + v.z * v.z;
@@ -1060,8 +1130,8 @@ __global__ void adaptive_dt_kernel(Scalars* scal, float dx, float cfl, float dt_
 // (0xFFFFFFFF outside the domain), and the per-block count.  Replaces
 // ActivateBlocksWithParticles + BuildParticleCellBucket
 // (include/mpm_algorithm.cuh:586-626,713-736).
-__global__ void setup_bin_kernel(SceneDev sc, uint32_t n, const float* __restrict__ x, uint32_t* __restrict__ keys,
-                                 uint32_t* __restrict__ vals, uint32_t* __restrict__ total) {
+__global__ void setup_bin_kernel(SceneDev sc, uint32_t n, const float* __restrict__ x, const uint32_t* __restrict__ sstart,
+                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t* __restrict__ total) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
@@ -1071,10 +1141,11 @@ __global__ void setup_bin_kernel(SceneDev sc, uint32_t n, const float* __restric
   uint32_t key = 0xFFFFFFFFu;
   const bool finite = isfinite(px) && isfinite(py) && isfinite(pz) && px >= 0.f && py >= 0.f && pz >= 0.f;
   if (finite && in_domain(sc, bx, by, bz)) {
+    const int w = sstart ? scene_of(sstart, sc.nstack, i) : 0;
     const int c = colour_of(bx, by, bz);
     const uint32_t nz = sc.cdims[c][2], ny = sc.cdims[c][1];
-    key = sc.cbase[c] + ((bx >> 1) * ny + (by >> 1)) * nz + (bz >> 1);
-    atomicAdd(total + flat_block(sc, bx, by, bz), 1u);
+    key = sc.cbase[c] + w * sc.ccount[c] + ((bx >> 1) * ny + (by >> 1)) * nz + (bz >> 1);
+    atomicAdd(total + flat_block(sc, w, bx, by, bz), 1u);
   }
   keys[i] = key;
   vals[i] = i;
@@ -1083,7 +1154,7 @@ __global__ void setup_bin_kernel(SceneDev sc, uint32_t n, const float* __restric
 // Sorted initial state: x from the input, F = I, aux = logJp0 (0) or J0,
 // id = input index, velocities gathered for the rasterisation
 // (include/mpm_algorithm.cuh:974-1081).
-__global__ void setup_gather_kernel(ModelDev md, uint32_t n, const uint32_t* __restrict__ perm,
+__global__ void setup_gather_kernel(ModelDev md, uint32_t nstack, uint32_t n, const uint32_t* __restrict__ perm,
                                     const float* __restrict__ x, const float* __restrict__ v, uint32_t nv, float aux0) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -1096,7 +1167,7 @@ __global__ void setup_gather_kernel(ModelDev md, uint32_t n, const uint32_t* __r
 #pragma unroll
     for (int k = 0; k < 9; ++k) st.F[k][i] = (k & 3) ? 0.f : 1.f;
   }
-  if (st.aux) st.aux[i] = aux0;
+  if (st.aux) st.aux[i] = md.smat ? md.smat[scene_of(md.sstart, nstack, s)].aux0 : aux0;
   if (st.id) st.id[i] = s;
   const uint32_t vs = nv == 1 ? 0u : s;
   md.vel_in[3 * i] = v[3 * vs];

@@ -183,15 +183,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   sc.mass_clamp = desc->mass_clamp;
   sc.boundary = desc->boundary;
   sc.floor_cells = desc->floor_cells;
-  sc.nblocks_domain = nbd;
-  uint32_t cb = 0;
-  for (int c = 0; c < 8; ++c) {
-    const int par[3] = {(c >> 2) & 1, (c >> 1) & 1, c & 1};
-    for (int a = 0; a < 3; ++a) sc.cdims[c][a] = (sc.dims[a] - par[a] + 1) / 2;
-    sc.cbase[c] = cb;
-    cb += static_cast<uint32_t>(sc.cdims[c][0]) * sc.cdims[c][1] * sc.cdims[c][2];
-  }
-  sc.cbase[8] = cb;
+  init_colour_classes(sc, 1);
 
   // Carve the scratch array (fixed layout at the maximum sizes).
   NaCarver cv{base};
@@ -278,7 +270,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
 
   // Setup: bin, sort by colour-major block index, compact, gather, identity
   // previous step, initial grid -- the sequence of ckmpm_setup.
-  setup_bin_kernel<<<(n + 255) / 256, 256, 0, st>>>(sc, n, x, sort_keys_in, sort_vals_in, d.dense_total);
+  setup_bin_kernel<<<(n + 255) / 256, 256, 0, st>>>(sc, n, x, nullptr, sort_keys_in, sort_vals_in, d.dense_total);
   NA_CUDA(cub::DeviceRadixSort::SortPairs(cub_temp, temp_bytes, sort_keys_in, sort_keys_out, sort_vals_in,
                                           sort_vals_out, static_cast<int>(n), 0, 32, st));
   compact_reduce_kernel<<<ntiles, kCompactThreads, 0, st>>>(sc, d.dense_total, d.tile_sums);
@@ -291,7 +283,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   const uint32_t n_valid = counts[1];
   const float aux0 = material->kind == CKMPM_FLUID ? material->p[3] : 0.f;
   if (n_valid > 0)
-    setup_gather_kernel<<<(n_valid + 255) / 256, 256, 0, st>>>(d, n_valid, sort_vals_out, x, v, nv, aux0);
+    setup_gather_kernel<<<(n_valid + 255) / 256, 256, 0, st>>>(d, 1, n_valid, sort_vals_out, x, v, nv, aux0);
   NA_CUDA(cudaMemcpyAsync(d.bl[1].table, d.bl[0].table, sizeof(int32_t) * nbd, cudaMemcpyDeviceToDevice, st));
   NA_CUDA(cudaMemcpyAsync(d.bl[1].start, d.bl[0].start, sizeof(uint32_t) * d.cap_slots, cudaMemcpyDeviceToDevice, st));
   NA_CUDA(cudaMemcpyAsync(d.bl[1].count, d.bl[0].count, sizeof(uint32_t) * d.cap_slots, cudaMemcpyDeviceToDevice, st));

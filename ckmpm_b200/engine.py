@@ -291,6 +291,43 @@ class Scene:
         return {"steps": int(out[0]), "lost": int(out[1]), "window_skips": int(out[2]), "status": int(out[3]),
                 "timeouts": int(out[4])}
 
+    # Launch shape, autotuner and checkpoints (no counterpart in the reference).
+    def tuning(self) -> dict:
+        t = capi.Tuning()
+        occ = (C.c_uint32 * 2)()
+        capi.check(capi.lib().ckmpm_get_tuning(self._h, C.byref(t), occ), "ckmpm_get_tuning", self._h)
+        d = t.as_dict()
+        d["max_ctas_per_sm"] = {128: int(occ[0]), 256: int(occ[1])}
+        return d
+
+    def set_tuning(self, threads: int, ctas_per_sm: int, graph_chunk: int) -> None:
+        t = capi.Tuning(threads, ctas_per_sm, graph_chunk, 0.0)
+        capi.check(capi.lib().ckmpm_set_tuning(self._h, C.byref(t)), "ckmpm_set_tuning", self._h)
+
+    def autotune(self, probe_steps: int, dt: float) -> tuple[dict, list[dict]]:
+        """Time every launch shape on this scene and keep the fastest; the
+        simulation state is left unchanged.  Returns (best, all candidates)."""
+        cap = 64
+        res = (capi.Tuning * cap)()
+        n = C.c_uint32()
+        best = capi.Tuning()
+        capi.check(capi.lib().ckmpm_autotune(self._h, probe_steps, dt, res, cap, C.byref(n), C.byref(best)),
+                   "ckmpm_autotune", self._h)
+        return best.as_dict(), [res[i].as_dict() for i in range(min(cap, n.value))]
+
+    def checkpoint_bytes(self) -> int:
+        b = C.c_uint64()
+        capi.check(capi.lib().ckmpm_checkpoint_bytes(self._h, C.byref(b)), "ckmpm_checkpoint_bytes", self._h)
+        return b.value
+
+    def checkpoint_save(self, device_ptr: int) -> None:
+        capi.check(capi.lib().ckmpm_checkpoint_save(self._h, C.c_void_p(device_ptr)), "ckmpm_checkpoint_save",
+                   self._h)
+
+    def checkpoint_restore(self, device_ptr: int) -> None:
+        capi.check(capi.lib().ckmpm_checkpoint_restore(self._h, C.c_void_p(device_ptr)),
+                   "ckmpm_checkpoint_restore", self._h)
+
     def dt_pair(self) -> tuple[float, float]:
         out = (C.c_float * 2)()
         capi.check(capi.lib().ckmpm_get_dt(self._h, out), "ckmpm_get_dt", self._h)

@@ -136,8 +136,56 @@ def small_sand(seed: int = 0, dx: float = 1 / 64, r: float = 0.1, h: float = 0.2
     return cfg, [MPMModel(rho * vol, vol, x, np.zeros((1, 3), np.float32), MPMMaterial.drucker_prager(lam, mu))]
 
 
+def batched_scenes(n_scenes: int = 256, seed: int = 0, dx: float = 1 / 64, ppc: int = 8, n_min: int = 2000,
+                   n_max: int = 200000, dt: float = 1e-4, gravity: float = -9.8) -> tuple[MPMConfig, list[MPMModel]]:
+    """Batched form: n_scenes independent scenes on a 64^3 domain (dx = 1/64,
+    sticky walls), one model each.  Per scene: target particle count
+    log-uniform in [n_min, n_max] at 8 ppc; shape box (aspect ratios
+    U(0.7, 1.4)) or sphere with equal odds; material uniform over
+    {fixed-corotated, J-fluid, Drucker-Prager}; E ~ logU[1e4, 1e6],
+    nu ~ U[0.2, 0.4]; rho 1000 (1600 for sand); v0 ~ U(-1, 1)^3 per scene; centre
+    uniform where the shape keeps one block of room inside the two-block
+    sticky margin.  The fluid's bulk modulus is E / gamma (gamma 7.15,
+    viscosity 0.1), so its acoustic stiffness bulk * gamma is the drawn E.
+    Actual counts follow the jittered lattice, not the target exactly."""
+    rng = np.random.default_rng(seed)
+    n_cells = round(1.0 / dx)
+    cfg = MPMConfig(dx=dx, domain_blocks=(n_cells // 4,) * 3, gravity=gravity, dt=dt, track_ids=True)
+    lo_free, hi_free = 12 * dx, 1.0 - 12 * dx
+    vol = dx ** 3 / ppc
+    models = []
+    for _ in range(n_scenes):
+        target = math.exp(rng.uniform(math.log(n_min), math.log(n_max)))
+        volume = target / ppc * dx ** 3
+        kind = int(rng.integers(0, 3))
+        E = math.exp(rng.uniform(math.log(1e4), math.log(1e6)))
+        nu = float(rng.uniform(0.2, 0.4))
+        v0 = rng.uniform(-1.0, 1.0, 3).astype(np.float32)
+        if rng.random() < 0.5:
+            a = rng.uniform(0.7, 1.4, 3)
+            ext = a * (volume / np.prod(a)) ** (1 / 3)
+            ext = np.minimum(ext, hi_free - lo_free - 2 * dx)
+            c = rng.uniform(lo_free + ext / 2, hi_free - ext / 2)
+            x = box_particles(c - ext / 2, c + ext / 2, dx, ppc, rng)
+        else:
+            r = min((3 * volume / (4 * math.pi)) ** (1 / 3), (hi_free - lo_free) / 2 - dx)
+            c = rng.uniform(lo_free + r, hi_free - r, 3)
+            x = sphere_particles(c, r, dx, ppc, rng)
+        if kind == 0:
+            lam, mu = compute_lame_parameters(E, nu)
+            mat, rho = MPMMaterial.fixed_corotated(lam, mu), 1000.0
+        elif kind == 1:
+            mat, rho = MPMMaterial.fluid(E / 7.15, 7.15, 0.1), 1000.0
+        else:
+            lam, mu = compute_lame_parameters(E, nu)
+            mat, rho = MPMMaterial.drucker_prager(lam, mu), 1600.0
+        models.append(MPMModel(rho * vol, vol, x, np.repeat(v0[None], len(x), 0), mat))
+    return cfg, models
+
+
 WORKLOADS = {
     "jelly_cube": jelly_cube,
     "sand_column": sand_column,
     "dam_break_mixed": dam_break_mixed,
+    "batched_256": batched_scenes,
 }

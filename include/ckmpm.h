@@ -187,6 +187,70 @@ ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, const ckmpm_ma
                                     uint32_t nsteps, float dt, void* cuda_stream, float* x_out, float* v_out,
                                     float* F_out, float* aux_out, uint32_t* n_live, const char** message);
 
+/* ---- Batched scenes.  No counterpart in the reference, which runs one scene
+ * per process (its MPMEngine is a per-GridConfig singleton,
+ * include/mpm_engine.cuh:80-90).  A batch holds nscenes independent scenes
+ * that share dx, the domain extent, gravity and the boundary rule of `desc`;
+ * each scene has one model with its own material, particle mass and volume.
+ * Every substep of every scene runs in the same launches (one persistent fused
+ * kernel and the rebinning, captured in CUDA graphs), and each scene's results
+ * equal those of the same scene run alone through ckmpm_create.  After
+ * ckmpm_add_batch, the scene calls (ckmpm_setup, ckmpm_step*, ckmpm_status_check,
+ * ckmpm_get_count, ckmpm_get_state, ckmpm_get_counters, ckmpm_destroy, ...)
+ * take the batch handle with model 0; ckmpm_get_state returns all live
+ * particles ordered by input index (ids count over the concatenated input). */
+#define CKMPM_MAX_BATCH_SCENES 65536u
+
+typedef struct ckmpm_batch_scene {
+  ckmpm_material material;
+  float mass;     /* per particle */
+  float volume;   /* per particle */
+  uint32_t n;     /* particles of this scene in the concatenated input */
+} ckmpm_batch_scene;
+
+ckmpm_status ckmpm_create_batch(const ckmpm_scene_desc* desc, uint32_t nscenes, ckmpm_scene** out);
+
+/* x, v: float3 per particle, scenes concatenated in order (host pointers). */
+ckmpm_status ckmpm_add_batch(ckmpm_scene* s, uint32_t nscenes, const ckmpm_batch_scene* scenes, const float* x,
+                             const float* v);
+
+/* ckmpm_get_blocks restricted to one scene of a batch (scene 0 for a single scene). */
+ckmpm_status ckmpm_get_blocks_in(ckmpm_scene* s, uint32_t scene, int32_t model, int32_t which, int32_t* keys,
+                                 uint32_t* counts, uint32_t cap, uint32_t* n_out);
+
+/* ---- Launch shape of the fused substep kernel.  No counterpart in the
+ * reference (fixed launch shapes, include/mpm_engine.cuh:519-866).  Results do
+ * not depend on it: the P2G sums are exact integers and the grid flushes are
+ * ordered by block colour. */
+typedef struct ckmpm_tuning {
+  uint32_t threads;      /* CTA size: 128 or 256 */
+  uint32_t ctas_per_sm;  /* resident persistent CTAs per SM, 1..occupancy */
+  uint32_t graph_chunk;  /* substeps per captured CUDA graph, even, 2..64 */
+  float probe_ms;        /* ckmpm_autotune: measured ms per substep; 0 otherwise */
+} ckmpm_tuning;
+
+ckmpm_status ckmpm_set_tuning(ckmpm_scene* s, const ckmpm_tuning* t);
+
+/* max_ctas_per_sm2 (may be NULL): occupancy limit at 128 and 256 threads. */
+ckmpm_status ckmpm_get_tuning(ckmpm_scene* s, ckmpm_tuning* t, uint32_t* max_ctas_per_sm2);
+
+/* Autotuner: times probe_steps substeps (rounded up to whole graphs) of this
+ * scene or batch at dt for every candidate launch shape (threads x CTAs per SM
+ * x graph chunk), restoring the saved state before each candidate and at the
+ * end, so the simulation is left exactly as it was; applies and returns the
+ * fastest.  results (cap entries, may be NULL) receives every candidate with
+ * its probe_ms. */
+ckmpm_status ckmpm_autotune(ckmpm_scene* s, uint32_t probe_steps, float dt, ckmpm_tuning* results, uint32_t cap,
+                            uint32_t* n_results, ckmpm_tuning* best);
+
+/* ---- Checkpoints: the whole device state of a set-up scene (particles, block
+ * lists, grids, counters and dt pair) copied to or from a caller-owned DEVICE
+ * buffer of ckmpm_checkpoint_bytes bytes, stream-ordered on the scene's
+ * stream.  No counterpart in the reference. */
+ckmpm_status ckmpm_checkpoint_bytes(ckmpm_scene* s, uint64_t* bytes);
+ckmpm_status ckmpm_checkpoint_save(ckmpm_scene* s, void* device_dst);
+ckmpm_status ckmpm_checkpoint_restore(ckmpm_scene* s, const void* device_src);
+
 /* Replaces the process exit at the end of Simulate (include/mpm_engine.cuh:908). */
 ckmpm_status ckmpm_destroy(ckmpm_scene* s);
 

@@ -12,11 +12,13 @@
 //   CKMPM_HARNESS_SCENE_JELLY : dx = 1/64,  16^3 blocks, g = -9.8, sticky walls (the built-in rule)
 //   CKMPM_HARNESS_SCENE_SAND  : dx = 1/256, 64^3 blocks, g = -9.8, slip floor at 8 cells
 //   CKMPM_HARNESS_SCENE_SLIP  : dx = 1/64,  16^3 blocks, g = -9.8, slip floor at 8 cells
+//   CKMPM_HARNESS_SCENE_DAM   : dx = 1/512, 128^3 blocks, g = -9.8, sticky walls
 // The slip floor is installed through the reference's irregular-boundary hook
 // (GetExistIrregularBoundary / ProcessGridCellVelocity, include/mpm_algorithm.cuh:795-799):
 // sticky x/z walls and ceiling two blocks deep, v_y >= 0 in cells below the floor.
 //
-// Usage: ref_<scene> <material> <params...4> <mass> <volume> <x.bin> <v.bin> <fps> <frames> <dt> <outdir> <mode>
+// Usage: ref_<scene> <manifest> <fps> <frames> <dt> <outdir> <mode>
+//   manifest: one model per line: <material> <p0> <p1> <p2> <p3> <mass> <volume> <x.bin> <v.bin>
 //   material: fc | dp | fluid; params: lambda mu 0 0 (fc/dp) or bulk gamma viscosity J0 (fluid)
 //   x.bin / v.bin: float32 xyz triples (v.bin holds 1 or n velocities)
 //   mode 0: export raw positions every frame (outdir/model_0_particle_frame_<k>.txt)
@@ -24,6 +26,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <sstream>
 #include <span>
 #include <string>
 #include <vector>
@@ -32,7 +35,12 @@
 
 namespace harness {
 
-#if defined(CKMPM_HARNESS_SCENE_SAND)
+#if defined(CKMPM_HARNESS_SCENE_DAM)
+constexpr float kDx = 1.f / 512.f;
+constexpr int kBlocks = 128;
+constexpr bool kSlipFloor = false;
+constexpr uint32_t kMaxBlocks = 650000;
+#elif defined(CKMPM_HARNESS_SCENE_SAND)
 constexpr float kDx = 1.f / 256.f;
 constexpr int kBlocks = 64;
 constexpr bool kSlipFloor = true;
@@ -119,38 +127,45 @@ std::vector<mpm::Vector<float, 3>> read_xyz(const char* path) {
 
 int main(int argc, char** argv) {
   using namespace harness;
-  if (argc != 15) {
-    std::fprintf(stderr,
-                 "usage: %s fc|dp|fluid p0 p1 p2 p3 mass volume x.bin v.bin fps frames dt outdir mode\n", argv[0]);
+  if (argc != 7) {
+    std::fprintf(stderr, "usage: %s manifest fps frames dt outdir mode\n", argv[0]);
     return 2;
   }
-  const std::string mat = argv[1];
-  const float p[4] = {std::strtof(argv[2], nullptr), std::strtof(argv[3], nullptr), std::strtof(argv[4], nullptr),
-                      std::strtof(argv[5], nullptr)};
-  const float mass = std::strtof(argv[6], nullptr), volume = std::strtof(argv[7], nullptr);
-  auto x = read_xyz(argv[8]);
-  auto v = read_xyz(argv[9]);
-  g_fps = static_cast<uint32_t>(std::strtoul(argv[10], nullptr, 10));
-  g_frames = static_cast<uint32_t>(std::strtoul(argv[11], nullptr, 10));
-  g_dt = std::strtof(argv[12], nullptr);
-  const std::string outdir = argv[13];
-  const int mode = std::atoi(argv[14]);
+  g_fps = static_cast<uint32_t>(std::strtoul(argv[2], nullptr, 10));
+  g_frames = static_cast<uint32_t>(std::strtoul(argv[3], nullptr, 10));
+  g_dt = std::strtof(argv[4], nullptr);
+  const std::string outdir = argv[5];
+  const int mode = std::atoi(argv[6]);
 
-  std::vector<mpm::MPMModelVariant> models;
   using namespace mpm;
-  if (mat == "fc") {
-    using M = MPMMaterial<MPMConstitutiveModel::kFixedCorotated>;
-    models.emplace_back(MPMModel<M>{mass, volume, std::span<const Vector<float, 3>>(x),
-                                    std::span<const Vector<float, 3>>(v), M{M::MaterialParameter_{p[0], p[1]}}});
-  } else if (mat == "dp") {
-    using M = MPMMaterial<MPMConstitutiveModel::kDruckerPragerStvkhencky>;
-    models.emplace_back(MPMModel<M>{mass, volume, std::span<const Vector<float, 3>>(x),
-                                    std::span<const Vector<float, 3>>(v), M{M::MaterialParameter_{p[0], p[1]}}});
-  } else {
-    using M = MPMMaterial<MPMConstitutiveModel::kFluid>;
-    models.emplace_back(MPMModel<M>{mass, volume, std::span<const Vector<float, 3>>(x),
-                                    std::span<const Vector<float, 3>>(v),
-                                    M{M::MaterialParameter_{p[0], p[1], p[2], p[3]}}});
+  std::vector<MPMModelVariant> models;
+  std::vector<std::vector<Vector<float, 3>>> xs, vs;  // kept alive: MPMModel copies them, spans must be valid
+  std::ifstream manifest(argv[1]);
+  std::string line;
+  while (std::getline(manifest, line)) {
+    if (line.empty()) continue;
+    std::istringstream in(line);
+    std::string mat, xf, vf;
+    float p[4], mass, volume;
+    in >> mat >> p[0] >> p[1] >> p[2] >> p[3] >> mass >> volume >> xf >> vf;
+    xs.push_back(read_xyz(xf.c_str()));
+    vs.push_back(read_xyz(vf.c_str()));
+    const auto xspan = std::span<const Vector<float, 3>>(xs.back());
+    const auto vspan = std::span<const Vector<float, 3>>(vs.back());
+    if (mat == "fc") {
+      using M = MPMMaterial<MPMConstitutiveModel::kFixedCorotated>;
+      models.emplace_back(MPMModel<M>{mass, volume, xspan, vspan, M{M::MaterialParameter_{p[0], p[1]}}});
+    } else if (mat == "dp") {
+      using M = MPMMaterial<MPMConstitutiveModel::kDruckerPragerStvkhencky>;
+      models.emplace_back(MPMModel<M>{mass, volume, xspan, vspan, M{M::MaterialParameter_{p[0], p[1]}}});
+    } else {
+      using M = MPMMaterial<MPMConstitutiveModel::kFluid>;
+      models.emplace_back(MPMModel<M>{mass, volume, xspan, vspan, M{M::MaterialParameter_{p[0], p[1], p[2], p[3]}}});
+    }
+  }
+  if (models.empty()) {
+    std::fprintf(stderr, "empty manifest\n");
+    return 2;
   }
   Config config;
   auto* engine = MPMEngine<GridConfig>::GetInstance();

@@ -28,19 +28,26 @@ def available(family: str) -> bool:
     return binary(family).exists()
 
 
-def run(family: str, model, fps: int, frames: int, dt: float, mode: int, outdir: Path | None = None,
-        timeout: float = 1800.0) -> tuple[str, Path]:
-    """Run one reference simulation of a single model; returns (stdout, outdir)."""
+def run(family: str, models, fps: int, frames: int, dt: float, mode: int, outdir: Path | None = None,
+        timeout: float = 3600.0) -> tuple[str, Path]:
+    """Run one reference simulation of one or more models; returns (stdout, outdir)."""
+    if not isinstance(models, (list, tuple)):
+        models = [models]
     outdir = Path(outdir or tempfile.mkdtemp(prefix="ckmpm_ref_"))
     outdir.mkdir(parents=True, exist_ok=True)
-    x = np.ascontiguousarray(model.particle_position, np.float32)
-    v = np.ascontiguousarray(model.particle_velocity, np.float32)
-    xf, vf = outdir / "x.bin", outdir / "v.bin"
-    x.tofile(xf)
-    v.tofile(vf)
-    p = [f"{float(t):.9g}" for t in model.material.params()]
-    cmd = [str(binary(family)), KIND_NAMES[model.material.kind_code], *p, f"{model.particle_mass:.9g}",
-           f"{model.particle_volume:.9g}", str(xf), str(vf), str(fps), str(frames), f"{dt:.9g}", str(outdir), str(mode)]
+    lines = []
+    for i, model in enumerate(models):
+        x = np.ascontiguousarray(model.particle_position, np.float32)
+        v = np.ascontiguousarray(model.particle_velocity, np.float32)
+        xf, vf = outdir / f"x{i}.bin", outdir / f"v{i}.bin"
+        x.tofile(xf)
+        v.tofile(vf)
+        p = " ".join(f"{float(t):.9g}" for t in model.material.params())
+        lines.append(f"{KIND_NAMES[model.material.kind_code]} {p} {model.particle_mass:.9g} "
+                     f"{model.particle_volume:.9g} {xf} {vf}")
+    manifest = outdir / "models.txt"
+    manifest.write_text("\n".join(lines) + "\n")
+    cmd = [str(binary(family)), str(manifest), str(fps), str(frames), f"{dt:.9g}", str(outdir), str(mode)]
     res = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
     if res.returncode != 0:
         raise RuntimeError(f"reference run failed ({res.returncode}): {res.stderr[-2000:]}")
@@ -72,17 +79,14 @@ def time_reference(family: str, cfg, models, steps: int, warmup: int) -> dict:
     "G2P2G (Cuda)") give the rate.  The loop includes the reference's per-substep
     host syncs and dt read-back, as in its stock Simulate.
     """
-    if len(models) != 1:
-        raise ValueError("the harness drives one model")
-    m = models[0]
     dt = cfg.dt
     total = warmup + steps
     fps = max(1, int(round(1.0 / (total * dt))))
-    text, _ = run(family, m, fps, 1, dt, 1)
+    text, _ = run(family, list(models), fps, 1, dt, 1)
     b = parse_benchmark(text)
     secs, _ = b["Total"]
     _, substeps = b["G2P2G (Cuda)"]
-    n = len(m.particle_position)
+    n = sum(len(m.particle_position) for m in models)
     return {"value": n * substeps / secs, "substeps": substeps, "seconds": secs, "particles": n,
             "sample": f"reference CUDA build (oracle/_ref/ref_{family}) via MPMEngine::Simulate in profile mode: "
                       f"{substeps} substeps of the {n}-particle scene, host timer around its frame loop"}

@@ -1,0 +1,160 @@
+"""Batched scenes (ckmpm_create_batch / ckmpm_add_batch) through the C ABI.
+
+A batch advances every scene in the same launches; each scene must come out
+exactly as the same scene run alone: the per-particle arithmetic is the same,
+P2G sums are exact integers and grid flushes are ordered by block colour, so
+the comparison is bitwise (x, v, F, aux, ids, block sets).  Launch shape
+(ckmpm_set_tuning, ckmpm_autotune) and checkpoint save/restore must not change
+any bit either.  Three scenes are also checked against the FP64 oracle with
+the tolerances of the plain-path parity tests.
+"""
+import numpy as np
+import pytest
+
+from ckmpm_b200 import CkmpmError, Scene, scenes
+from ckmpm_b200.batch import SceneBatch
+
+pytestmark = pytest.mark.gpu
+
+DT = 1e-4
+# Plain-path parity tolerances (the same values as the single-scene tests).
+X_TOL, F_TOL, V_REL, AUX_TOL = 2e-6, 5e-5, 1e-4, 5e-5
+
+
+def small_batch(n=9, seed=3, n_min=500, n_max=6000):
+    return scenes.batched_scenes(n_scenes=n, seed=seed, n_min=n_min, n_max=n_max)
+
+
+def run_batch(cfg, models, nsteps, tuning=None):
+    b = SceneBatch(cfg, models)
+    b.setup()
+    if tuning is not None:
+        b.set_tuning(*tuning)
+    if nsteps:
+        b.step(nsteps, DT)
+    return b
+
+
+def run_alone(cfg, model, nsteps):
+    s = Scene(cfg)
+    s.add_model(model)
+    s.setup()
+    if nsteps:
+        s.step(nsteps, DT)
+    return s
+
+
+def assert_same_state(a, b, what):
+    for name in ("id", "x", "v", "F", "aux"):
+        pa, pb = getattr(a, name), getattr(b, name)
+        assert pa.shape == pb.shape, (what, name, pa.shape, pb.shape)
+        if not np.array_equal(pa, pb):
+            d = np.abs(pa.astype(np.float64) - pb.astype(np.float64)).max()
+            raise AssertionError(f"{what}: {name} differs (max |diff| {d:.3e})")
+
+
+def test_batch_equals_each_scene_run_alone(engine_lib):
+    cfg, models = small_batch()
+    b = run_batch(cfg, models, 24)
+    st = b.state()
+    kinds = set()
+    for i, m in enumerate(models):
+        alone = run_alone(cfg, m, 24)
+        assert_same_state(b.scene_state(i, st), alone.state(0), f"scene {i} ({m.material.kind})")
+        for which in (0, 2):
+            kb, cb = b.blocks_in(i, which)
+            ka, ca = alone.blocks(-1, which)
+            assert np.array_equal(kb, ka) and np.array_equal(cb, ca), (i, which)
+        kinds.add(m.material.kind)
+        alone.close()
+    assert kinds == {"fixed_corotated", "fluid", "drucker_prager"}
+    c = b.counters()
+    assert c["steps"] == 24 and c["status"] == 0 and c["timeouts"] == 0
+
+
+def test_batch_scenes_match_oracle(engine_lib, oracle_mod):
+    cfg, models = small_batch(n=12, seed=5, n_min=800, n_max=3000)
+    picked = {}
+    for i, m in enumerate(models):
+        picked.setdefault(m.material.kind, i)
+    idx = sorted(picked.values())
+    sub = [models[i] for i in idx]
+    b = run_batch(cfg, sub, 16)
+    st = b.state()
+    for j, m in enumerate(sub):
+        o = oracle_mod.OracleScene(cfg, [m])
+        o.setup()
+        o.step(16, DT)
+        r = o.state(0)
+        g = b.scene_state(j, st)
+        alive = np.nonzero(r["alive"])[0]
+        assert np.array_equal(g.id, alive.astype(np.uint32))
+        ex = np.abs(g.x - r["x"][alive]).max(axis=1)
+        eF = np.abs(g.F - r["F"][alive]).max(axis=(1, 2))
+        ev = np.abs(g.v - r["v"][alive]).max(axis=1)
+        ea = np.abs(g.aux - r["aux"][alive])
+        vmax = np.abs(r["v"][alive]).max()
+        print(f"{m.material.kind}: n={len(alive)} |dx|={ex.max():.2e} |dF|={eF.max():.2e} |dv|={ev.max():.2e} "
+              f"(vmax {vmax:.2e}) |daux|={ea.max():.2e}")
+        if m.material.kind == "drucker_prager":
+            assert np.percentile(ev, 99) <= 0.03 * vmax + 1e-6 and ev.max() <= 0.05 * vmax + 1e-6
+            assert np.percentile(ex, 99) <= X_TOL and ex.max() <= 10 * X_TOL
+            assert np.percentile(eF, 99) <= F_TOL and np.percentile(ea, 99) <= AUX_TOL
+        else:
+            assert ex.max() <= X_TOL and eF.max() <= F_TOL and ea.max() <= AUX_TOL
+            assert ev.max() <= V_REL * vmax + 1e-6
+
+
+def test_launch_shape_does_not_change_results(engine_lib):
+    cfg, models = small_batch(n=6, seed=7)
+    ref = run_batch(cfg, models, 16).state()
+    for tuning in ((128, 1, 2), (128, 5, 32), (256, 2, 8), (256, 4, 64)):
+        got = run_batch(cfg, models, 16, tuning).state()
+        assert_same_state(got, ref, f"tuning {tuning}")
+
+
+def test_autotune_leaves_state_unchanged(engine_lib):
+    cfg, models = small_batch(n=6, seed=11)
+    ref = run_batch(cfg, models, 10).state()
+    b = SceneBatch(cfg, models)
+    b.setup()
+    b.step(4, DT)
+    best, tried = b.autotune(4, DT)
+    assert len(tried) >= 4 and all(t["probe_ms"] > 0 for t in tried)
+    assert best["probe_ms"] == min(t["probe_ms"] for t in tried)
+    assert b.tuning()["threads"] == best["threads"]
+    assert b.counters()["steps"] == 4
+    b.step(6, DT)
+    assert_same_state(b.state(), ref, "after autotune")
+
+
+def test_checkpoint_roundtrip(engine_lib):
+    import torch
+    cfg, models = small_batch(n=5, seed=13)
+    b = run_batch(cfg, models, 8)
+    buf = torch.empty(b.checkpoint_bytes(), dtype=torch.uint8, device="cuda")
+    b.checkpoint_save(buf.data_ptr())
+    b.step(7, DT)
+    first = b.state()
+    b.checkpoint_restore(buf.data_ptr())
+    assert b.counters()["steps"] == 8
+    b.step(7, DT)
+    assert_same_state(b.state(), first, "after restore")
+
+
+def test_batch_argument_errors(engine_lib):
+    cfg, models = small_batch(n=3, seed=1)
+    bad = scenes.MPMModel(models[0].particle_mass, models[0].particle_volume, models[0].particle_position,
+                          models[0].particle_velocity, scenes.MPMMaterial.fixed_corotated(1e4, 0.0))
+    with pytest.raises(CkmpmError):
+        SceneBatch(cfg, [models[0], bad])
+    b = SceneBatch(cfg, models)
+    with pytest.raises(CkmpmError):
+        b.set_tuning(64, 1, 8)
+    with pytest.raises(CkmpmError):
+        b.set_tuning(256, 1, 7)
+    with pytest.raises(CkmpmError):
+        b.step(1, DT)  # before setup
+    b.setup()
+    with pytest.raises(CkmpmError):
+        b.blocks_in(3)
