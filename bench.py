@@ -41,6 +41,8 @@ WORKLOADS = {
                        "dt=2e-5, sticky walls",
     "batched_256": "batched_256: 256 independent scenes, dx=1/64 (16^3 blocks each), 2k-200k particles log-uniform, "
                    "fixed-corotated/j-fluid/drucker-prager, box or sphere, v0~U(-1,1)^3, 8 ppc, dt=1e-4, sticky walls",
+    "diff_cube": "diff_cube: differentiable fixed-corotated cube, ~50.6k particles, 64^3 grid, per-particle log E ~ "
+                 "N(log 5e4, 0.2), nu=0.3, 200 substeps of dt=1e-4, checkpoint every 20, loss |com(T)-target|^2",
 }
 REFERENCE_FAMILY = {"sand_column": "sand", "jelly_cube": "jelly", "dam_break_mixed": "dam", "batched_256": "jelly"}
 STATE_BYTES = {0: 48, 2: 52, 3: 16}  # x + F (+ logJp) or x + J, read once and written once per substep
@@ -248,6 +250,125 @@ def workload(name: str):
     return scenes.WORKLOADS[name](track_ids=False)
 
 
+def run_diff(args, rank, world, local_rank):
+    """Differentiable form: a step is one forward + adjoint rollout (torch.autograd)
+    of the 200-substep cube; value counts the forward's particle-substeps."""
+    import torch
+
+    from ckmpm_b200 import Scene
+    from ckmpm_b200.diff import DiffRollout, rollout
+    from ckmpm_b200.engine import MPMMaterial, MPMModel
+
+    torch.cuda.set_device(local_rank)
+    from ckmpm_b200 import scenes
+    d = scenes.diff_cube()
+    cfg = d["config"]
+    cfg.device = local_rank
+    n, nsteps = len(d["x0"]), d["nsteps"]
+    steps = min(args.steps, 20)
+    sim = DiffRollout(cfg, n, d["mass"], d["volume"], d["nu"], nsteps, d["dt"], d["checkpoint_every"])
+    x0 = torch.tensor(d["x0"], device="cuda")
+    v0 = torch.tensor(d["v0"], device="cuda")
+    lE = torch.tensor(d["logE"], device="cuda")
+    target = torch.tensor(d["target"], device="cuda")
+
+    def train_step():
+        v = v0.clone().requires_grad_()
+        e = lE.clone().requires_grad_()
+        xT, _ = rollout(sim, x0, v, e)
+        loss = ((xT.mean(0) - target) ** 2).sum()
+        loss.backward()
+        return loss, v.grad, e.grad
+
+    for _ in range(max(args.warmup, 3)):
+        train_step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(device_uuid(local_rank))
+    sampler.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    fwd_ms, bwd_ms = [], []
+    ev0.record()
+    for _ in range(steps):
+        loss, gv, ge = train_step()
+        f, b = sim.timing_ms()
+        fwd_ms.append(f)
+        bwd_ms.append(b)
+    ev1.record()
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    clocks = sampler.stop()
+    fwd = statistics.median(fwd_ms)
+    bwd = statistics.median(bwd_ms)
+    # The plain engine's forward on the same cube (uniform E) for the per-substep comparison.
+    lam, mu = (np.exp(np.log(5e4)) * 0.3 / (1.3 * 0.4), np.exp(np.log(5e4)) / 2.6)
+    s = Scene(cfg)
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    s.add_model(MPMModel(d["mass"], d["volume"], d["x0"], d["v0"], MPMMaterial.fixed_corotated(lam, mu)))
+    s.setup()
+    s.step(8, d["dt"])
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step_async(nsteps, d["dt"])
+    e1.record(stream)
+    e1.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    s.close()
+    # Gradient check: d loss / d v0 along each axis (every particle's v0 moved
+    # together), FP64 central differences through the oracle.
+    grad = gv.detach().cpu().numpy().astype(np.float64)
+    gradcheck = {}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        E = np.exp(d["logE"].astype(np.float64))
+        lam_p, mu_p = E * d["nu"] / ((1 + d["nu"]) * (1 - 2 * d["nu"])), E / (2 * (1 + d["nu"]))
+
+        def oracle_loss(v):
+            m = MPMModel(d["mass"], d["volume"], d["x0"], v.astype(np.float32), MPMMaterial.fixed_corotated(1.0, 1.0))
+            o = O.OracleScene(cfg, [m])
+            o.set_state(0, x=d["x0"].astype(np.float64))
+            o.set_initial_velocity(0, v)
+            o.set_lame(0, lam_p, mu_p)
+            o.setup()
+            o.step(nsteps, d["dt"])
+            x = o.state(0)["x"]
+            o.close()
+            return float(((x.mean(0) - d["target"].astype(np.float64)) ** 2).sum())
+
+        eps = 1e-4
+        for a, name in enumerate("xyz"):
+            vp = d["v0"].astype(np.float64).copy()
+            vm = vp.copy()
+            vp[:, a] += eps
+            vm[:, a] -= eps
+            fd = (oracle_loss(vp) - oracle_loss(vm)) / (2 * eps)
+            ad = float(grad[:, a].sum())
+            gradcheck[f"v0_{name}"] = {"fd_fp64": fd, "adjoint_fp32": ad, "rel_err": abs(fd - ad) / max(abs(fd), 1e-30)}
+    line = {
+        "metric": METRIC, "value": n * nsteps / (fwd / 1e3), "unit": METRIC, "n_gpus": world, "steps": steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded cube, numpy PCG64 seed 0)",
+        "config": {"workload": WORKLOADS["diff_cube"], "particles": n, "substeps": nsteps,
+                   "checkpoint_every": d["checkpoint_every"], "parallelism": "single GPU",
+                   "step": "one forward + adjoint rollout through torch.autograd",
+                   "l2": "working set ~60 MB < L2; each step re-runs the whole rollout"},
+        "forward_ms": fwd, "adjoint_ms": bwd, "train_step_ms": ms,
+        "fwd_adj_over_fwd": (fwd + bwd) / fwd,
+        "plain_forward_ms": plain_ms, "fwd_adj_over_plain_forward": (fwd + bwd) / plain_ms,
+        "train_step_particle_substeps_per_s": n * nsteps / (ms / 1e3),
+        "gradcheck": gradcheck, "loss": float(loss.item()), "clocks": clocks,
+        "gpu_launches": 4 + 2 * nsteps + 1 + (2 * nsteps + 2 * nsteps) + 4,
+        "e2e": {"value": n * nsteps / (ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8, "includes": "torch tensors already on the device; loss read back per step"},
+    }
+    sim.close()
+    return line
+
+
 def run_batched(args, rank, world, local_rank):
     """Batched form: this rank's shard of the 256 scenes in one SceneBatch
     (one persistent fused launch + rebinning per substep, CUDA graphs), launch
@@ -347,11 +468,18 @@ def run_batched(args, rank, world, local_rank):
     b2.set_stream(stream.cuda_stream)
     b2.setup()
     exports = 0
-    for k in range(args.steps):
-        b2.step(1, dt)
-        if (k + 1) % args.e2e_frame == 0:
-            b2.state()
-            exports += 1
+    xb = np.zeros((sum(len(m.particle_position) for m in sub), 3), np.float32)
+    from ckmpm_b200 import _capi as capi
+    import ctypes as C
+    nout = C.c_uint32()
+    done = 0
+    while done < args.steps:
+        k = min(args.e2e_frame, args.steps - done)
+        b2.step(k, dt)
+        capi.check(capi.lib().ckmpm_get_state(b2._h, 0, capi.fptr(xb), None, None, None, None, len(xb),
+                                              C.byref(nout)), "ckmpm_get_state", b2._h)
+        exports += 1
+        done += k
     e1.record(stream)
     e1.synchronize()
     e2e_ms, _ = reduce_over_ranks(e0.elapsed_time(e1), 0.0)
@@ -359,9 +487,10 @@ def run_batched(args, rank, world, local_rank):
     n_in = sum(len(m.particle_position) for m in sub)
     e2e = {"value": total_live * args.steps / (e2e_ms / 1e3), "unit": METRIC,
            "h2d_bytes_per_step": n_in * 24 / args.steps,
-           "d2h_bytes_per_step": 64 + exports * n_live * (12 + 12 + 36 + 4 + 4) / args.steps,
-           "includes": "batch construction and setup (upload of x, v; binning; initial grid), every substep's "
-                       f"status read, a full state export every {args.e2e_frame} substeps"}
+           "d2h_bytes_per_step": exports * (n_live * 12 + 64) / args.steps,
+           "includes": "batch construction and setup (upload of x, v; binning; initial grid); frames of "
+                       f"{args.e2e_frame} substeps, each followed by the status read and a position export in "
+                       "input order"}
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -458,13 +587,15 @@ def run_ours(args, rank, world, local_rank):
     import ctypes as C
     L = capi.lib()
     nout = C.c_uint32()
-    for k in range(args.steps):
-        s2.step(1, dt)  # one substep + device->host read of its status word
-        if (k + 1) % args.e2e_frame == 0:
-            for i in range(len(models)):
-                capi.check(L.ckmpm_get_state(s2._h, i, capi.fptr(xbuf), None, None, None, None, n_total,
-                                             C.byref(nout)), "ckmpm_get_state", s2._h)
-            exports += 1
+    done = 0
+    while done < args.steps:
+        k = min(args.e2e_frame, args.steps - done)
+        s2.step(k, dt)  # one frame of substeps, then the device status word read back
+        for i in range(len(models)):
+            capi.check(L.ckmpm_get_state(s2._h, i, capi.fptr(xbuf), None, None, None, None, n_total,
+                                         C.byref(nout)), "ckmpm_get_state", s2._h)
+        exports += 1
+        done += k
     e1.record(stream)
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
@@ -475,9 +606,9 @@ def run_ours(args, rank, world, local_rank):
     s2.close()
     e2e = {"value": world * n_live * args.steps / (e2e_ms / 1e3), "unit": METRIC,
            "h2d_bytes_per_step": (n_total * 12 + 12) / args.steps,
-           "d2h_bytes_per_step": 64 + exports * (n_live * 12 + 4) / args.steps,
-           "includes": "setup (upload of x, v; binning; initial grid), every substep's status read, "
-                       f"a position export every {args.e2e_frame} substeps"}
+           "d2h_bytes_per_step": exports * (n_live * 12 + 64) / args.steps,
+           "includes": "setup (upload of x, v; binning; initial grid); frames of "
+                       f"{args.e2e_frame} substeps, each followed by the status read and a position export"}
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -496,6 +627,9 @@ def run_reference(args, rank, world):
     """Reference arm: the reference CUDA build driven through its own MPMEngine API
     (oracle/_ref, built from the reference's headers) when present, otherwise the
     FP64 port of its algorithm on a bounded sample."""
+    if args.workload == "diff_cube":
+        return {"impl": "reference", "unavailable": "the reference has no differentiable form (no adjoint of its "
+                                                    "substep, no autograd binding)"}
     cfg, models = workload(args.workload)
     family = REFERENCE_FAMILY.get(args.workload)
     harness = ROOT / "oracle" / "_ref" / f"ref_{family}"
@@ -559,6 +693,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.workload == "batched_256":
         line = run_batched(args, rank, world, local_rank)
+    elif args.workload == "diff_cube":
+        line = run_diff(args, rank, world, local_rank)
+        print(json.dumps(line), flush=True)
+        return
     else:
         line = run_ours(args, rank, world, local_rank)
     if rank == 0:

@@ -41,8 +41,10 @@ struct ModelHost {
   float* oF = nullptr;
   float* oaux = nullptr;
   uint32_t* oid = nullptr;
-  std::vector<float> hx, hv, hF, ha;
-  std::vector<uint32_t> hid;
+  uint32_t* oflag = nullptr;  // input-order export: live flags by id, then their exclusive scan
+  uint32_t* opos = nullptr;
+  void* oscan = nullptr;
+  size_t oscan_bytes = 0;
   // Batch: per-scene materials and input offsets (host copies and device arrays).
   std::vector<SceneMat> smat;
   std::vector<uint32_t> sstart;
@@ -698,70 +700,45 @@ ckmpm_status ckmpm_get_state(ckmpm_scene* s, int32_t model, float* x, float* v, 
   if (cap < n) return fail(s, CKMPM_ERR_NOT_FOUND, "output capacity too small");
   if (n == 0) return CKMPM_OK;
   const size_t cap_p = m.dev.cap_particles;
+  const bool sorted = m.dev.track_ids != 0;
   if (!m.ox) {
     CK_CUDA(s, dalloc(s, &m.ox, 3 * cap_p));
     CK_CUDA(s, dalloc(s, &m.ov, 3 * cap_p));
     CK_CUDA(s, dalloc(s, &m.oF, 9 * cap_p));
     CK_CUDA(s, dalloc(s, &m.oaux, cap_p));
     CK_CUDA(s, dalloc(s, &m.oid, cap_p));
-  }
-  const bool sorted = m.dev.track_ids != 0;
-  const bool want_id = sorted || id;
-  probe_kernel<kProbeThreads><<<s->sm_count * 4, kProbeThreads, kSmemVTile, s->stream>>>(
-      s->sc, m.dev, s->grid, s->scal, x ? m.ox : nullptr, v ? m.ov : nullptr,
-      (F && m.mat.kind != CKMPM_FLUID) ? m.oF : nullptr, (aux && m.mat.kind != CKMPM_FIXED_COROTATED) ? m.oaux : nullptr,
-      want_id ? m.oid : nullptr);
-  CK_CUDA(s, cudaGetLastError());
-  // Copy straight into the caller's arrays when no reordering is needed.
-  auto fetch = [&](void* dst_user, std::vector<float>& tmp, const float* src, size_t width) -> cudaError_t {
-    if (!dst_user) return cudaSuccess;
-    void* dst = dst_user;
     if (sorted) {
-      tmp.resize(width * n);
-      dst = tmp.data();
+      CK_CUDA(s, dalloc(s, &m.oflag, cap_p));
+      CK_CUDA(s, dalloc(s, &m.opos, cap_p));
+      CK_CUDA(s, cub::DeviceScan::ExclusiveSum(nullptr, m.oscan_bytes, m.oflag, m.opos, static_cast<int>(cap_p),
+                                               s->stream));
+      unsigned char* t = nullptr;
+      CK_CUDA(s, dalloc(s, &t, m.oscan_bytes));
+      m.oscan = t;
     }
-    return cudaMemcpyAsync(dst, src, sizeof(float) * width * n, cudaMemcpyDeviceToHost, s->stream);
-  };
-  CK_CUDA(s, fetch(x, m.hx, m.ox, 3));
-  CK_CUDA(s, fetch(v, m.hv, m.ov, 3));
-  if (F && m.mat.kind != CKMPM_FLUID) CK_CUDA(s, fetch(F, m.hF, m.oF, 9));
-  if (aux && m.mat.kind != CKMPM_FIXED_COROTATED) CK_CUDA(s, fetch(aux, m.ha, m.oaux, 1));
-  if (want_id) {
-    m.hid.resize(n);
-    CK_CUDA(s, cudaMemcpyAsync(m.hid.data(), m.oid, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s->stream));
   }
-  CK_CUDA(s, cudaStreamSynchronize(s->stream));
-  if (F && m.mat.kind == CKMPM_FLUID)
-    for (uint32_t j = 0; j < n; ++j)
-      for (int k = 0; k < 9; ++k) F[9 * j + k] = (k & 3) ? 0.f : 1.f;
-  if (aux && m.mat.kind == CKMPM_FIXED_COROTATED) std::fill(aux, aux + n, 0.f);
-  // Batch: a fluid scene's particles carry no F (reported as I) and a
-  // fixed-corotated scene's no aux (reported as 0).
-  auto scene_kind = [&](uint32_t pid) {
-    const auto it = std::upper_bound(m.sstart.begin(), m.sstart.end(), pid);
-    return m.skind[static_cast<size_t>(it - m.sstart.begin()) - 1];
-  };
+  const dim3 pg(s->sm_count * 4), pb(kProbeThreads);
+  const uint32_t* dest = nullptr;
   if (sorted) {
-    std::vector<uint32_t> order(n);
-    for (uint32_t i = 0; i < n; ++i) order[i] = i;
-    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return m.hid[a] < m.hid[b]; });
-    for (uint32_t j = 0; j < n; ++j) {
-      const uint32_t i = order[j];
-      if (x) std::memcpy(x + 3 * j, &m.hx[3 * i], sizeof(float) * 3);
-      if (v) std::memcpy(v + 3 * j, &m.hv[3 * i], sizeof(float) * 3);
-      if (F && m.mat.kind != CKMPM_FLUID) std::memcpy(F + 9 * j, &m.hF[9 * i], sizeof(float) * 9);
-      if (aux && m.mat.kind != CKMPM_FIXED_COROTATED) aux[j] = m.ha[i];
-      if (id) id[j] = m.hid[i];
-      if (m.mat.kind == kMixedKind) {
-        const int32_t k = scene_kind(m.hid[i]);
-        if (F && k == CKMPM_FLUID)
-          for (int c = 0; c < 9; ++c) F[9 * j + c] = (c & 3) ? 0.f : 1.f;
-        if (aux && k == CKMPM_FIXED_COROTATED) aux[j] = 0.f;
-      }
-    }
-  } else if (id) {
-    std::memcpy(id, m.hid.data(), sizeof(uint32_t) * n);
+    // ids in block order, then the position of each live id in input order
+    probe_kernel<kProbeThreads><<<pg, pb, kSmemVTile, s->stream>>>(s->sc, m.dev, s->grid, s->scal, nullptr, nullptr,
+                                                                 nullptr, nullptr, m.oid, nullptr);
+    CK_CUDA(s, cudaMemsetAsync(m.oflag, 0, sizeof(uint32_t) * cap_p, s->stream));
+    mark_ids_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(n, m.oid, m.oflag, static_cast<uint32_t>(cap_p));
+    size_t tb = m.oscan_bytes;
+    CK_CUDA(s, cub::DeviceScan::ExclusiveSum(m.oscan, tb, m.oflag, m.opos, static_cast<int>(cap_p), s->stream));
+    dest = m.opos;
   }
+  probe_kernel<kProbeThreads><<<pg, pb, kSmemVTile, s->stream>>>(s->sc, m.dev, s->grid, s->scal, x ? m.ox : nullptr,
+                                                               v ? m.ov : nullptr, F ? m.oF : nullptr,
+                                                               aux ? m.oaux : nullptr, id ? m.oid : nullptr, dest);
+  CK_CUDA(s, cudaGetLastError());
+  if (x) CK_CUDA(s, cudaMemcpyAsync(x, m.ox, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (v) CK_CUDA(s, cudaMemcpyAsync(v, m.ov, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (F) CK_CUDA(s, cudaMemcpyAsync(F, m.oF, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost, s->stream));
+  if (aux) CK_CUDA(s, cudaMemcpyAsync(aux, m.oaux, sizeof(float) * n, cudaMemcpyDeviceToHost, s->stream));
+  if (id) CK_CUDA(s, cudaMemcpyAsync(id, m.oid, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s->stream));
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
   return CKMPM_OK;
 }
 

@@ -1187,12 +1187,15 @@ __global__ void setup_identity_kernel(BlockListDev cur, BlockListDev prev) {
 }
 
 // ------------------------------------------------------------------ probe / export
-// Gathers the current state into block order (x, F, aux, id) and interpolates
-// v at each particle from the current grid with the grid update applied, as
-// the next G2P will (include/mpm_algorithm.cuh:1306-1331).
+// Gathers the current state (x, F, aux, id) and interpolates v at each
+// particle from the current grid with the grid update applied, as the next
+// G2P will (include/mpm_algorithm.cuh:1306-1331).  Output slot: block order,
+// or dest[id] when dest is given (ids tracked).  Materials without F write
+// the identity, without aux zero (per scene in a batch).
 template <int NT>
 __global__ void __launch_bounds__(NT) probe_kernel(SceneDev sc, ModelDev md, GridDev gd, Scalars* scal, float* ox,
-                                                  float* ov, float* oF, float* oaux, uint32_t* oid) {
+                                                  float* ov, float* oF, float* oaux, uint32_t* oid,
+                                                  const uint32_t* __restrict__ dest) {
   extern __shared__ __align__(16) unsigned char smem[];
   float4* vtile = reinterpret_cast<float4*>(smem);
   __shared__ SharedSmall sh;
@@ -1207,12 +1210,13 @@ __global__ void __launch_bounds__(NT) probe_kernel(SceneDev sc, ModelDev md, Gri
     const int4 key = cur.keys[item];
     const uint32_t start = cur.start[item];
     const uint32_t n = cur.count[item];
+    const int kind = md.smat ? md.smat[key.w].kind : md.mat.kind;
     if (threadIdx.x < 32)
       incoming_groups(sc, prev, key, sh.off, sh.idx, sh.src);
     else if (threadIdx.x < 40)
       window_blocks(sc, gd.stamp[parity], step, key, sh.blk, threadIdx.x - 32);
     __syncthreads();
-    load_velocity_tile<NT>(sc, gd.grid[parity], sh.blk, key, dt, vtile);
+    if (ov) load_velocity_tile<NT>(sc, gd.grid[parity], sh.blk, key, dt, vtile);
     __syncthreads();
     const uint32_t nn = min(n, sh.off[27]);
     for (uint32_t q = threadIdx.x; q < nn; q += NT) {
@@ -1223,19 +1227,21 @@ __global__ void __launch_bounds__(NT) probe_kernel(SceneDev sc, ModelDev md, Gri
         set_status(scal, kStatusConsistency);
         iin = 0;
       }
-      const uint32_t o = start + q;
+      const uint32_t pid = sin.id ? sin.id[iin] : start + q;
+      const uint32_t o = dest ? dest[pid] : start + q;
       const float x[3] = {sin.x[0][iin], sin.x[1][iin], sin.x[2][iin]};
       if (ox) {
         ox[3 * o] = x[0];
         ox[3 * o + 1] = x[1];
         ox[3 * o + 2] = x[2];
       }
-      if (oF && sin.F[0]) {
+      if (oF) {
+        const bool hasF = kind != kFluid && sin.F[0];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) oF[9 * o + k] = sin.F[k][iin];
+        for (int k = 0; k < 9; ++k) oF[9 * o + k] = hasF ? sin.F[k][iin] : ((k & 3) ? 0.f : 1.f);
       }
-      if (oaux && sin.aux) oaux[o] = sin.aux[iin];
-      if (oid) oid[o] = sin.id ? sin.id[iin] : o;
+      if (oaux) oaux[o] = (kind != kFixedCorotated && sin.aux) ? sin.aux[iin] : 0.f;
+      if (oid) oid[o] = pid;
       if (ov) {
         const float xs[3] = {x[0] * sc.inv_dx, x[1] * sc.inv_dx, x[2] * sc.inv_dx};
         float v[3], C[9];
@@ -1248,6 +1254,15 @@ __global__ void __launch_bounds__(NT) probe_kernel(SceneDev sc, ModelDev md, Gri
     }
     __syncthreads();
   }
+}
+
+// Input-order export: flag[id] = 1 for every live particle (ids from the
+// block-order probe); an exclusive scan of the flags gives each live id its
+// position among the live particles in input order.
+__global__ void mark_ids_kernel(uint32_t n, const uint32_t* __restrict__ ids, uint32_t* __restrict__ flag,
+                               uint32_t cap) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && ids[i] < cap) flag[ids[i]] = 1u;
 }
 
 // ------------------------------------------------------------------ debug hook

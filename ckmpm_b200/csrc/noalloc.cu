@@ -327,7 +327,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   int sms = 0;
   NA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, desc->device));
   probe_kernel<kProbeThreads><<<sms * 4, kProbeThreads, kSmemVTile, st>>>(sc, d, grid, scal, ex, ev, hasF ? eF : nullptr,
-                                                                         hasAux ? ea : nullptr, eid);
+                                                                         hasAux ? ea : nullptr, eid, nullptr);
   NA_CUDA(cudaStreamSynchronize(st));
   if (x_out || v_out || F_out || aux_out) {
     noalloc_fill_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, x_out, v_out, F_out, aux_out);

@@ -183,6 +183,27 @@ def batched_scenes(n_scenes: int = 256, seed: int = 0, dx: float = 1 / 64, ppc: 
     return cfg, models
 
 
+def diff_cube(seed: int = 0, dx: float = 1 / 64, half: float = 0.1445, ppc: int = 8, E: float = 5e4,
+              log_e_sigma: float = 0.2, nu: float = 0.3, rho: float = 1000.0, nsteps: int = 200, dt: float = 1e-4,
+              checkpoint_every: int = 20, gravity: float = -9.8) -> dict:
+    """Differentiable form: fixed-corotated cube of ~50k particles (8 ppc, side
+    2 * half centred at 0.5) on a 64^3 grid with sticky walls; per-particle
+    log E ~ N(log E, log_e_sigma), nu = 0.3; v0 ~ U(-0.5, 0.5)^3 shared by all
+    particles (learnable per particle); 200 substeps of dt = 1e-4, a checkpoint
+    every 20; target = initial centre of mass + U(-0.05, 0.05)^3."""
+    rng = np.random.default_rng(seed)
+    x = box_particles((0.5 - half,) * 3, (0.5 + half,) * 3, dx, ppc, rng)
+    n = len(x)
+    logE = (math.log(E) + log_e_sigma * rng.standard_normal(n)).astype(np.float32)
+    v0 = np.repeat(rng.uniform(-0.5, 0.5, (1, 3)), n, 0).astype(np.float32)
+    target = (x.astype(np.float64).mean(0) + rng.uniform(-0.05, 0.05, 3)).astype(np.float32)
+    n_cells = round(1.0 / dx)
+    cfg = MPMConfig(dx=dx, domain_blocks=(n_cells // 4,) * 3, gravity=gravity, dt=dt, track_ids=True)
+    vol = dx ** 3 / ppc
+    return {"config": cfg, "x0": x, "v0": v0, "logE": logE, "target": target, "mass": rho * vol, "volume": vol,
+            "nu": nu, "nsteps": nsteps, "dt": dt, "checkpoint_every": checkpoint_every}
+
+
 WORKLOADS = {
     "jelly_cube": jelly_cube,
     "sand_column": sand_column,

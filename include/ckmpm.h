@@ -251,6 +251,31 @@ ckmpm_status ckmpm_checkpoint_bytes(ckmpm_scene* s, uint64_t* bytes);
 ckmpm_status ckmpm_checkpoint_save(ckmpm_scene* s, void* device_dst);
 ckmpm_status ckmpm_checkpoint_restore(ckmpm_scene* s, const void* device_src);
 
+/* ---- Differentiable rollout.  No counterpart in the reference.  A
+ * fixed-corotated model of n particles (mass, volume, Poisson ratio nu; a
+ * per-particle Young's modulus given as log E) advanced nsteps substeps of dt
+ * on the dense grid of desc's domain (5..64 blocks per axis; the first substep
+ * advects with dt = 0, as ckmpm_step after setup).  ckmpm_diff_forward keeps a
+ * checkpoint every checkpoint_every substeps; ckmpm_diff_backward recomputes
+ * one segment at a time from its checkpoint and runs the hand-written adjoint
+ * of P2G, the grid update, G2P and the SVD-based stress.  All array arguments
+ * are DEVICE pointers, float32, particle-major: x0, v0, xT, gxT, gx0, gv0 are
+ * n x 3; FT, gFT are n x 3 x 3 row-major; logE, glogE are n.  Work is ordered
+ * after, and results are visible to, cuda_stream (NULL: the legacy stream).
+ * backward gives the gradients of <gxT, xT> + <gFT, FT> for the last forward. */
+typedef struct ckmpm_diff ckmpm_diff;
+
+ckmpm_status ckmpm_diff_create(const ckmpm_scene_desc* desc, uint32_t n, float mass, float volume, float nu,
+                               uint32_t nsteps, float dt, uint32_t checkpoint_every, ckmpm_diff** out);
+ckmpm_status ckmpm_diff_forward(ckmpm_diff* d, const float* x0, const float* v0, const float* logE, float* xT,
+                                float* FT, void* cuda_stream);
+ckmpm_status ckmpm_diff_backward(ckmpm_diff* d, const float* gxT, const float* gFT, float* gx0, float* gv0,
+                                 float* glogE, void* cuda_stream);
+/* Device time (ms) of the last forward [0] and backward [1]; generation counts forwards. */
+ckmpm_status ckmpm_diff_timing(ckmpm_diff* d, float* ms_out2, uint64_t* generation);
+const char* ckmpm_diff_last_error(const ckmpm_diff* d);
+ckmpm_status ckmpm_diff_destroy(ckmpm_diff* d);
+
 /* Replaces the process exit at the end of Simulate (include/mpm_engine.cuh:908). */
 ckmpm_status ckmpm_destroy(ckmpm_scene* s);
 

@@ -61,6 +61,7 @@ struct Model {
   int n = 0;
   std::vector<double> x, F, aux;  // aux: J (fluid) or logJp (DP)
   std::vector<double> v0;         // initial velocities (n or 1 entries of 3)
+  std::vector<double> plam, pmu;  // optional per-particle Lame parameters (fixed-corotated)
   std::vector<uint8_t> alive;
   std::vector<uint8_t> skipped;   // P2G skipped in the last step (window escape)
 };
@@ -452,7 +453,7 @@ void substep(Scene& s, double next_dt) {
         double* F = &m.F[9 * p];
         matmul3(dW, F, F);
         if (m.kind == 0)
-          stress_fc(m.p[0], m.p[1], F, tau);
+          stress_fc(m.plam.empty() ? m.p[0] : m.plam[p], m.pmu.empty() ? m.p[1] : m.pmu[p], F, tau);
         else
           stress_dp(m.p[0], m.p[1], F, &m.aux[p], tau);
       }
@@ -542,6 +543,32 @@ int oracle_add_model(void* h, int kind, const double* params, int n, const float
 }
 
 // Initial grid: mass and momentum only (mpm_algorithm.cuh:872-947); first dt is 0.
+// Per-particle Lame parameters of a fixed-corotated model (the differentiable
+// form's per-particle Young's modulus); NULL restores the model's own.
+int oracle_set_lame(void* h, int model, const double* lam, const double* mu) {
+  Scene* s = static_cast<Scene*>(h);
+  if (model < 0 || model >= static_cast<int>(s->models.size())) return -1;
+  Model& m = s->models[model];
+  if (!lam || !mu) {
+    m.plam.clear();
+    m.pmu.clear();
+    return 0;
+  }
+  m.plam.assign(lam, lam + m.n);
+  m.pmu.assign(mu, mu + m.n);
+  return 0;
+}
+
+// Initial velocities in double precision (nv = 1 or n rows), before oracle_setup.
+int oracle_set_velocity(void* h, int model, const double* v, int nv) {
+  Scene* s = static_cast<Scene*>(h);
+  if (model < 0 || model >= static_cast<int>(s->models.size())) return -1;
+  Model& m = s->models[model];
+  if (nv != 1 && nv != m.n) return -1;
+  m.v0.assign(v, v + 3 * static_cast<size_t>(nv));
+  return 0;
+}
+
 int oracle_setup(void* h) {
   Scene* s = static_cast<Scene*>(h);
   s->grid.clear();

@@ -35,6 +35,8 @@ def lib() -> C.CDLL:
         L.oracle_destroy.argtypes = [C.c_void_p]
         L.oracle_add_model.argtypes = [C.c_void_p, C.c_int, d, C.c_int, f, f, C.c_int, C.c_double, C.c_double]
         L.oracle_setup.argtypes = [C.c_void_p]
+        L.oracle_set_lame.argtypes = [C.c_void_p, C.c_int, d, d]
+        L.oracle_set_velocity.argtypes = [C.c_void_p, C.c_int, d, C.c_int]
         L.oracle_step.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.oracle_step_frame.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]
         L.oracle_get_state.argtypes = [C.c_void_p, C.c_int, d, d, d, d, C.POINTER(C.c_uint8)]
@@ -83,6 +85,21 @@ class OracleScene:
                                      m.particle_mass, m.particle_volume)
         self.n.append(len(x))
         return idx
+
+    def set_lame(self, model: int, lam, mu) -> None:
+        """Per-particle Lame parameters for a fixed-corotated model (None restores the model's own)."""
+        if lam is None:
+            rc = lib().oracle_set_lame(self._h, model, None, None)
+        else:
+            lam = np.ascontiguousarray(lam, np.float64)
+            mu = np.ascontiguousarray(mu, np.float64)
+            rc = lib().oracle_set_lame(self._h, model, _d(lam), _d(mu))
+        assert rc == 0
+
+    def set_initial_velocity(self, model: int, v) -> None:
+        """Initial velocities in double precision (1 or n rows); call before setup()."""
+        v = np.ascontiguousarray(v, np.float64).reshape(-1, 3)
+        assert lib().oracle_set_velocity(self._h, model, _d(v), len(v)) == 0
 
     def setup(self):
         lib().oracle_setup(self._h)
