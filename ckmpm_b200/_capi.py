@@ -41,7 +41,8 @@ EXPORTED = (
     "ckmpm_step_profiled", "ckmpm_debug_constitutive", "ckmpm_destroy", "ckmpm_last_error",
     "ckmpm_version", "ckmpm_simulate_noalloc", "ckmpm_create_batch", "ckmpm_add_batch", "ckmpm_get_blocks_in",
     "ckmpm_set_tuning", "ckmpm_get_tuning", "ckmpm_autotune", "ckmpm_checkpoint_bytes", "ckmpm_checkpoint_save",
-    "ckmpm_checkpoint_restore",
+    "ckmpm_checkpoint_restore", "ckmpm_diff_create", "ckmpm_diff_forward", "ckmpm_diff_backward", "ckmpm_diff_timing",
+    "ckmpm_diff_last_error", "ckmpm_diff_destroy",
 )
 
 MAX_BATCH_SCENES = 65536
@@ -136,8 +137,9 @@ def lib() -> C.CDLL:
         L.ckmpm_version.restype = C.c_char_p
         for name in EXPORTED:
             fn = getattr(L, name)
-            if name not in ("ckmpm_last_error", "ckmpm_version"):
+            if name not in ("ckmpm_last_error", "ckmpm_version", "ckmpm_diff_last_error"):
                 fn.restype = C.c_int
+        L.ckmpm_diff_last_error.restype = C.c_char_p
         _lib = L
     return _lib
 
