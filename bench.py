@@ -502,7 +502,7 @@ def run_batched(args, rank, world, local_rank):
                    "tuning": best, "tuning_candidates": len(tried),
                    "l2": "particle state ~560 MB > 126 MB L2: no flush"},
         "roofline": roofline, "e2e": e2e, "clocks": clocks,
-        "gpu_launches": 1 + args.steps * 4,
+        "gpu_launches": 1 + args.steps * 5,
     }
     if looped:
         line["looped_plain"] = looped
@@ -618,7 +618,7 @@ def run_ours(args, rank, world, local_rank):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "particle state ~190 MB > 126 MB L2: no flush"},
         "roofline": roofline, "e2e": e2e, "clocks": clocks,
-        "gpu_launches": 1 + args.steps * (3 * len(models) + 1),
+        "gpu_launches": 1 + args.steps * (3 * len(models) + 2),
     }
     return line
 

@@ -168,9 +168,20 @@ __global__ void set_frame_end_kernel(Scalars* scal, double frame_time) {
   if (threadIdx.x == 0) scal->frame_end = scal->time + frame_time;
 }
 
+// Zero (and stamp with step + epoch_offset) the blocks of grid[grid_parity]
+// that a substep over block lists bl[list_parity] deposits into.
+cudaError_t launch_zero(ckmpm_scene* s, int list_parity, int grid_parity, int32_t epoch_offset) {
+  for (auto& m : s->models)
+    zero_windows_kernel<<<s->sm_count * 4, 256, 0, s->stream>>>(s->sc, m.dev.bl[list_parity],
+                                                                 s->grid.grid[grid_parity],
+                                                                 s->grid.stamp[grid_parity], s->scal, epoch_offset);
+  return cudaGetLastError();
+}
+
 // Enqueue one substep for every model.  The compaction of each model writes
 // the block list the fused kernel did not read: that of the other parity.
-
+// Once every model's fused kernel has read grid[parity], its blocks that the
+// next substep deposits into are zeroed for it (epoch step + 2).
 cudaError_t enqueue_substep(ckmpm_scene* s, int parity_of_step) {
   for (auto& m : s->models) {
     cudaError_t e = launch_fused_any(s, m);
@@ -178,6 +189,8 @@ cudaError_t enqueue_substep(ckmpm_scene* s, int parity_of_step) {
     e = launch_compact(s, m, m.dev.bl[parity_of_step ^ 1]);
     if (e != cudaSuccess) return e;
   }
+  cudaError_t e = launch_zero(s, parity_of_step ^ 1, parity_of_step, 2);
+  if (e != cudaSuccess) return e;
   end_substep_kernel<<<1, 32, 0, s->stream>>>(s->scal);
   return cudaGetLastError();
 }
@@ -449,8 +462,15 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
   CK_CUDA(s, cudaSetDevice(s->desc.device));
   const uint32_t nbd = s->sc.nblocks_domain;
   uint32_t lost_at_setup = 0;
+  // The grid's fixed-point unit: 2^-36 of the heaviest model's particle mass;
+  // lighter models' sums are rescaled when they are added.  A batch uses each
+  // scene's own mass (one model per scene).
+  float heaviest = 0.f;
+  for (const auto& m : s->models) heaviest = std::max(heaviest, m.mass);
+  s->sc.grid_unit = heaviest * kFixInvScale;
   for (auto& m : s->models) {
     ModelDev& d = m.dev;
+    d.flush_ratio = static_cast<double>(m.mass) / static_cast<double>(heaviest);
     const uint32_t n = m.n;
     const bool batch = m.mat.kind == kMixedKind;
     // A batch always tracks ids: they map each particle back to its scene.
@@ -494,8 +514,6 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     CK_CUDA(s, dalloc(s, &d.tile_sums, 2 * static_cast<size_t>(m.ntiles)));
     CK_CUDA(s, dalloc(s, &d.ticket, 1));
     CK_CUDA(s, cudaMemsetAsync(d.ticket, 0, sizeof(uint32_t), s->stream));
-    CK_CUDA(s, dalloc(s, &d.done, d.cap_slots));
-    CK_CUDA(s, cudaMemsetAsync(d.done, 0xFF, sizeof(int32_t) * d.cap_slots, s->stream));
     CK_CUDA(s, dalloc(s, &d.vel_in, 3 * static_cast<size_t>(n)));
     d.smat = nullptr;
     d.sstart = nullptr;
@@ -564,7 +582,9 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     cudaFree(v_out);
     cudaFree(temp);
   }
-  // Initial grid: every model deposits mass and momentum into grid[0], epoch 0.
+  // Initial grid: every model deposits mass and momentum into grid[0], epoch 0;
+  // then the blocks substep 0 deposits into are zeroed in grid[1] (epoch 1).
+  CK_CUDA(s, launch_zero(s, 0, 0, 0));
   for (auto& m : s->models) {
     CK_CUDA(s, cudaMemsetAsync(m.dev.ticket, 0, sizeof(uint32_t), s->stream));
     rasterize_kernel<kFusedThreads><<<s->fused_ctas, kFusedThreads, kSmemFused, s->stream>>>(s->sc, m.dev, s->grid,
@@ -572,6 +592,7 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     CK_CUDA(s, cudaGetLastError());
     CK_CUDA(s, cudaMemsetAsync(m.dev.ticket, 0, sizeof(uint32_t), s->stream));
   }
+  CK_CUDA(s, launch_zero(s, 0, 1, 1));
   Scalars h{};
   h.step = 0;
   h.cur_dt = 0.f;
@@ -640,6 +661,7 @@ ckmpm_status ckmpm_step_adaptive(ckmpm_scene* s, uint32_t nsteps, float dt_max, 
   if (!s || !s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
   if (!(dt_max > 0.f) || !(cfl > 0.f) || !(frame_time > 0.0))
     return fail(s, CKMPM_ERR_INVALID, "dt_max, cfl and frame_time must be positive");
+  if (s->nstack > 1) return fail(s, CKMPM_ERR_INVALID, "a batch steps with a fixed dt (ckmpm_step)");
   CK_CUDA(s, cudaSetDevice(s->desc.device));
   Scalars h{};
   CK_CUDA(s, cudaMemcpyAsync(&h, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
@@ -911,6 +933,7 @@ ckmpm_status ckmpm_step_profiled(ckmpm_scene* s, uint32_t nsteps, float dt, doub
       CK_CUDA(s, launch_fused_any(s, m));
       CK_CUDA(s, cudaEventRecord(E[1], s->stream));
       CK_CUDA(s, launch_compact(s, m, m.dev.bl[parity ^ 1]));
+      if (mi + 1 == nm) CK_CUDA(s, launch_zero(s, parity ^ 1, parity, 2));
       CK_CUDA(s, cudaEventRecord(E[2], s->stream));
     }
     end_substep_kernel<<<1, 32, 0, s->stream>>>(s->scal);

@@ -3,13 +3,16 @@
 // Data layout (per scene; a batch stacks `nstack` identical domains, scene w
 // owning table entries [w * blocks, (w + 1) * blocks), and no stencil, wait or
 // rebin ever crosses from one stacked domain into another):
-//  * grid[2]: dense over every 4^3 block of the domain, 2 KB per block:
+//  * grid[2]: dense over every 4^3 block of the domain, 4 KB per block of
+//    exact 64-bit fixed-point sums (2^-36 of a particle mass per unit):
 //    [m, mvx, mvy, mvz][grid -dx/4, +dx/4][cell i*16 + j*4 + k], the per-block
 //    SoA of the reference's MPMGridBlock (include/mpm_grid.cuh:18-67) but
 //    addressed directly by block coordinate instead of through a partition
-//    slot.  grid[s&1] is read by substep s, grid[(s+1)&1] written by it.
-//  * stamp[2]: per block, the epoch of the substep that last wrote it; a block
-//    whose stamp is stale reads as empty, so nothing is ever cleared.
+//    slot.  grid[s&1] is read by substep s, grid[(s+1)&1] written by it with
+//    integer reductions, so the sums do not depend on the order they arrive in.
+//  * stamp[2]: per block, the epoch for which it was last zeroed; a block whose
+//    stamp is stale reads as empty.  Only the blocks a substep deposits into
+//    are zeroed, by zero_windows_kernel before that substep.
 //  * per model, particle state SoA (x[3], F[9], aux, id) double-buffered and
 //    sorted by particle block; the block list (keys, start, count) in
 //    colour-major key order; a dense block table; 28 outgoing-direction prefix
@@ -17,8 +20,9 @@
 //    block, which of its particles leave in which of the 27 directions.
 //
 // Every substep is: one fused kernel per model (grid update + G2P + F update,
-// SVD, return map + rebin record + P2G, flushed deterministically), then the
-// colour-major compaction that builds the next block list.  No host sync.
+// SVD, return map + rebin record + P2G, flushed as exact integer sums), then
+// the colour-major compaction that builds the next block list and the zeroing
+// of the blocks the next substep deposits into.  No host sync.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -31,12 +35,11 @@ namespace ckmpm {
 constexpr int kMaxParticlesPerBlock = 4096;  // u16 in-block index, 64 per cell x 64 cells as in the reference
 constexpr int kTileNodes = 1024;             // 2 grids x 8^3 nodes around a particle block
 constexpr int kCompactThreads = 256;
-constexpr int kCompactPerThread = 16;
+constexpr int kCompactPerThread = 4;
 constexpr int kCompactTile = kCompactThreads * kCompactPerThread;
 constexpr float kFixScale = 68719476736.0f;        // 2^36: P2G fixed-point scale (per unit particle mass)
 constexpr float kFixInvScale = 1.4551915228366852e-11f;  // 2^-36
 constexpr float kFixMaxValue = 131072.0f;          // |contribution| bound per unit mass (2^17)
-constexpr uint32_t kSpinLimit = 1u << 20;          // polls per flush before a wait gives up (~0.1 s)
 
 enum StatusBits : uint32_t {
   kStatusCapacity = 1u,
@@ -58,6 +61,7 @@ struct SceneDev {
   uint32_t ccount[8];    // blocks of each colour class in one domain
   uint32_t nstack;       // stacked domains (1 for a single scene, the scene count for a batch)
   uint32_t nblocks_domain;  // table entries over all stacked domains
+  float grid_unit;       // single scene: mass of one fixed-point unit (heaviest model's mass x 2^-36)
 };
 
 // Per-scene material of a batch (one model per stacked domain).
@@ -65,7 +69,7 @@ struct SceneMat {
   int32_t kind;
   float p[4];
   float vol_over_mass;  // V_p / m_p
-  float unit;           // m_p * 2^-36: value of one fixed-point unit of the P2G tile
+  float unit;           // m_p * 2^-36: mass of one fixed-point unit of the scene's grid
   float aux0;           // initial logJp (0) or J
 };
 
@@ -110,7 +114,6 @@ struct ModelDev {
   uint32_t* dense_total;  // per domain block: particles binned into it (zero between uses)
   uint32_t* tile_sums;    // compaction partials
   uint32_t* ticket;       // work counter of the fused kernel
-  int32_t* done;          // per slot: epoch of the last completed P2G flush
   float* vel_in;          // setup: sorted initial velocities
   uint32_t cap_slots;
   uint32_t cap_particles;
@@ -118,12 +121,13 @@ struct ModelDev {
   int32_t track_ids;
   MaterialParams mat;
   float mass, vol;
+  double flush_ratio;       // single scene: this model's particle mass / the grid unit's mass (1 for one model)
   const SceneMat* smat;     // batch: per stacked domain; null for a single scene
   const uint32_t* sstart;   // batch setup: first input particle of each scene (nstack + 1)
 };
 
 struct GridDev {
-  float* grid[2];
+  long long* grid[2];
   int32_t* stamp[2];
 };
 
@@ -169,29 +173,20 @@ __device__ __forceinline__ int colour_of(int x, int y, int z) { return ((x & 1) 
 
 __device__ __forceinline__ int trunc_div4(int a) { return a / 4; }  // truncation toward zero, as the reference
 
-__device__ __forceinline__ int32_t ld_acquire(const int32_t* p) {
-  int32_t v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ void st_release(int32_t* p, int32_t v) {
-  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
 __device__ __forceinline__ void set_status(Scalars* s, uint32_t bits) { atomicOr(&s->status, bits); }
 
 // Grid update of one node (include/mpm_algorithm.cuh:739-869): v = mv / m,
-// gravity on y, boundary rule; zero when m <= mass clamp.
-__device__ __forceinline__ float4 node_velocity(const SceneDev& sc, const float* blk, int cell, int bx, int by, int bz,
-                                                int cell_y, float dt) {
+// gravity on y, boundary rule; zero when m <= mass clamp.  The block holds
+// fixed-point sums; unit is the mass of one unit.
+__device__ __forceinline__ float4 node_velocity(const SceneDev& sc, const long long* blk, float unit, int cell, int bx,
+                                                int by, int bz, int cell_y, float dt) {
   float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-  const float m = blk[cell];
+  const float m = __ll2float_rn(__ldcg(blk + cell)) * unit;
   if (m > sc.mass_clamp) {
     const float inv = 1.0f / m;
-    v.x = blk[128 + cell] * inv;
-    v.y = blk[256 + cell] * inv;
-    v.z = blk[384 + cell] * inv;
+    v.x = __ll2float_rn(__ldcg(blk + 128 + cell)) * unit * inv;
+    v.y = __ll2float_rn(__ldcg(blk + 256 + cell)) * unit * inv;
+    v.z = __ll2float_rn(__ldcg(blk + 384 + cell)) * unit * inv;
     v.y += sc.gravity * dt;
     if (sc.boundary == 0) {
       const bool out = (bx < 2 || bx + 2 >= sc.dims[0]) || (by < 2 || by + 2 >= sc.dims[1]) ||
@@ -236,8 +231,9 @@ __device__ __forceinline__ void window_blocks(const SceneDev& sc, const int32_t*
 
 // Loads the velocity tile, applying the grid update on the fly.
 template <int NT>
-__device__ __forceinline__ void load_velocity_tile(const SceneDev& sc, const float* __restrict__ gin, const int64_t* s_blk,
-                                                   int4 key, float dt, float4* vtile) {
+__device__ __forceinline__ void load_velocity_tile(const SceneDev& sc, const long long* __restrict__ gin,
+                                                   const int64_t* s_blk, int4 key, float unit, float dt,
+                                                   float4* vtile) {
   for (int i = threadIdx.x; i < kVelNodes; i += NT) {
     int g, lx, ly, lz;
     if (i < 125) {
@@ -257,7 +253,7 @@ __device__ __forceinline__ void load_velocity_tile(const SceneDev& sc, const flo
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
     if (fb >= 0) {
       const int cell = g * 64 + (lx & 3) * 16 + (ly & 3) * 4 + (lz & 3);
-      v = node_velocity(sc, gin + fb * 512, cell, key.x + (lx >> 2), key.y + (ly >> 2), key.z + (lz >> 2),
+      v = node_velocity(sc, gin + fb * 512, unit, cell, key.x + (lx >> 2), key.y + (ly >> 2), key.z + (lz >> 2),
                         (key.y + (ly >> 2)) * 4 + (ly & 3), dt);
     }
     vtile[i] = v;
@@ -437,89 +433,71 @@ __device__ __forceinline__ void p2g_scatter(unsigned long long* __restrict__ pti
   }
 }
 
-// Epilogue shared by the substep and the initial rasterisation: wait until
-// every lower-colour neighbour block has flushed (they were dequeued earlier,
-// so the waits end), then add this block's tile into the 2x2x2 grid blocks it
-// covers with plain loads and stores.  Writers of one grid block are its 8
-// covering particle blocks, one per colour, so flushes land in colour order
-// and the grid sums are deterministic.
+// Epilogue shared by the substep and the initial rasterisation: add this
+// block's tile into the 2x2x2 grid blocks it covers with 64-bit integer
+// reductions, one node (4 channels) per thread, skipping nodes nothing touched.
+// Integer addition is associative, so the grid sums are bitwise deterministic
+// whatever order the up to 8 covering particle blocks flush in, and no block
+// waits for another (the reference adds floats with atomicAdd,
+// include/mpm_algorithm.cuh:1799-1844).  The target blocks were zeroed and
+// stamped before the launch; ratio rescales a model's per-unit-mass sums to
+// the grid's unit (1 when the scene has one particle mass).
 template <int NT>
-__device__ __forceinline__ void flush_tile(const SceneDev& sc, const BlockListDev& cur, int32_t* done, uint32_t item,
-                                           int4 key, const unsigned long long* __restrict__ ptile, float unit,
-                                           float* __restrict__ gout, int32_t* __restrict__ stout, int32_t epoch,
-                                           Scalars* scal, int* s_mode, bool waiter) {
-  if (waiter) {
-    // One spin budget for all waits of this flush; once any wait in the launch
-    // has given up (status bit set), later waits do not spin at all.
-    const int c0 = colour_of(key.x, key.y, key.z);
-    bool give_up = (*reinterpret_cast<volatile uint32_t*>(&scal->status) & kStatusTimeout) != 0;
-    uint32_t spins = 0;
-    for (int nb = 0; nb < 27 && !give_up; ++nb) {
-      if (nb == 13) continue;
-      const int x = key.x + nb / 9 - 1, y = key.y + (nb / 3) % 3 - 1, z = key.z + nb % 3 - 1;
-      if (!in_domain(sc, x, y, z) || colour_of(x, y, z) >= c0) continue;
-      const int32_t slot = cur.table[flat_block(sc, key.w, x, y, z)];
-      if (slot < 0) continue;
-      while (ld_acquire(done + slot) != epoch) {
-        if (++spins > kSpinLimit) {
-          give_up = true;
-          set_status(scal, kStatusTimeout);
-          atomicAdd(&scal->timeouts, 1u);
-          break;
-        }
-        __nanosleep(32);
-      }
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < 8) {
-    const int e = threadIdx.x;
+__device__ __forceinline__ void flush_tile(const SceneDev& sc, int4 key, const unsigned long long* __restrict__ ptile,
+                                           double ratio, long long* __restrict__ gout) {
+  int64_t fb[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
     const int x = key.x + (e >> 2), y = key.y + ((e >> 1) & 1), z = key.z + (e & 1);
-    int mode = 2;
-    if (in_domain(sc, x, y, z)) mode = (ld_acquire(stout + flat_block(sc, key.w, x, y, z)) == epoch) ? 1 : 0;
-    s_mode[e] = mode;
+    fb[e] = in_domain(sc, x, y, z) ? flat_block(sc, key.w, x, y, z) : -1;
   }
-  __syncthreads();
-  // One node (4 channels) per thread.  In add mode a node that nothing touched
-  // (all four sums zero) is skipped.
   for (int i = threadIdx.x; i < 8 * 128; i += NT) {
     const int e = i >> 7;
-    const int mode = s_mode[e];
-    if (mode == 2) continue;
+    int64_t f = fb[0];
+#pragma unroll
+    for (int k = 1; k < 8; ++k)
+      if (e == k) f = fb[k];
+    if (f < 0) continue;
     const int w = i & 127;
     const int gi = w >> 6, cell = w & 63;
     const int lx = (e >> 2) * 4 + (cell >> 4), ly = ((e >> 1) & 1) * 4 + ((cell >> 2) & 3), lz = (e & 1) * 4 + (cell & 3);
     const unsigned long long* src = ptile + ((gi * 8 + lx) * 64 + ly * 8 + lz);
-    const unsigned long long s0 = src[0], s1 = src[kTileNodes], s2 = src[2 * kTileNodes], s3 = src[3 * kTileNodes];
-    if (mode == 1 && (s0 | s1 | s2 | s3) == 0ull) continue;
-    float* dst =
-        gout + flat_block(sc, key.w, key.x + (e >> 2), key.y + ((e >> 1) & 1), key.z + (e & 1)) * 512 + gi * 64 + cell;
-    const float v0 = __ll2float_rn(static_cast<long long>(s0)) * unit;
-    const float v1 = __ll2float_rn(static_cast<long long>(s1)) * unit;
-    const float v2 = __ll2float_rn(static_cast<long long>(s2)) * unit;
-    const float v3 = __ll2float_rn(static_cast<long long>(s3)) * unit;
-    if (mode == 0) {
-      dst[0] = v0;
-      dst[128] = v1;
-      dst[256] = v2;
-      dst[384] = v3;
-    } else {
-      const float o0 = __ldcg(dst), o1 = __ldcg(dst + 128), o2 = __ldcg(dst + 256), o3 = __ldcg(dst + 384);
-      dst[0] = o0 + v0;
-      dst[128] = o1 + v1;
-      dst[256] = o2 + v2;
-      dst[384] = o3 + v3;
+    unsigned long long v[4] = {src[0], src[kTileNodes], src[2 * kTileNodes], src[3 * kTileNodes]};
+    if ((v[0] | v[1] | v[2] | v[3]) == 0ull) continue;
+    if (ratio != 1.0) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        v[c] = static_cast<unsigned long long>(__double2ll_rn(__ll2double_rn(static_cast<long long>(v[c])) * ratio));
     }
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(gout + f * 512 + gi * 64 + cell);
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      if (v[c]) atomicAdd(dst + c * 128, v[c]);
   }
-  __syncthreads();
-  if (threadIdx.x < 8 && s_mode[threadIdx.x] == 0) {
-    const int e = threadIdx.x;
-    stout[flat_block(sc, key.w, key.x + (e >> 2), key.y + ((e >> 1) & 1), key.z + (e & 1))] = epoch;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    st_release(done + item, epoch);
+}
+
+// Zero the grid blocks that the next substep deposits into -- the 2x2x2
+// window of every block of `list` -- and stamp them with `epoch`, each block
+// once (the first warp to swap its stamp zeroes it).  One warp per (block,
+// window corner).  Runs after every kernel that reads the buffer.
+__global__ void zero_windows_kernel(SceneDev sc, BlockListDev list, long long* __restrict__ g, int32_t* stamp,
+                                    const Scalars* __restrict__ scal, int32_t epoch_offset) {
+  const uint32_t nb = *list.nblocks;
+  const int32_t epoch = scal->step + epoch_offset;
+  const int lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nb * 8u; t += nwarps) {
+    const int4 key = list.keys[t >> 3];
+    const int e = static_cast<int>(t & 7u);
+    const int x = key.x + (e >> 2), y = key.y + ((e >> 1) & 1), z = key.z + (e & 1);
+    if (!in_domain(sc, x, y, z)) continue;
+    const int64_t f = flat_block(sc, key.w, x, y, z);
+    int won = 0;
+    if (lane == 0) won = atomicExch(stamp + f, epoch) != epoch ? 1 : 0;
+    won = __shfl_sync(0xffffffffu, won, 0);
+    if (!won) continue;
+    longlong2* p = reinterpret_cast<longlong2*>(g + f * 512);
+    for (int i = lane; i < 256; i += 32) p[i] = make_longlong2(0, 0);
   }
 }
 
@@ -577,8 +555,6 @@ struct SharedSmall {
   uint32_t off[28];
   uint32_t idx[27];
   uint32_t src[27];
-  int mode[8];
-  uint32_t nflag;
 };
 
 constexpr size_t kSmemVTile = sizeof(float4) * 344;                      // 5.5 KB (341 nodes)
@@ -612,16 +588,15 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
 
   const int32_t step = scal->step;
   const int parity = step & 1;
-  const int32_t read_epoch = step, write_epoch = step + 1;
+  const int32_t read_epoch = step;
   const float dt = scal->cur_dt, ndt = scal->next_dt;
   const BlockListDev cur = md.bl[parity];
   const BlockListDev prev = md.bl[parity ^ 1];
   const StateDev sin = md.st[parity];
   const StateDev sout = md.st[parity ^ 1];
-  const float* __restrict__ gin = gd.grid[parity];
-  float* __restrict__ gout = gd.grid[parity ^ 1];
+  const long long* __restrict__ gin = gd.grid[parity];
+  long long* __restrict__ gout = gd.grid[parity ^ 1];
   const int32_t* __restrict__ stin = gd.stamp[parity];
-  int32_t* __restrict__ stout = gd.stamp[parity ^ 1];
   const uint32_t nb = *cur.nblocks;
   const float dx = sc.dx, inv_dx = sc.inv_dx;
   const uint32_t maxp = min(md.max_per_block, static_cast<uint32_t>(kMaxParticlesPerBlock));
@@ -636,7 +611,8 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
     uint32_t n = cur.count[item];
     int kind = KIND;
     float mp0 = md.mat.p[0], mp1 = md.mat.p[1], mp2 = md.mat.p[2];
-    float vol_over_mass = md.vol / md.mass, unit = md.mass * kFixInvScale;
+    float vol_over_mass = md.vol / md.mass, unit = sc.grid_unit;
+    double ratio = md.flush_ratio;
     if (KIND == kMixed) {
       const SceneMat& sm = md.smat[key.w];
       kind = sm.kind;
@@ -645,6 +621,7 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
       mp2 = sm.p[2];
       vol_over_mass = sm.vol_over_mass;
       unit = sm.unit;
+      ratio = 1.0;
     }
 
     if (threadIdx.x < 32)
@@ -654,7 +631,7 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
     for (int i = threadIdx.x; i < 8 * 28; i += NT) (&sh.wcnt[0][0])[i] = 0u;
     for (int i = threadIdx.x; i < kTileNodes * 4; i += NT) ptile[i] = 0ull;
     __syncthreads();
-    load_velocity_tile<NT>(sc, gin, sh.blk, key, dt, vtile);
+    load_velocity_tile<NT>(sc, gin, sh.blk, key, unit, dt, vtile);
     __syncthreads();
     if (threadIdx.x == 0) {
       uint32_t flags = 0;
@@ -835,8 +812,7 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
         __syncwarp();
       }
     }
-    flush_tile<NT>(sc, cur, md.done, item, key, ptile, unit, gout, stout, write_epoch, scal, sh.mode,
-                   threadIdx.x == 32);
+    flush_tile<NT>(sc, key, ptile, ratio, gout);
   }
 }
 
@@ -886,9 +862,7 @@ __global__ void __launch_bounds__(NT, 2) rasterize_kernel(SceneDev sc, ModelDev 
       if (ok && finite) p2g_scatter(ptile, st, lb, v, Z);
     }
     __syncthreads();
-    const float unit = md.smat ? md.smat[key.w].unit : md.mass * kFixInvScale;
-    flush_tile<NT>(sc, cur, md.done, item, key, ptile, unit, gd.grid[0], gd.stamp[0], 0, scal, sh.mode,
-                   threadIdx.x == 32);
+    flush_tile<NT>(sc, key, ptile, md.smat ? 1.0 : md.flush_ratio, gd.grid[0]);
   }
 }
 
@@ -1086,7 +1060,7 @@ __global__ void grid_maxv_kernel(SceneDev sc, GridDev gd, Scalars* scal, float m
   sc.mass_clamp = fmaxf(sc.mass_clamp, mass_floor);
   const int32_t step = scal->step;
   const int parity = step & 1;
-  const float* g = gd.grid[parity];
+  const long long* g = gd.grid[parity];
   const int32_t* stamp = gd.stamp[parity];
   const float dt = scal->cur_dt;
   const int lane = threadIdx.x & 31;
@@ -1098,7 +1072,8 @@ __global__ void grid_maxv_kernel(SceneDev sc, GridDev gd, Scalars* scal, float m
     const int by = static_cast<int>((b / sc.dims[2]) % sc.dims[1]);
     const int bx = static_cast<int>((b / (static_cast<uint32_t>(sc.dims[2]) * sc.dims[1])) % sc.dims[0]);
     for (int node = lane; node < 128; node += 32) {
-      const float4 v = node_velocity(sc, g + static_cast<int64_t>(b) * 512, node, bx, by, bz, by * 4 + ((node >> 2) & 3), dt);
+      const float4 v = node_velocity(sc, g + static_cast<int64_t>(b) * 512, sc.grid_unit, node, bx, by, bz,
+                                     by * 4 + ((node >> 2) & 3), dt);
       float n2 = v.x * v.x + v.y * v.y + v.z * v.z;
       if (isnan(n2)) n2 = __int_as_float(0x7f800000);
       vmax2 = fmaxf(vmax2, n2);
@@ -1216,7 +1191,8 @@ __global__ void __launch_bounds__(NT) probe_kernel(SceneDev sc, ModelDev md, Gri
     else if (threadIdx.x < 40)
       window_blocks(sc, gd.stamp[parity], step, key, sh.blk, threadIdx.x - 32);
     __syncthreads();
-    if (ov) load_velocity_tile<NT>(sc, gd.grid[parity], sh.blk, key, dt, vtile);
+    if (ov) load_velocity_tile<NT>(sc, gd.grid[parity], sh.blk, key, md.smat ? md.smat[key.w].unit : sc.grid_unit, dt,
+                                   vtile);
     __syncthreads();
     const uint32_t nn = min(n, sh.off[27]);
     for (uint32_t q = threadIdx.x; q < nn; q += NT) {

@@ -32,7 +32,7 @@ constexpr int kNoAllocMaxDevices = 64;
 constexpr size_t na_align(size_t b) { return (b + 255) & ~size_t(255); }
 
 // Bytes of every region at the maximum sizes (see carve() below).
-constexpr size_t kNaGrid = na_align(sizeof(float) * 512 * kNoAllocMaxDomainBlocks);
+constexpr size_t kNaGrid = na_align(sizeof(long long) * 512 * kNoAllocMaxDomainBlocks);
 constexpr size_t kNaDomainU32 = na_align(sizeof(uint32_t) * kNoAllocMaxDomainBlocks);
 constexpr size_t kNaParticleU32 = na_align(sizeof(uint32_t) * kNoAllocMaxParticles);
 constexpr size_t kNaParticleU16 = na_align(sizeof(uint16_t) * kNoAllocMaxParticles);
@@ -44,10 +44,10 @@ constexpr size_t kNaState = 14 * kNaParticleU32;  // x[3], F[9], aux, id
 constexpr size_t kNoAllocScratchBytes =
     2 * kNaGrid + 2 * kNaDomainU32 + na_align(sizeof(Scalars)) + 2 * kNaState + 2 * kNaBlockList +
     kNaDomainU32 /*dense totals*/ + na_align(sizeof(uint32_t) * 2 * 64) /*tile sums*/ + na_align(4) /*ticket*/ +
-    na_align(sizeof(int32_t) * kNaSlots) /*done*/ + 3 * kNaParticleU32 /*initial velocities*/ +
+    3 * kNaParticleU32 /*initial velocities*/ +
     4 * kNaParticleU32 /*sort keys and values*/ + kNoAllocCubTempBytes + 18 * kNaParticleU32 /*export*/;
 
-static_assert(kNoAllocScratchBytes < (size_t(48) << 20), "no-alloc scratch must stay modest");
+static_assert(kNoAllocScratchBytes < (size_t(56) << 20), "no-alloc scratch must stay modest");
 
 // The scratch.  In host code `g_noalloc_scratch` is only a host-side stand-in
 // for the symbol, not a device address: its device address comes from
@@ -183,6 +183,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   sc.mass_clamp = desc->mass_clamp;
   sc.boundary = desc->boundary;
   sc.floor_cells = desc->floor_cells;
+  sc.grid_unit = mass * kFixInvScale;
   init_colour_classes(sc, 1);
 
   // Carve the scratch array (fixed layout at the maximum sizes).
@@ -192,7 +193,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   ModelDev d{};
   const bool hasF = material->kind != CKMPM_FLUID;
   const bool hasAux = material->kind != CKMPM_FIXED_COROTATED;
-  for (int b = 0; b < 2; ++b) grid.grid[b] = cv.take<float>(size_t(512) * kNoAllocMaxDomainBlocks);
+  for (int b = 0; b < 2; ++b) grid.grid[b] = cv.take<long long>(size_t(512) * kNoAllocMaxDomainBlocks);
   for (int b = 0; b < 2; ++b) grid.stamp[b] = cv.take<int32_t>(kNoAllocMaxDomainBlocks);
   scal = cv.take<Scalars>(1);
   for (int b = 0; b < 2; ++b) {
@@ -220,7 +221,6 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   d.dense_total = cv.take<uint32_t>(kNoAllocMaxDomainBlocks);
   d.tile_sums = cv.take<uint32_t>(2 * 64);
   d.ticket = cv.take<uint32_t>(1);
-  d.done = cv.take<int32_t>(kNaSlots);
   d.vel_in = cv.take<float>(3 * size_t(kNoAllocMaxParticles));
   uint32_t* sort_keys_in = cv.take<uint32_t>(kNoAllocMaxParticles);
   uint32_t* sort_keys_out = cv.take<uint32_t>(kNoAllocMaxParticles);
@@ -243,6 +243,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   for (int k = 0; k < 4; ++k) d.mat.p[k] = material->p[k];
   d.mass = mass;
   d.vol = volume;
+  d.flush_ratio = 1.0;
   const uint32_t ntiles = (nbd + kCompactTile - 1) / kCompactTile;
 
   size_t temp_bytes = 0;
@@ -266,7 +267,6 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   }
   NA_CUDA(cudaMemsetAsync(d.dense_total, 0, sizeof(uint32_t) * nbd, st));
   NA_CUDA(cudaMemsetAsync(d.ticket, 0, sizeof(uint32_t), st));
-  NA_CUDA(cudaMemsetAsync(d.done, 0xFF, sizeof(int32_t) * d.cap_slots, st));
 
   // Setup: bin, sort by colour-major block index, compact, gather, identity
   // previous step, initial grid -- the sequence of ckmpm_setup.
@@ -292,8 +292,12 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   NA_CUDA(cudaMemcpyAsync(d.bl[1].nparticles, d.bl[0].nparticles, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
   if (counts[0] > 0) setup_identity_kernel<<<counts[0], 256, 0, st>>>(d.bl[0], d.bl[1]);
   NA_CUDA(cudaMemsetAsync(d.ticket, 0, sizeof(uint32_t), st));
+  int sms = 0;
+  NA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, desc->device));
+  zero_windows_kernel<<<sms * 4, 256, 0, st>>>(sc, d.bl[0], grid.grid[0], grid.stamp[0], scal, 0);
   rasterize_kernel<kFusedThreads><<<ctas, kFusedThreads, kSmemFused, st>>>(sc, d, grid, scal);
   NA_CUDA(cudaMemsetAsync(d.ticket, 0, sizeof(uint32_t), st));
+  zero_windows_kernel<<<sms * 4, 256, 0, st>>>(sc, d.bl[0], grid.grid[1], grid.stamp[1], scal, 1);
   Scalars h{};
   h.lost = n - n_valid;
   NA_CUDA(cudaMemcpyAsync(scal, &h, sizeof(Scalars), cudaMemcpyHostToDevice, st));
@@ -316,6 +320,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
     compact_reduce_kernel<<<ntiles, kCompactThreads, 0, st>>>(sc, d.dense_total, d.tile_sums);
     compact_scatter_kernel<<<ntiles, kCompactThreads, 0, st>>>(sc, d.dense_total, d.tile_sums, d.bl[parity ^ 1],
                                                                d.cap_slots, d.ticket, scal);
+    zero_windows_kernel<<<sms * 4, 256, 0, st>>>(sc, d.bl[parity ^ 1], grid.grid[parity], grid.stamp[parity], scal, 2);
     end_substep_kernel<<<1, 32, 0, st>>>(scal);
   }
   NA_CUDA(cudaGetLastError());
@@ -324,8 +329,6 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   const BlockListDev& cur = d.bl[nsteps & 1];
   uint32_t live = 0;
   NA_CUDA(cudaMemcpyAsync(&live, cur.nparticles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-  int sms = 0;
-  NA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, desc->device));
   probe_kernel<kProbeThreads><<<sms * 4, kProbeThreads, kSmemVTile, st>>>(sc, d, grid, scal, ex, ev, hasF ? eF : nullptr,
                                                                          hasAux ? ea : nullptr, eid, nullptr);
   NA_CUDA(cudaStreamSynchronize(st));

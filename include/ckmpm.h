@@ -147,7 +147,7 @@ ckmpm_status ckmpm_get_blocks(ckmpm_scene* s, int32_t model, int32_t which, int3
 
 /* Device counters: [0] substeps taken, [1] particles lost at the domain edge,
  * [2] P2G window escapes (particle skipped in P2G, include/mpm_algorithm.cuh:1670-1683),
- * [3] status bits, [4] bounded-wait timeouts. */
+ * [3] status bits, [4] bounded-wait timeouts (the substep has no device-side waits; kept for the ABI, 0). */
 ckmpm_status ckmpm_get_counters(ckmpm_scene* s, uint64_t* out5);
 
 /* Current dt pair: [0] the dt the next substep advects with, [1] the dt it deposits stress with. */
@@ -173,7 +173,7 @@ ckmpm_status ckmpm_debug_constitutive(const ckmpm_material* material, uint32_t n
  * code running while another framework captures a CUDA graph on the stream,
  * plugins whose host runtime owns the device memory budget, and real-time
  * loops that cannot take the device-wide synchronisation of an allocation.
- * All scratch lives in one fixed __device__ array of 34.7 MB that every GPU
+ * All scratch lives in one fixed __device__ array of 53.1 MB that every GPU
  * loading this library keeps until exit; limits: n <= 65536 particles and at
  * most 4096 blocks in the domain (e.g. 16^3), else CKMPM_ERR_CAPACITY.  The
  * first call on a device looks up the array's device address, so make that
