@@ -25,8 +25,12 @@ STATUS_NAMES = {
 }
 
 FIXED_COROTATED = 0
+LINEAR = 1
 DRUCKER_PRAGER = 2
 FLUID = 3
+VON_MISES = 4
+NACC = 5
+MATERIAL_PARAMS = 8
 
 BOUNDARY_STICKY_BLOCKS = 0
 BOUNDARY_SLIP_FLOOR = 1
@@ -63,7 +67,7 @@ class SceneDesc(C.Structure):
 
 
 class Material(C.Structure):
-    _fields_ = [("kind", C.c_int32), ("p", C.c_float * 4)]
+    _fields_ = [("kind", C.c_int32), ("p", C.c_float * MATERIAL_PARAMS)]
 
 
 class BatchScene(C.Structure):

@@ -17,8 +17,9 @@ ROOT = PKG.parent
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libckmpm_b200.so"
 SOURCES = [PKG / "csrc" / "library.cu"]
-DEPS = SOURCES + [PKG / "csrc" / "engine.cu", PKG / "csrc" / "noalloc.cu", PKG / "csrc" / "kernels.cuh",
-                  PKG / "csrc" / "mpm_math.cuh", ROOT / "include" / "ckmpm.h"]
+# Every source and header the library's single translation unit pulls in.
+DEPS = SOURCES + sorted((PKG / "csrc").glob("*.cu")) + sorted((PKG / "csrc").glob("*.cuh")) + \
+    sorted((ROOT / "include").glob("*.h"))
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

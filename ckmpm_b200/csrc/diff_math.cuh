@@ -8,7 +8,9 @@
 //   G2P at x:   v = 1/2 sum_i w_i v_i,  B = sum_i w_i v_i r_i^T,  C = B D^-1
 //   x' = x + dt v;   F' = (I + dt C) F
 //   tau = 2 mu (F' - R) F'^T + lambda J (J - 1) I        (R = U V^T, F' = U S V^T)
-//   P2G at x':  m_i += m w'_i,  mv_i += m w'_i (v + A r'_i),  A = C - ndt V/m (D'/2)^-1 tau
+//   P2G at x':  m_i += m w'_i,  mv_i += m w'_i (v + A r'_i),  A = C - ndt V/m M tau,
+//               M = (0.5 (D + D'))^-1 (the reference adds D' at x' onto the G2P D at x
+//               and inverts half the sum, include/mpm_algorithm.cuh:1524,1604,1729-1732)
 // with r_i = (d - o) dx the node offset from the particle, w_i the tensor
 // product of CK weights w0(o) = 1 - o + sin(2 pi o) / (2 pi) (include/mpm_kernel.cuh:91-114),
 // and D = sum_i w_i r_i r_i^T over both staggered grids (g = -1/4, +1/4 dx).
@@ -18,13 +20,13 @@
 //   P2G:  vbar += m sum w' mvbar_i;  Abar = m sum w' mvbar_i r'_i^T;
 //         x'bar from dw'/dx', from dr'/dx' = -I and from D'(x')
 //   A:    Cbar += Abar;  (M tau)bar = -ndt V/m Abar;  Mbar = (M tau)bar tau^T;
-//         taubar = M (M tau)bar;  Dbar' = -1/2 M Mbar M
+//         taubar = M (M tau)bar;  Dbar' = Dbar(M) = -1/2 M Mbar M
 //   tau:  Fbar' += 2 mu (taubar F' + taubar (F' - R)) + polar term of Rbar = -2 mu taubar F'
 //         + lambda (2J - 1) tr(taubar) cof(F');  mubar, lambdabar for the parameters
 //         polar term: Q = U^T Rbar V, Mbar_ij = (Q_ij - Q_ji) / (s_i + s_j), Fbar += U Mbar V^T
 //   F:    Fbar = (I + dt C)^T Fbar';  Cbar += dt Fbar' F^T
 //   x:    xbar += x'bar;  vbar += dt x'bar
-//   C:    Bbar = Cbar D^-1;  Dbar = -D^-1 B^T Cbar D^-1
+//   C:    Bbar = Cbar D^-1;  Dbar = -D^-1 B^T Cbar D^-1 + Dbar(M)
 //   G2P:  vibar_i += 1/2 w_i vbar + w_i Bbar r_i;  xbar from dw/dx, dr/dx, D(x)
 #pragma once
 
@@ -346,7 +348,7 @@ struct Fwd {
   Stencil<T> st, stn;       // stencils at x and at x'
   T v[3], B[9], C[9], Di[9];  // G2P result, D^-1
   T xn[3], Fn[9];
-  T tau[9], M[9], A[9];     // M = (D'/2)^-1, A per unit mass
+  T tau[9], M[9], A[9];     // M = (0.5 (D + D'))^-1, A per unit mass
 };
 
 // G2P + x, F update + stress + affine term.  vel(g, cx, cy, cz, T* v) returns
@@ -400,7 +402,7 @@ CKD void particle_forward(const Particle<T>& p, T lambda, T mu, T vol_over_mass,
   T Dn6[6], M6[6];
   d_matrix(f.stn, dx, Dn6);
   CKD_UNROLL
-  for (int k = 0; k < 6; ++k) Dn6[k] *= T(0.5);
+  for (int k = 0; k < 6; ++k) Dn6[k] = T(0.5) * (D6[k] + Dn6[k]);
   inv_sym(Dn6, M6);
   sym_full(M6, f.M);
   T Mt[9];
@@ -499,7 +501,7 @@ CKD void particle_adjoint(const Particle<T>& p, const Fwd<T>& f, const T* U, con
   T Mb[9], taub[9];
   mmt(MTb, f.tau, Mb);   // Mbar = (M tau)bar tau^T
   mm(f.M, MTb, taub);    // taubar = M^T (M tau)bar, M symmetric
-  // M = X^-1, X = D'/2: Xbar = -M Mbar M; D'bar = Xbar / 2
+  // M = X^-1, X = (D + D') / 2: Xbar = -M Mbar M; D'bar = Dbar(old) = Xbar / 2
   T t1[9], Dnb[9];
   mm(f.M, Mb, t1);
   mm(t1, f.M, Dnb);
@@ -530,7 +532,7 @@ CKD void particle_adjoint(const Particle<T>& p, const Fwd<T>& f, const T* U, con
   mm(f.Di, t2, t3);
   mm(t3, f.Di, Db);
   CKD_UNROLL
-  for (int k = 0; k < 9; ++k) Db[k] = -Db[k];
+  for (int k = 0; k < 9; ++k) Db[k] = Dnb[k] - Db[k];
   d_matrix_adjoint(f.st, dx, inv_dx, Db, xbar);
   // G2P at x: v = 1/2 sum w v_i, B = sum w v_i r^T
   CKD_UNROLL

@@ -118,7 +118,10 @@ template <int NT>
 cudaError_t launch_fused_nt(ckmpm_scene* s, const ModelHost& m) {
   switch (m.mat.kind) {
     case CKMPM_FIXED_COROTATED: return launch_fused<kFixedCorotated, NT>(s, m);
+    case CKMPM_LINEAR: return launch_fused<kLinear, NT>(s, m);
     case CKMPM_DRUCKER_PRAGER: return launch_fused<kDruckerPrager, NT>(s, m);
+    case CKMPM_VON_MISES: return launch_fused<kVonMises, NT>(s, m);
+    case CKMPM_NACC: return launch_fused<kNacc, NT>(s, m);
     case kMixedKind: return launch_fused<kMixed, NT>(s, m);
     default: return launch_fused<kFluid, NT>(s, m);
   }
@@ -130,9 +133,12 @@ cudaError_t launch_fused_any(ckmpm_scene* s, const ModelHost& m) {
 
 template <int NT>
 cudaError_t set_fused_attributes(int* occ) {
-  const void* fns[4] = {reinterpret_cast<const void*>(g2p2g_kernel<kFixedCorotated, NT>),
+  const void* fns[7] = {reinterpret_cast<const void*>(g2p2g_kernel<kFixedCorotated, NT>),
+                        reinterpret_cast<const void*>(g2p2g_kernel<kLinear, NT>),
                         reinterpret_cast<const void*>(g2p2g_kernel<kDruckerPrager, NT>),
                         reinterpret_cast<const void*>(g2p2g_kernel<kFluid, NT>),
+                        reinterpret_cast<const void*>(g2p2g_kernel<kVonMises, NT>),
+                        reinterpret_cast<const void*>(g2p2g_kernel<kNacc, NT>),
                         reinterpret_cast<const void*>(g2p2g_kernel<kMixed, NT>)};
   int lowest = 1 << 30;
   for (const void* fn : fns) {
@@ -212,6 +218,30 @@ cudaError_t build_graph(ckmpm_scene* s, int nsub, int first_parity, cudaGraphExe
   e = cudaGraphInstantiate(exec, g, 0);
   cudaGraphDestroy(g);
   return e;
+}
+
+// Material kinds this engine runs and the parameter each needs to be positive.
+bool valid_material(const ckmpm_material& m, std::string* why) {
+  switch (m.kind) {
+    case CKMPM_FIXED_COROTATED:
+    case CKMPM_LINEAR:
+    case CKMPM_DRUCKER_PRAGER:
+      if (!(m.p[1] > 0.f)) return (*why = "mu (p[1]) must be positive", false);
+      return true;
+    case CKMPM_VON_MISES:
+    case CKMPM_NACC:
+      if (!(m.p[0] > 0.f)) return (*why = "mu (p[0]) must be positive", false);
+      return true;
+    case CKMPM_FLUID:
+      return true;
+    default:
+      return (*why = "unsupported material kind", false);
+  }
+}
+
+// Initial aux value: J0 for the fluid, alpha0 (the initial logJp) for NACC, else 0.
+float initial_aux(const ckmpm_material& m) {
+  return m.kind == CKMPM_FLUID ? m.p[3] : (m.kind == CKMPM_NACC ? m.p[2] : 0.f);
 }
 
 ckmpm_status status_from(ckmpm_scene* s, const Scalars& h) {
@@ -357,18 +387,16 @@ ckmpm_status ckmpm_add_batch(ckmpm_scene* s, uint32_t nscenes, const ckmpm_batch
   for (uint32_t i = 0; i < nscenes; ++i) {
     const ckmpm_batch_scene& b = scenes[i];
     const int k = b.material.kind;
-    if (k != CKMPM_FIXED_COROTATED && k != CKMPM_DRUCKER_PRAGER && k != CKMPM_FLUID)
-      return fail(s, CKMPM_ERR_INVALID, "unsupported material kind in scene " + std::to_string(i));
+    std::string why;
+    if (!valid_material(b.material, &why)) return fail(s, CKMPM_ERR_INVALID, why + " (scene " + std::to_string(i) + ")");
     if (!(b.mass > 0.f) || !(b.volume > 0.f))
       return fail(s, CKMPM_ERR_INVALID, "mass and volume must be positive (scene " + std::to_string(i) + ")");
-    if (k != CKMPM_FLUID && !(b.material.p[1] > 0.f))
-      return fail(s, CKMPM_ERR_INVALID, "mu must be positive (scene " + std::to_string(i) + ")");
     SceneMat& sm = m.smat[i];
     sm.kind = k;
-    for (int j = 0; j < 4; ++j) sm.p[j] = b.material.p[j];
+    for (int j = 0; j < kMaterialParams; ++j) sm.p[j] = b.material.p[j];
     sm.vol_over_mass = b.volume / b.mass;
     sm.unit = b.mass * kFixInvScale;
-    sm.aux0 = k == CKMPM_FLUID ? b.material.p[3] : 0.f;
+    sm.aux0 = initial_aux(b.material);
     m.skind[i] = k;
     m.sstart[i] = static_cast<uint32_t>(total);
     total += b.n;
@@ -437,11 +465,9 @@ ckmpm_status ckmpm_add_model(ckmpm_scene* s, const ckmpm_material* material, uin
   if (s->setup_done) return fail(s, CKMPM_ERR_INVALID, "models must be added before ckmpm_setup");
   if (n == 0) return fail(s, CKMPM_ERR_INVALID, "empty model");
   if (nv != 1 && nv != n) return fail(s, CKMPM_ERR_INVALID, "nv must be 1 or n");
-  if (material->kind != CKMPM_FIXED_COROTATED && material->kind != CKMPM_DRUCKER_PRAGER && material->kind != CKMPM_FLUID)
-    return fail(s, CKMPM_ERR_INVALID, "unsupported material kind");
+  std::string why;
+  if (!valid_material(*material, &why)) return fail(s, CKMPM_ERR_INVALID, why);
   if (!(mass > 0.f) || !(volume > 0.f)) return fail(s, CKMPM_ERR_INVALID, "mass and volume must be positive");
-  if ((material->kind != CKMPM_FLUID) && !(material->p[1] > 0.f))
-    return fail(s, CKMPM_ERR_INVALID, "mu must be positive");
   ModelHost m;
   m.mat = *material;
   m.mass = mass;
@@ -480,12 +506,13 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     d.max_per_block = s->desc.max_particles_per_block;
     d.track_ids = track ? 1 : 0;
     d.mat.kind = m.mat.kind;
-    for (int k = 0; k < 4; ++k) d.mat.p[k] = m.mat.p[k];
+    for (int k = 0; k < kMaterialParams; ++k) d.mat.p[k] = m.mat.p[k];
     d.mass = m.mass;
     d.vol = m.vol;
     m.ntiles = (nbd + kCompactTile - 1) / kCompactTile;
-    const bool hasF = m.mat.kind != CKMPM_FLUID;
-    const bool hasAux = m.mat.kind != CKMPM_FIXED_COROTATED;
+    const bool hasF = batch || material_has_F(m.mat.kind);
+    const bool hasAux = batch || material_has_aux(m.mat.kind);
+    const bool hasQ = batch ? std::count(m.skind.begin(), m.skind.end(), CKMPM_LINEAR) > 0 : m.mat.kind == CKMPM_LINEAR;
     for (int b = 0; b < 2; ++b) {
       StateDev& st = d.st[b];
       for (int a = 0; a < 3; ++a) CK_CUDA(s, dalloc(s, &st.x[a], n));
@@ -495,6 +522,10 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
       }
       st.aux = nullptr;
       if (hasAux) CK_CUDA(s, dalloc(s, &st.aux, n));
+      for (int k = 0; k < 9; ++k) {
+        st.Q[k] = nullptr;
+        if (hasQ) CK_CUDA(s, dalloc(s, &st.Q[k], n));
+      }
       st.id = nullptr;
       if (track) CK_CUDA(s, dalloc(s, &st.id, n));
       BlockListDev& bl = d.bl[b];
@@ -555,7 +586,7 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     CK_CUDA(s, cudaStreamSynchronize(s->stream));
     m.n_valid = counts[1];
     lost_at_setup += n - m.n_valid;
-    const float aux0 = m.mat.kind == CKMPM_FLUID ? m.mat.p[3] : 0.f;
+    const float aux0 = initial_aux(m.mat);
     if (m.n_valid > 0)
       setup_gather_kernel<<<(m.n_valid + 255) / 256, 256, 0, s->stream>>>(d, s->nstack, m.n_valid, v_out, dx_in,
                                                                            dv_in, m.nv, aux0);
@@ -960,7 +991,10 @@ ckmpm_status ckmpm_debug_constitutive(const ckmpm_material* material, uint32_t n
   if (!material || !C || !F || !tau || n == 0) return fail(nullptr, CKMPM_ERR_INVALID, "null argument");
   MaterialParams mp{};
   mp.kind = material->kind;
-  for (int k = 0; k < 4; ++k) mp.p[k] = material->p[k];
+  std::string why;
+  if (!valid_material(*material, &why)) return fail(nullptr, CKMPM_ERR_INVALID, why);
+  if (material->kind == CKMPM_LINEAR) return fail(nullptr, CKMPM_ERR_INVALID, "the linear model keeps a stored stress");
+  for (int k = 0; k < kMaterialParams; ++k) mp.p[k] = material->p[k];
   float *dC, *dF, *dA, *dT, *dU, *dS, *dV;
   auto chk = [](cudaError_t e) { return e == cudaSuccess; };
   if (!chk(cudaMalloc(&dC, sizeof(float) * 9 * n)) || !chk(cudaMalloc(&dF, sizeof(float) * 9 * n)) ||

@@ -67,10 +67,10 @@ struct SceneDev {
 // Per-scene material of a batch (one model per stacked domain).
 struct SceneMat {
   int32_t kind;
-  float p[4];
+  float p[kMaterialParams];
   float vol_over_mass;  // V_p / m_p
   float unit;           // m_p * 2^-36: mass of one fixed-point unit of the scene's grid
-  float aux0;           // initial logJp (0) or J
+  float aux0;           // initial logJp (0; alpha0 for NACC) or J (J0)
 };
 
 constexpr int kMixed = 7;  // material kind read per work item from the scene's SceneMat
@@ -104,9 +104,16 @@ struct BlockListDev {
 struct StateDev {
   float* x[3];
   float* F[9];
-  float* aux;
+  float* aux;    // logJp (Drucker-Prager, NACC) or J (fluid)
+  float* Q[9];   // the linear model's stored stress
   uint32_t* id;
 };
+
+// Which per-particle arrays a material keeps.
+__host__ __device__ __forceinline__ bool material_has_F(int kind) { return kind != kFluid; }
+__host__ __device__ __forceinline__ bool material_has_aux(int kind) {
+  return kind == kDruckerPrager || kind == kFluid || kind == kNacc;
+}
 
 struct ModelDev {
   StateDev st[2];
@@ -315,11 +322,12 @@ __device__ __forceinline__ void sym_to_full(const float* s6, float* f) {
 
 // G2P on both grids (include/mpm_algorithm.cuh:1555-1638): returns the
 // halved interpolated velocity and C = B D^-1, where B = sum v_i (w r_i)^T
-// and D = sum w r_i r_i^T with r_i = x_i - x_p, both over the 16 nodes.
+// and D = sum w r_i r_i^T with r_i = x_i - x_p, both over the 16 nodes, and
+// D itself (6 entries) in D6.
 // B is accumulated through the separable sums S = sum w v and
 // T_a = sum over nodes with d_a = 1 of w v:  B[r][a] = dx (T_a[r] - o_a S[r]).
 __device__ __forceinline__ void g2p(const float4* __restrict__ vtile, const float (&xs)[3], int4 key, float dx,
-                                    float* v, float* C, bool& inside) {
+                                    float* v, float* C, bool& inside, float* D6) {
   AxisStencil st[2][3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -372,7 +380,7 @@ __device__ __forceinline__ void g2p(const float4* __restrict__ vtile, const floa
       for (int a = 0; a < 3; ++a) B[r * 3 + a] += dx * (T[r][a] - st[g][a].o * S[r]);
     }
   }
-  float D6[6], Di6[6], Di[9];
+  float Di6[6], Di[9];
   d_matrix(st, dx, D6);
   inv_sym3(D6[0], D6[1], D6[2], D6[3], D6[4], D6[5], Di6);
   sym_to_full(Di6, Di);
@@ -548,6 +556,9 @@ __device__ __forceinline__ int find_group(const uint32_t* s_off, uint32_t q) {
   return lo;
 }
 
+// Output slot of the q-th particle of a block that starts at `start`.
+__device__ __forceinline__ uint32_t o_slot(uint32_t start, uint32_t q) { return start + q; }
+
 struct SharedSmall {
   int64_t blk[8];
   uint32_t wcnt[8][28];
@@ -652,15 +663,15 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
       float x[3] = {sin.x[0][iin], sin.x[1][iin], sin.x[2][iin]};
       float F[9];
       float aux = 0.f;
-      if (kind != kFluid) {
+      if (material_has_F(kind)) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) F[k] = sin.F[k][iin];
       }
-      if (kind != kFixedCorotated) aux = sin.aux[iin];
+      if (material_has_aux(kind)) aux = sin.aux[iin];
       float xs[3] = {x[0] * inv_dx, x[1] * inv_dx, x[2] * inv_dx};
       bool inside = true;
-      float v[3], C[9];
-      g2p(vtile, xs, key, dx, v, C, inside);
+      float v[3], C[9], Dold[6];
+      g2p(vtile, xs, key, dx, v, C, inside, Dold);
 #pragma unroll
       for (int a = 0; a < 3; ++a) x[a] += dt * v[a];
 
@@ -672,21 +683,36 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
 #pragma unroll
         for (int k = 0; k < 9; ++k) dW[k] = C[k] * dt + ((k & 3) ? 0.f : 1.f);
         matmul3(dW, F, F);
-        if (kind == kFixedCorotated)
+        if (kind == kFixedCorotated) {
           stress_fixed_corotated(mp0, mp1, F, tau);
-        else
+        } else if (kind == kDruckerPrager) {
           stress_drucker_prager(mp0, mp1, F, aux, tau);
+        } else if (kind == kVonMises) {
+          stress_von_mises(mp0, mp1, mp2, F, tau);
+        } else if (kind == kNacc) {
+          float prm[kMaterialParams];
+#pragma unroll
+          for (int k = 0; k < kMaterialParams; ++k) prm[k] = KIND == kMixed ? md.smat[key.w].p[k] : md.mat.p[k];
+          stress_nacc(prm, F, aux, tau);
+        } else {  // kLinear
+          float Q[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) Q[k] = sin.Q[k][iin];
+          stress_linear(C, dt, F, Q, tau);
+#pragma unroll
+          for (int k = 0; k < 9; ++k) sout.Q[k][o_slot(start, q)] = Q[k];
+        }
       }
 
-      const uint32_t o = start + q;
+      const uint32_t o = o_slot(start, q);
       sout.x[0][o] = x[0];
       sout.x[1][o] = x[1];
       sout.x[2][o] = x[2];
-      if (kind != kFluid) {
+      if (material_has_F(kind)) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) sout.F[k][o] = F[k];
       }
-      if (kind != kFixedCorotated) sout.aux[o] = aux;
+      if (material_has_aux(kind)) sout.aux[o] = aux;
       if (md.track_ids) sout.id[o] = sin.id[iin];
 
       // Rebin record: direction code of (old block - new block), 27 = lost.
@@ -714,7 +740,10 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
       }
 
       // P2G at the new position (include/mpm_algorithm.cuh:1687-1792):
-      // A = C m - ndt V (D/2)^-1 tau, scaled here per unit mass and by dx.
+      // A = C m - ndt V M tau, scaled here per unit mass and by dx.  The
+      // reference adds the new position's D onto the G2P D of the old position
+      // (it never resets it, :1524,1604,1729) and inverts half the sum (:1732),
+      // so M = (0.5 (D_old + D_new))^-1.
       AxisStencil st[2][3];
       int lb[2][3];
 #pragma unroll
@@ -727,7 +756,7 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
       float D6[6], Di6[6], Di[9], DT[9];
       d_matrix(st, dx, D6);
 #pragma unroll
-      for (int k = 0; k < 6; ++k) D6[k] *= 0.5f;
+      for (int k = 0; k < 6; ++k) D6[k] = 0.5f * (Dold[k] + D6[k]);
       inv_sym3(D6[0], D6[1], D6[2], D6[3], D6[4], D6[5], Di6);
       sym_to_full(Di6, Di);
       matmul3(Di, tau, DT);
@@ -1143,6 +1172,10 @@ __global__ void setup_gather_kernel(ModelDev md, uint32_t nstack, uint32_t n, co
     for (int k = 0; k < 9; ++k) st.F[k][i] = (k & 3) ? 0.f : 1.f;
   }
   if (st.aux) st.aux[i] = md.smat ? md.smat[scene_of(md.sstart, nstack, s)].aux0 : aux0;
+  if (st.Q[0]) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) st.Q[k][i] = 0.f;
+  }
   if (st.id) st.id[i] = s;
   const uint32_t vs = nv == 1 ? 0u : s;
   md.vel_in[3 * i] = v[3 * vs];
@@ -1212,17 +1245,17 @@ __global__ void __launch_bounds__(NT) probe_kernel(SceneDev sc, ModelDev md, Gri
         ox[3 * o + 2] = x[2];
       }
       if (oF) {
-        const bool hasF = kind != kFluid && sin.F[0];
+        const bool hasF = material_has_F(kind) && sin.F[0];
 #pragma unroll
         for (int k = 0; k < 9; ++k) oF[9 * o + k] = hasF ? sin.F[k][iin] : ((k & 3) ? 0.f : 1.f);
       }
-      if (oaux) oaux[o] = (kind != kFixedCorotated && sin.aux) ? sin.aux[iin] : 0.f;
+      if (oaux) oaux[o] = (material_has_aux(kind) && sin.aux) ? sin.aux[iin] : 0.f;
       if (oid) oid[o] = pid;
       if (ov) {
         const float xs[3] = {x[0] * sc.inv_dx, x[1] * sc.inv_dx, x[2] * sc.inv_dx};
-        float v[3], C[9];
+        float v[3], C[9], D6[6];
         bool inside = true;
-        g2p(vtile, xs, key, sc.dx, v, C, inside);
+        g2p(vtile, xs, key, sc.dx, v, C, inside, D6);
         ov[3 * o] = v[0];
         ov[3 * o + 1] = v[1];
         ov[3 * o + 2] = v[2];
@@ -1268,8 +1301,12 @@ __global__ void debug_constitutive_kernel(MaterialParams mat, uint32_t n, const 
     }
     if (mat.kind == kFixedCorotated)
       stress_fixed_corotated(mat.p[0], mat.p[1], f, t);
-    else
+    else if (mat.kind == kDruckerPrager)
       stress_drucker_prager(mat.p[0], mat.p[1], f, a, t);
+    else if (mat.kind == kVonMises)
+      stress_von_mises(mat.p[0], mat.p[1], mat.p[2], f, t);
+    else
+      stress_nacc(mat.p, f, a, t);
     for (int k = 0; k < 9; ++k) F[9 * i + k] = f[k];
   }
   if (aux) aux[i] = a;

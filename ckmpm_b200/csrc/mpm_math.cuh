@@ -173,15 +173,23 @@ CKMPM_DEV float ck_w0(float o) {
 }
 
 // ------------------------------------------------------------------ materials
+// Numbering of MPMConstitutiveModel (include/mpm_material.cuh:10-18).
 enum MaterialKind : int32_t {
   kFixedCorotated = 0,
+  kLinear = 1,
   kDruckerPrager = 2,
   kFluid = 3,
+  kVonMises = 4,
+  kNacc = 5,
 };
+
+constexpr int kMaterialParams = 8;
 
 struct MaterialParams {
   int32_t kind;
-  float p[4];  // FC / DP: lambda, mu.  Fluid: bulk, gamma, viscosity, J0.
+  // FC / DP / Linear: lambda, mu.  Fluid: bulk, gamma, viscosity, J0.  Von Mises: mu, lambda, yield
+  // stress.  NACC: mu, lambda, alpha0, beta, hardening factor, M, hardening on (0 / 1).
+  float p[kMaterialParams];
 };
 
 // Fixed-corotated Kirchhoff stress, tau = U diag(2 mu s (s - 1) + lambda J (J - 1)) U^T
@@ -259,6 +267,167 @@ CKMPM_DEV void stress_drucker_prager(float lambda, float mu, float* F, float& lo
 #pragma unroll
     for (int c = 0; c < 3; ++c)
       tau[r * 3 + c] = P[r * 3] * F[c * 3] + P[r * 3 + 1] * F[c * 3 + 1] + P[r * 3 + 2] * F[c * 3 + 2];
+}
+
+// Von Mises plasticity on the Hencky strain of the trial elastic F, then the
+// StVK-Hencky stress of the projected F from its own SVD, as the reference
+// computes it (include/mpm_algorithm.cuh:404-520, include/mpm_material.cuh:480-518):
+//   eps = log S, eps_hat = eps - tr(eps) / 3, f = |eps_hat| - yield / (2 mu);
+//   f > 0: S <- exp(eps - f eps_hat / |eps_hat|), Fe <- U diag(S) V^T;
+//   tau = U diag((2 mu log S + lambda tr log S) / S) V^T Fe^T.
+// Fe holds the trial elastic F on entry and the projected one on exit.
+CKMPM_DEV void stress_von_mises(float mu, float lambda, float yield, float* Fe, float* tau) {
+  float U[9], S[3], V[9];
+  svd3(Fe, U, S, V);
+  float eps[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) eps[i] = logf(S[i]);
+  const float etr = eps[0] + eps[1] + eps[2];
+  float eh[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) eh[i] = eps[i] - etr / 3.0f;
+  const float ehn = sqrtf(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2]);
+  const float yf = ehn - yield / (2.0f * mu);
+  if (yf > 0.0f) {
+    float ns[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) ns[i] = expf(eps[i] - yf * eh[i] / ehn);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        Fe[r * 3 + c] = U[r * 3] * ns[0] * V[c * 3] + U[r * 3 + 1] * ns[1] * V[c * 3 + 1] + U[r * 3 + 2] * ns[2] * V[c * 3 + 2];
+  }
+  svd3(Fe, U, S, V);
+  float ls[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) ls[i] = logf(S[i]);
+  const float lsum = ls[0] + ls[1] + ls[2];
+  float ph[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float inv = 1.0f / S[i];
+    ph[i] = 2.0f * mu * inv * ls[i] + lambda * lsum * inv;
+  }
+  float P[9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      P[r * 3 + c] = U[r * 3] * ph[0] * V[c * 3] + U[r * 3 + 1] * ph[1] * V[c * 3 + 1] + U[r * 3 + 2] * ph[2] * V[c * 3 + 2];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      tau[r * 3 + c] = P[r * 3] * Fe[c * 3] + P[r * 3 + 1] * Fe[c * 3 + 1] + P[r * 3 + 2] * Fe[c * 3 + 2];
+}
+
+// Non-associated Cam-clay (include/mpm_material.cuh:520-669, driven from
+// include/mpm_algorithm.cuh:330-402), restated step for step, including what
+// it does beyond the textbook model, so that results match the reference:
+//  * the projected F is U diag(S) V (V itself, not its transpose); the stress
+//    only sees F F^T = U S^2 U^T, so V never affects the motion, but the stored
+//    F is fixed only up to a rotation on the right;
+//  * the hardening update of the yield-surface branch sits in a loop of 9
+//    identical iterations, so logJp takes the same increment 9 times;
+//  * thresholds written as double literals (1e-4) compare in double.
+// Both branches (pressure clamped to [pMin, p0], or the return to the yield
+// surface) end in the same stress: mu Je_trial^(-2/3) dev(F F^T) + K/2 (J^2 - 1) I.
+// F holds dW F_old on entry and the projected F on exit.
+CKMPM_DEV void stress_nacc(const float* prm, float* F, float& logJp, float* tau) {
+  const float mu = prm[0], lambda = prm[1], beta = prm[3], xi = prm[4], msq = prm[5] * prm[5];
+  const bool hardening = prm[6] != 0.0f;
+  const float K = 2.0f * mu / 3.0f + lambda;
+  float U[9], S[3], V[9];
+  svd3(F, U, S, V);
+  const float p0 = K * (1e-5f + sinhf(xi * (-logJp > 0.0f ? -logJp : 0.0f)));
+  const float pmin = -beta * p0;
+  const float je = S[0] * S[1] * S[2];
+  const float bh[3] = {S[0] * S[0], S[1] * S[1], S[2] * S[2]};
+  const float btr3 = (bh[0] + bh[1] + bh[2]) / 3.0f;
+  const float devf = mu * powf(je, -2.0f / 3.0f);
+  const float sh[3] = {devf * (bh[0] - btr3), devf * (bh[1] - btr3), devf * (bh[2] - btr3)};
+  const float hydro = K * 0.5f * (je - 1.0f / je);
+  const float ptrial = -hydro * je;
+  const float ysh = 3.0f / 2.0f * (1.0f + 2.0f * beta);
+  const float yph = msq * (ptrial - pmin) * (ptrial - p0);
+  const float sn2 = sh[0] * sh[0] + sh[1] * sh[1] + sh[2] * sh[2];
+  const float y = ysh * sn2 + yph;
+  float Sn[3] = {S[0], S[1], S[2]};
+  if (ptrial > p0 || ptrial < pmin) {
+    const float pp = ptrial > p0 ? p0 : pmin;
+    const float jn = sqrtf(-2.0f * pp / K + 1.0f);
+    const float sc = powf(jn, 1.0f / 3.0f);
+    Sn[0] = Sn[1] = Sn[2] = sc;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        F[r * 3 + c] = sc * (U[r * 3] * V[c] + U[r * 3 + 1] * V[3 + c] + U[r * 3 + 2] * V[6 + c]);
+    if (hardening) logJp += logf(je / jn);
+  } else if (static_cast<double>(y) >= 1e-4) {
+    const float coef = powf(je, 2.0f / 3.0f) / mu * sqrtf(-yph / ysh) / sqrtf(sn2);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) Sn[i] = sqrtf(sh[i] * coef + btr3);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        F[r * 3 + c] = U[r * 3] * Sn[0] * V[c] + U[r * 3 + 1] * Sn[1] * V[3 + c] + U[r * 3 + 2] * Sn[2] * V[6 + c];
+    if (hardening && static_cast<double>(p0) > 1e-4 && static_cast<double>(ptrial) < static_cast<double>(p0) - 1e-4 &&
+        static_cast<double>(ptrial) > 1e-4 + static_cast<double>(pmin)) {
+      const float pc = (1.0f - beta) * p0 / 2.0f;
+      const float qt = sqrtf(3.0f / 2.0f * sn2);
+      float d0 = pc - ptrial, d1 = -qt;
+      const float dn = sqrtf(d0 * d0 + d1 * d1);
+      d0 /= dn;
+      d1 /= dn;
+      const float A = msq * d0 * d0 + (1.0f + 2.0f * beta) * d1 * d1;
+      const float B = msq * d0 * (2.0f * pc - p0 - pmin);
+      const float C = msq * (pc - pmin) * (pc - p0);
+      const float disc = B * B - 4.0f * A * C;
+      const float l1 = (-B + sqrtf(disc)) / (2.0f * A);
+      const float l2 = (-B - sqrtf(disc)) / (2.0f * A);
+      const float p1 = pc + l1 * d0, p2 = pc + l2 * d0;
+      const float pf = (ptrial - pc) * (p1 - pc) > 0.0f ? p1 : p2;
+      const float jsq = -2.0f * pf / K + 1.0f;
+      const float jn = sqrtf(jsq > 0.0f ? jsq : -jsq);
+      if (static_cast<double>(jn) > 1e-4) {
+        const float inc = logf(je / jn);
+        for (int it = 0; it < 9; ++it) logJp += inc;
+      }
+    }
+  }
+  const float J = Sn[0] * Sn[1] * Sn[2];
+  float b[9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) b[r * 3 + c] = F[r * 3] * F[c * 3] + F[r * 3 + 1] * F[c * 3 + 1] + F[r * 3 + 2] * F[c * 3 + 2];
+  const float btr = (b[0] + b[4] + b[8]) / 3.0f;
+  const float hc = K * 0.5f * (J * J - 1.0f);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) tau[k] = devf * (b[k] - ((k & 3) ? 0.0f : btr));
+  tau[0] += hc;
+  tau[4] += hc;
+  tau[8] += hc;
+}
+
+// Linear model as the reference updates it (include/mpm_algorithm.cuh:107-191):
+// F <- dW F (done by the caller); the stored stress Q <- (Q + 50 (C + C^T - I) dt)
+// det(F), with its rows 1 and 2 zeroed; tau = Q.  lambda and mu are not read.
+CKMPM_DEV void stress_linear(const float* C, float dt, const float* F, float* Q, float* tau) {
+  const float detF = det3(F);
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int k = r * 3 + c;
+      const float t = 50.0f * (C[k] + C[c * 3 + r] - ((k & 3) ? 0.0f : 1.0f)) * dt;
+      Q[k] = r == 0 ? (Q[k] + t) * detF : 0.0f;
+    }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) tau[k] = Q[k];
 }
 
 // J-fluid: J += tr(C) dt J; p = bulk (J^-gamma - 1); tau = J (visc (C + C^T) - p I)

@@ -27,8 +27,9 @@ import numpy as np
 
 from . import _capi as capi
 
-ConstitutiveModel = {"fixed_corotated": capi.FIXED_COROTATED, "drucker_prager": capi.DRUCKER_PRAGER,
-                     "fluid": capi.FLUID}
+ConstitutiveModel = {"fixed_corotated": capi.FIXED_COROTATED, "linear": capi.LINEAR,
+                     "drucker_prager": capi.DRUCKER_PRAGER, "fluid": capi.FLUID, "von_mises": capi.VON_MISES,
+                     "nacc": capi.NACC}
 
 
 def compute_lame_parameters(E: float, nu: float) -> tuple[float, float]:
@@ -50,11 +51,14 @@ def evaluate_timestep(dx: float, E: float, nu: float, rho: float, cfl: float = 0
 
 @dataclass
 class MPMMaterial:
-    """One constitutive model and its parameters.
+    """One constitutive model and its parameters, as MaterialParameter_ of
+    MPMMaterial<k> (include/mpm_material.cuh:24-257):
 
-    kind: 'fixed_corotated' | 'drucker_prager' (params lambda_, mu_) or
-    'fluid' (bulk_, gamma_, viscosity_, J0_), as MaterialParameter_ in
-    include/mpm_material.cuh:63-175.
+    * 'fixed_corotated' | 'drucker_prager' | 'linear': lambda_, mu_;
+    * 'fluid': bulk_, gamma_, viscosity_, J0_;
+    * 'von_mises': mu_, lambda_, yield_stress_;
+    * 'nacc' (non-associated Cam-clay): mu_, lambda_, alpha0_, beta_,
+      hardening_factor_, m_, hardening_on_.
     """
     kind: str
     lambda_: float = 0.0
@@ -63,6 +67,12 @@ class MPMMaterial:
     gamma_: float = 0.0
     viscosity_: float = 0.0
     J0_: float = 1.0
+    yield_stress_: float = 0.0
+    alpha0_: float = 0.0
+    beta_: float = 0.0
+    hardening_factor_: float = 0.0
+    m_: float = 0.0
+    hardening_on_: bool = True
 
     @staticmethod
     def fixed_corotated(lambda_: float, mu_: float) -> "MPMMaterial":
@@ -73,17 +83,39 @@ class MPMMaterial:
         return MPMMaterial("drucker_prager", lambda_=lambda_, mu_=mu_)
 
     @staticmethod
+    def linear(lambda_: float, mu_: float) -> "MPMMaterial":
+        return MPMMaterial("linear", lambda_=lambda_, mu_=mu_)
+
+    @staticmethod
     def fluid(bulk: float, gamma: float, viscosity: float, J0: float = 1.0) -> "MPMMaterial":
         return MPMMaterial("fluid", bulk_=bulk, gamma_=gamma, viscosity_=viscosity, J0_=J0)
+
+    @staticmethod
+    def von_mises(mu: float, lambda_: float, yield_stress: float) -> "MPMMaterial":
+        return MPMMaterial("von_mises", mu_=mu, lambda_=lambda_, yield_stress_=yield_stress)
+
+    @staticmethod
+    def nacc(mu: float, lambda_: float, alpha0: float, beta: float, hardening_factor: float, m: float,
+             hardening_on: bool = True) -> "MPMMaterial":
+        return MPMMaterial("nacc", mu_=mu, lambda_=lambda_, alpha0_=alpha0, beta_=beta,
+                           hardening_factor_=hardening_factor, m_=m, hardening_on_=hardening_on)
 
     @property
     def kind_code(self) -> int:
         return ConstitutiveModel[self.kind]
 
     def params(self) -> list[float]:
+        """The 8 parameter slots of ckmpm_material.p, in the reference's field order."""
         if self.kind == "fluid":
-            return [self.bulk_, self.gamma_, self.viscosity_, self.J0_]
-        return [self.lambda_, self.mu_, 0.0, 0.0]
+            p = [self.bulk_, self.gamma_, self.viscosity_, self.J0_]
+        elif self.kind == "von_mises":
+            p = [self.mu_, self.lambda_, self.yield_stress_]
+        elif self.kind == "nacc":
+            p = [self.mu_, self.lambda_, self.alpha0_, self.beta_, self.hardening_factor_, self.m_,
+                 1.0 if self.hardening_on_ else 0.0]
+        else:
+            p = [self.lambda_, self.mu_]
+        return [float(v) for v in p] + [0.0] * (capi.MATERIAL_PARAMS - len(p))
 
     def to_c(self) -> capi.Material:
         m = capi.Material()
@@ -417,11 +449,22 @@ class MPMEngine:
         return self.scene.counters()["steps"] - start
 
 
+def load_raw_positions(path: str | Path) -> np.ndarray:
+    """Particle positions from a raw float32 xyz file (the reference's asset/*.bin format)."""
+    a = np.fromfile(path, dtype=np.float32)
+    if a.size % 3:
+        raise ValueError(f"{path}: {a.size} floats is not a whole number of xyz triples")
+    return a.reshape(-1, 3)
+
+
 def load_scene_json(path: str | Path) -> tuple[MPMConfig, list[MPMModel]]:
     """JSON scene files (a project addition; the reference's importer at
     include/mpm_io.h:168-199 is commented out).  Schema:
       {"config": {MPMConfig fields}, "models": [{"material": {...}, "mass": m,
-       "volume": v, "positions": "file.npy" | [[x,y,z],...], "velocity": [[vx,vy,vz]]}]}
+       "volume": v, "positions": "file.npy" | "file.bin" | [[x,y,z],...], "velocity": [[vx,vy,vz]]}]}
+    A ".bin" file is raw float32 xyz triples, the reference's asset format
+    (asset/*.bin, read by the scenes' SetupModel, e.g.
+    tests/sand_armadillo/test_sand_armadillo.cuh:137-192).
     """
     path = Path(path)
     spec = json.loads(path.read_text())
@@ -434,7 +477,7 @@ def load_scene_json(path: str | Path) -> tuple[MPMConfig, list[MPMModel]]:
         mat = MPMMaterial(**md["material"])
         pos = md["positions"]
         if isinstance(pos, str):
-            pos = np.load(path.parent / pos)
+            pos = load_raw_positions(path.parent / pos) if pos.endswith(".bin") else np.load(path.parent / pos)
         models.append(MPMModel(md["mass"], md["volume"], np.asarray(pos, np.float32),
                                np.asarray(md.get("velocity", [[0, 0, 0]]), np.float32), mat,
                                md.get("freeze_time", 0.0)))

@@ -136,6 +136,40 @@ def small_sand(seed: int = 0, dx: float = 1 / 64, r: float = 0.1, h: float = 0.2
     return cfg, [MPMModel(rho * vol, vol, x, np.zeros((1, 3), np.float32), MPMMaterial.drucker_prager(lam, mu))]
 
 
+def material_cube(kind: str, seed: int = 0, dx: float = 1 / 64, lo=(0.42, 0.42, 0.42), hi=(0.58, 0.58, 0.58),
+                  ppc: int = 8, rho: float = 1000.0, gravity: float = -9.8,
+                  track_ids: bool = True) -> tuple[MPMConfig, list[MPMModel]]:
+    """Small cube of one of the reference's other materials, with an initial
+    velocity field that loads it at once (parity tests):
+    * 'von_mises': E 2e4, nu 0.3, yield stress 100 Pa, shear v = (20 (y - 0.5), 0, 0);
+    * 'nacc': E 2e4, nu 0.4 (mu, lambda in the model's field order), alpha0 -0.01,
+      beta 0.5, hardening factor 0.8, M 2.36, hardening on (the reference's oreo
+      scene, tests/oreo/test_oreo.cuh), converging v = -10 (x - centre);
+    * 'linear': E 5e4, nu 0.3, v0 = (0, -1, 0)."""
+    rng = np.random.default_rng(seed)
+    x = box_particles(lo, hi, dx, ppc, rng)
+    c = (np.asarray(lo) + np.asarray(hi)) / 2
+    if kind == "von_mises":
+        lam, mu = compute_lame_parameters(2e4, 0.3)
+        mat = MPMMaterial.von_mises(mu, lam, 100.0)
+        v = np.zeros_like(x)
+        v[:, 0] = 20.0 * (x[:, 1] - c[1])
+    elif kind == "nacc":
+        lam, mu = compute_lame_parameters(2e4, 0.4)
+        mat = MPMMaterial.nacc(mu, lam, -0.01, 0.5, 0.8, 2.36, True)
+        v = (-10.0 * (x - c)).astype(np.float32)
+    elif kind == "linear":
+        lam, mu = compute_lame_parameters(5e4, 0.3)
+        mat = MPMMaterial.linear(lam, mu)
+        v = np.asarray([[0.0, -1.0, 0.0]], np.float32)
+    else:
+        raise ValueError(kind)
+    n_cells = round(1.0 / dx)
+    cfg = MPMConfig(dx=dx, domain_blocks=(n_cells // 4,) * 3, gravity=gravity, track_ids=track_ids)
+    vol = dx ** 3 / ppc
+    return cfg, [MPMModel(rho * vol, vol, x, np.asarray(v, np.float32), mat)]
+
+
 def batched_scenes(n_scenes: int = 256, seed: int = 0, dx: float = 1 / 64, ppc: int = 8, n_min: int = 2000,
                    n_max: int = 200000, dt: float = 1e-4, gravity: float = -9.8) -> tuple[MPMConfig, list[MPMModel]]:
     """Batched form: n_scenes independent scenes on a 64^3 domain (dx = 1/64,

@@ -39,8 +39,11 @@ typedef enum ckmpm_status {
  * (include/mpm_material.cuh:10-18). */
 typedef enum ckmpm_material_kind {
   CKMPM_FIXED_COROTATED = 0,
+  CKMPM_LINEAR = 1,
   CKMPM_DRUCKER_PRAGER = 2,
-  CKMPM_FLUID = 3
+  CKMPM_FLUID = 3,
+  CKMPM_VON_MISES = 4,
+  CKMPM_NACC = 5 /* kNonAssociatedCamClay */
 } ckmpm_material_kind;
 
 /* Grid boundary rules.  STICKY_BLOCKS is the reference's built-in rule: every
@@ -71,12 +74,17 @@ typedef struct ckmpm_scene_desc {
 /* Keep a per-particle original index so state can be returned in input order. */
 #define CKMPM_FLAG_TRACK_IDS 1u
 
-/* Material parameters, MPMMaterial<k>::MaterialParameter_
- * (include/mpm_material.cuh:63-175): FC / DP use p[0] = lambda, p[1] = mu;
- * fluid uses p[0] = bulk, p[1] = gamma, p[2] = viscosity, p[3] = J0. */
+/* Material parameters in the field order of each MPMMaterial<k>::MaterialParameter_
+ * (include/mpm_material.cuh:24-257):
+ *   FIXED_COROTATED, DRUCKER_PRAGER, LINEAR: p[0] = lambda, p[1] = mu;
+ *   FLUID: p[0] = bulk, p[1] = gamma, p[2] = viscosity, p[3] = J0;
+ *   VON_MISES: p[0] = mu, p[1] = lambda, p[2] = yield stress;
+ *   NACC: p[0] = mu, p[1] = lambda, p[2] = alpha0 (initial logJp), p[3] = beta,
+ *         p[4] = hardening factor, p[5] = M, p[6] = hardening on (0 or 1).
+ * Unused entries are ignored. */
 typedef struct ckmpm_material {
   int32_t kind; /* ckmpm_material_kind */
-  float p[4];
+  float p[8];
 } ckmpm_material;
 
 /* Replaces MPMEngine<GridConfig>::GetInstance() + Initialize(config)
@@ -126,8 +134,9 @@ ckmpm_status ckmpm_get_count(ckmpm_scene* s, int32_t model, uint32_t* n_live);
 
 /* Per-particle state, replacing the export path's RetrieveParticleBuffer +
  * D2H (include/mpm_algorithm.cuh:1977-2020, include/mpm_engine.cuh:386-454).
- * Arrays hold n_live entries (x, v: 3 floats; F: 9 floats row-major; aux:
- * J for fluid, logJp for Drucker-Prager; id: input index).  With
+ * Arrays hold n_live entries (x, v: 3 floats; F: 9 floats row-major, the
+ * identity for the fluid; aux: J for the fluid, logJp for Drucker-Prager and
+ * NACC, 0 otherwise; id: input index).  With
  * CKMPM_FLAG_TRACK_IDS the arrays are in input order and id is the identity
  * over live particles; without it they are in block order.  v is the velocity
  * the next G2P interpolates at each particle (the reference's conservation
@@ -162,7 +171,8 @@ ckmpm_status ckmpm_step_profiled(ckmpm_scene* s, uint32_t nsteps, float dt, doub
  * the GPU exactly as the substep does (dW = I + dt C; F <- dW F; SVD; return
  * map; stress).  F (9n), aux (n) are updated in place; tau (9n) receives the
  * Kirchhoff stress; U, S, V (9n, 3n, 9n, may be NULL) receive the SVD of the
- * trial F.  Host pointers. */
+ * trial F.  Every kind but LINEAR (whose stress is stored per particle).
+ * Host pointers. */
 ckmpm_status ckmpm_debug_constitutive(const ckmpm_material* material, uint32_t n, const float* C, float dt,
                                       float* F, float* aux, float* tau, float* U, float* S, float* V);
 

@@ -56,10 +56,13 @@ struct GridBlock {
 
 struct Model {
   int kind = 0;           // 0 fixed-corotated, 2 Drucker-Prager, 3 J-fluid
-  double p[4] = {0, 0, 0, 0};  // FC/DP: lambda, mu; fluid: bulk, gamma, viscosity, J0
+  // FC / DP / linear: lambda, mu; fluid: bulk, gamma, viscosity, J0; von Mises: mu,
+  // lambda, yield stress; NACC: mu, lambda, alpha0, beta, hardening factor, M, hardening on.
+  double p[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   double mass = 0, vol = 0;
   int n = 0;
-  std::vector<double> x, F, aux;  // aux: J (fluid) or logJp (DP)
+  std::vector<double> x, F, aux;  // aux: J (fluid) or logJp (DP, NACC)
+  std::vector<double> Q;          // the linear model's stored stress (9 per particle)
   std::vector<double> v0;         // initial velocities (n or 1 entries of 3)
   std::vector<double> plam, pmu;  // optional per-particle Lame parameters (fixed-corotated)
   std::vector<uint8_t> alive;
@@ -378,6 +381,132 @@ void stress_dp(double lambda, double mu, double* F, double* logJp, double* tau) 
   matmul3(P, Ft, tau);
 }
 
+// Von Mises plasticity on the Hencky strain of the trial elastic F, then the
+// StVK-Hencky stress of the projected F from its own SVD,
+// mpm_algorithm.cuh:404-520 and mpm_material.cuh:480-518.  F in/out.
+void stress_vm(double mu, double lambda, double yield, double* F, double* tau) {
+  double U[9], S[3], V[9];
+  svd3(F, U, S, V);
+  double eps[3];
+  for (int i = 0; i < 3; ++i) eps[i] = std::log(S[i]);
+  const double etr = eps[0] + eps[1] + eps[2];
+  double eh[3];
+  for (int i = 0; i < 3; ++i) eh[i] = eps[i] - etr / 3.0;
+  const double ehn = std::sqrt(eh[0] * eh[0] + eh[1] * eh[1] + eh[2] * eh[2]);
+  const double yf = ehn - yield / (2.0 * mu);
+  if (yf > 0.0) {
+    double ns[3];
+    for (int i = 0; i < 3; ++i) ns[i] = std::exp(eps[i] - yf * eh[i] / ehn);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) {
+        double acc = 0;
+        for (int k = 0; k < 3; ++k) acc += U[r * 3 + k] * ns[k] * V[c * 3 + k];
+        F[r * 3 + c] = acc;
+      }
+  }
+  svd3(F, U, S, V);
+  double ls[3];
+  for (int i = 0; i < 3; ++i) ls[i] = std::log(S[i]);
+  const double lsum = ls[0] + ls[1] + ls[2];
+  double P[9];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double acc = 0;
+      for (int k = 0; k < 3; ++k) acc += U[r * 3 + k] * ((2.0 * mu * ls[k] + lambda * lsum) / S[k]) * V[c * 3 + k];
+      P[r * 3 + c] = acc;
+    }
+  double Ft[9];
+  transpose3(F, Ft);
+  matmul3(P, Ft, tau);
+}
+
+// Non-associated Cam-clay, mpm_material.cuh:520-669 (driven from
+// mpm_algorithm.cuh:330-402), restated step for step: the projected F is
+// U diag(S) V (V, not its transpose); the hardening increment of the
+// yield-surface branch is applied 9 times (it sits in a loop of 9 identical
+// iterations); both branches end in the same stress from the projected F
+// (:649-667).  F in/out; tau out.
+void stress_nacc(const double* prm, double* F, double* logJp, double* tau) {
+  const double mu = prm[0], lambda = prm[1], beta = prm[3], xi = prm[4], msq = prm[5] * prm[5];
+  const bool hardening = prm[6] != 0.0;
+  const double K = 2.0 * mu / 3.0 + lambda;
+  double U[9], S[3], V[9];
+  svd3(F, U, S, V);
+  const double p0 = K * (1e-5 + std::sinh(xi * std::max(-*logJp, 0.0)));
+  const double pmin = -beta * p0;
+  const double je = S[0] * S[1] * S[2];
+  const double bh[3] = {S[0] * S[0], S[1] * S[1], S[2] * S[2]};
+  const double btr3 = (bh[0] + bh[1] + bh[2]) / 3.0;
+  const double devf = mu * std::pow(je, -2.0 / 3.0);
+  double sh[3];
+  for (int i = 0; i < 3; ++i) sh[i] = devf * (bh[i] - btr3);
+  const double ptrial = -K * 0.5 * (je - 1.0 / je) * je;
+  const double ysh = 1.5 * (1.0 + 2.0 * beta);
+  const double yph = msq * (ptrial - pmin) * (ptrial - p0);
+  const double sn2 = sh[0] * sh[0] + sh[1] * sh[1] + sh[2] * sh[2];
+  const double y = ysh * sn2 + yph;
+  auto u_diag_v = [&](const double* d) {  // F = U diag(d) V
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) {
+        double acc = 0;
+        for (int k = 0; k < 3; ++k) acc += U[r * 3 + k] * d[k] * V[k * 3 + c];
+        F[r * 3 + c] = acc;
+      }
+  };
+  double Sn[3] = {S[0], S[1], S[2]};
+  if (ptrial > p0 || ptrial < pmin) {
+    const double pp = ptrial > p0 ? p0 : pmin;
+    const double jn = std::sqrt(-2.0 * pp / K + 1.0);
+    const double sc = std::cbrt(jn);
+    Sn[0] = Sn[1] = Sn[2] = sc;
+    u_diag_v(Sn);
+    if (hardening) *logJp += std::log(je / jn);
+  } else if (y >= 1e-4) {
+    const double coef = std::pow(je, 2.0 / 3.0) / mu * std::sqrt(-yph / ysh) / std::sqrt(sn2);
+    for (int i = 0; i < 3; ++i) Sn[i] = std::sqrt(sh[i] * coef + btr3);
+    u_diag_v(Sn);
+    if (hardening && p0 > 1e-4 && ptrial < p0 - 1e-4 && ptrial > 1e-4 + pmin) {
+      const double pc = (1.0 - beta) * p0 / 2.0;
+      const double qt = std::sqrt(1.5 * sn2);
+      double d0 = pc - ptrial, d1 = -qt;
+      const double dn = std::sqrt(d0 * d0 + d1 * d1);
+      d0 /= dn;
+      d1 /= dn;
+      const double A = msq * d0 * d0 + (1.0 + 2.0 * beta) * d1 * d1;
+      const double B = msq * d0 * (2.0 * pc - p0 - pmin);
+      const double C = msq * (pc - pmin) * (pc - p0);
+      const double disc = B * B - 4.0 * A * C;
+      const double l1 = (-B + std::sqrt(disc)) / (2.0 * A), l2 = (-B - std::sqrt(disc)) / (2.0 * A);
+      const double p1 = pc + l1 * d0, p2 = pc + l2 * d0;
+      const double pf = (ptrial - pc) * (p1 - pc) > 0.0 ? p1 : p2;
+      const double jsq = -2.0 * pf / K + 1.0;
+      const double jn = std::sqrt(std::fabs(jsq));
+      if (jn > 1e-4)
+        for (int it = 0; it < 9; ++it) *logJp += std::log(je / jn);
+    }
+  }
+  const double J = Sn[0] * Sn[1] * Sn[2];
+  double b[9];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) b[r * 3 + c] = F[r * 3] * F[c * 3] + F[r * 3 + 1] * F[c * 3 + 1] + F[r * 3 + 2] * F[c * 3 + 2];
+  const double btr = (b[0] + b[4] + b[8]) / 3.0;
+  const double hc = K * 0.5 * (J * J - 1.0);
+  for (int k = 0; k < 9; ++k) tau[k] = devf * (b[k] - ((k & 3) ? 0.0 : btr)) + ((k & 3) ? 0.0 : hc);
+}
+
+// Linear model as the reference updates it, mpm_algorithm.cuh:107-191: with
+// F already dW F, the stored stress Q <- (Q + 50 (C + C^T - I) dt) det(F) with
+// rows 1 and 2 zeroed; tau = Q.
+void stress_linear(const double* C, double dt, const double* F, double* Q, double* tau) {
+  const double d = det3(F);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      const int k = r * 3 + c;
+      Q[k] = r == 0 ? (Q[k] + 50.0 * (C[k] + C[c * 3 + r] - ((k & 3) ? 0.0 : 1.0)) * dt) * d : 0.0;
+    }
+  for (int k = 0; k < 9; ++k) tau[k] = Q[k];
+}
+
 // J-fluid: J += tr(C) dt J; p = bulk (J^-gamma - 1); tau = J (visc (C + C^T) - p I),
 // mpm_algorithm.cuh:528-569 and mpm_material.cuh:468-477.
 void stress_fluid(const double* prm, const double* C, double dt, double* J, double* tau) {
@@ -442,8 +571,11 @@ void substep(Scene& s, double next_dt) {
       particle_block(x, invdx, K);
       double v[3], C[9];
       g2p(s, x, dt, v, C);
-      double xn[3];
-      for (int a = 0; a < 3; ++a) xn[a] = x[a] + dt * v[a];
+      double xn[3], xold[3];
+      for (int a = 0; a < 3; ++a) {
+        xold[a] = x[a];
+        xn[a] = x[a] + dt * v[a];
+      }
       double tau[9];
       if (m.kind == 3) {
         stress_fluid(m.p, C, dt, &m.aux[p], tau);
@@ -454,8 +586,14 @@ void substep(Scene& s, double next_dt) {
         matmul3(dW, F, F);
         if (m.kind == 0)
           stress_fc(m.plam.empty() ? m.p[0] : m.plam[p], m.pmu.empty() ? m.p[1] : m.pmu[p], F, tau);
-        else
+        else if (m.kind == 2)
           stress_dp(m.p[0], m.p[1], F, &m.aux[p], tau);
+        else if (m.kind == 4)
+          stress_vm(m.p[0], m.p[1], m.p[2], F, tau);
+        else if (m.kind == 5)
+          stress_nacc(m.p, F, &m.aux[p], tau);
+        else
+          stress_linear(C, dt, F, &m.Q[9 * p], tau);
       }
       for (int a = 0; a < 3; ++a) x[a] = xn[a];
       // Advection: new block must be a neighbour inside the domain.
@@ -478,9 +616,13 @@ void substep(Scene& s, double next_dt) {
         ++s.window_skips;
         continue;
       }
-      double D[9], Di[9], halfD[9];
+      // The reference's P2G adds the new position's D onto the G2P D of the old
+      // position (it is never reset in between, mpm_algorithm.cuh:1524,1604,1729)
+      // and inverts half the sum (:1732).
+      double D[9], Dold[9], Di[9], halfD[9];
       d_matrix(xn, invdx, dx, D);
-      for (int k = 0; k < 9; ++k) halfD[k] = 0.5 * D[k];
+      d_matrix(xold, invdx, dx, Dold);
+      for (int k = 0; k < 9; ++k) halfD[k] = 0.5 * (D[k] + Dold[k]);
       inv3(halfD, Di);
       double DT[9];
       matmul3(Di, tau, DT);
@@ -519,14 +661,15 @@ int oracle_add_model(void* h, int kind, const double* params, int n, const float
   Scene* s = static_cast<Scene*>(h);
   Model m;
   m.kind = kind;
-  for (int k = 0; k < 4; ++k) m.p[k] = params[k];
+  for (int k = 0; k < 8; ++k) m.p[k] = params[k];
   m.mass = mass;
   m.vol = vol;
   m.n = n;
   m.x.assign(x, x + 3 * static_cast<size_t>(n));
   m.F.assign(9 * static_cast<size_t>(n), 0.0);
   for (int p = 0; p < n; ++p) m.F[9 * p] = m.F[9 * p + 4] = m.F[9 * p + 8] = 1.0;
-  m.aux.assign(n, kind == 3 ? params[3] : 0.0);
+  m.aux.assign(n, kind == 3 ? params[3] : (kind == 5 ? params[2] : 0.0));
+  if (kind == 1) m.Q.assign(9 * static_cast<size_t>(n), 0.0);
   m.v0.assign(v, v + 3 * static_cast<size_t>(nv));
   m.alive.assign(n, 1);
   m.skipped.assign(n, 0);
@@ -762,8 +905,12 @@ void oracle_constitutive(int kind, const double* params, const double* C, double
   matmul3(dW, F, F);
   if (kind == 0)
     stress_fc(params[0], params[1], F, tau);
-  else
+  else if (kind == 2)
     stress_dp(params[0], params[1], F, aux, tau);
+  else if (kind == 4)
+    stress_vm(params[0], params[1], params[2], F, tau);
+  else if (kind == 5)
+    stress_nacc(params, F, aux, tau);
 }
 
 }  // extern "C"

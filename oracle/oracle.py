@@ -80,7 +80,8 @@ class OracleScene:
     def add_model(self, m) -> int:
         x = np.ascontiguousarray(m.particle_position, np.float32)
         v = np.ascontiguousarray(m.particle_velocity, np.float32)
-        p = np.asarray(m.material.params(), np.float64)
+        p = np.zeros(8, np.float64)
+        p[:len(m.material.params())] = m.material.params()
         idx = lib().oracle_add_model(self._h, m.material.kind_code, _d(p), len(x), _f(x), _f(v), len(v),
                                      m.particle_mass, m.particle_volume)
         self.n.append(len(x))
@@ -177,7 +178,8 @@ def ck_w0(o: float) -> float:
 
 
 def constitutive(kind: int, params, C_, dt, F, aux):
-    p = np.ascontiguousarray(params, np.float64)
+    p = np.zeros(8, np.float64)
+    p[:len(params)] = params
     Cm = np.ascontiguousarray(C_, np.float64).reshape(9)
     Fm = np.ascontiguousarray(F, np.float64).reshape(9).copy()
     a = np.asarray([aux], np.float64)

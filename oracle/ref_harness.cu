@@ -18,8 +18,11 @@
 // sticky x/z walls and ceiling two blocks deep, v_y >= 0 in cells below the floor.
 //
 // Usage: ref_<scene> <manifest> <fps> <frames> <dt> <outdir> <mode>
-//   manifest: one model per line: <material> <p0> <p1> <p2> <p3> <mass> <volume> <x.bin> <v.bin>
-//   material: fc | dp | fluid; params: lambda mu 0 0 (fc/dp) or bulk gamma viscosity J0 (fluid)
+//   manifest: one model per line: <material> <p0> ... <p7> <mass> <volume> <x.bin> <v.bin>
+//   material and parameters, in the field order of each MaterialParameter_
+//   (include/mpm_material.cuh:24-257): fc | dp | linear: lambda mu; fluid: bulk
+//   gamma viscosity J0; vm: mu lambda yield; nacc: mu lambda alpha0 beta
+//   hardeningFactor M hardeningOn
 //   x.bin / v.bin: float32 xyz triples (v.bin holds 1 or n velocities)
 //   mode 0: export raw positions every frame (outdir/model_0_particle_frame_<k>.txt)
 //   mode 1: profile mode, no export; the reference prints its MPMBenchmark statistics
@@ -146,8 +149,10 @@ int main(int argc, char** argv) {
     if (line.empty()) continue;
     std::istringstream in(line);
     std::string mat, xf, vf;
-    float p[4], mass, volume;
-    in >> mat >> p[0] >> p[1] >> p[2] >> p[3] >> mass >> volume >> xf >> vf;
+    float p[8], mass, volume;
+    in >> mat;
+    for (float& q : p) in >> q;
+    in >> mass >> volume >> xf >> vf;
     xs.push_back(read_xyz(xf.c_str()));
     vs.push_back(read_xyz(vf.c_str()));
     const auto xspan = std::span<const Vector<float, 3>>(xs.back());
@@ -158,6 +163,16 @@ int main(int argc, char** argv) {
     } else if (mat == "dp") {
       using M = MPMMaterial<MPMConstitutiveModel::kDruckerPragerStvkhencky>;
       models.emplace_back(MPMModel<M>{mass, volume, xspan, vspan, M{M::MaterialParameter_{p[0], p[1]}}});
+    } else if (mat == "linear") {
+      using M = MPMMaterial<MPMConstitutiveModel::kLinear>;
+      models.emplace_back(MPMModel<M>{mass, volume, xspan, vspan, M{M::MaterialParameter_{p[0], p[1]}}});
+    } else if (mat == "vm") {
+      using M = MPMMaterial<MPMConstitutiveModel::kVonMises>;
+      models.emplace_back(MPMModel<M>{mass, volume, xspan, vspan, M{M::MaterialParameter_{p[0], p[1], p[2]}}});
+    } else if (mat == "nacc") {
+      using M = MPMMaterial<MPMConstitutiveModel::kNonAssociatedCamClay>;
+      models.emplace_back(
+          MPMModel<M>{mass, volume, xspan, vspan, M{M::MaterialParameter_{p[0], p[1], p[2], p[3], p[4], p[5], p[6] != 0.f}}});
     } else {
       using M = MPMMaterial<MPMConstitutiveModel::kFluid>;
       models.emplace_back(MPMModel<M>{mass, volume, xspan, vspan, M{M::MaterialParameter_{p[0], p[1], p[2], p[3]}}});

@@ -17,7 +17,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 REF_DIR = HERE / "_ref"
 
-KIND_NAMES = {0: "fc", 2: "dp", 3: "fluid"}
+KIND_NAMES = {0: "fc", 1: "linear", 2: "dp", 3: "fluid", 4: "vm", 5: "nacc"}
 
 
 def binary(family: str) -> Path:

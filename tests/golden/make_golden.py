@@ -43,6 +43,9 @@ def golden_scenes():
     yield "fluid", "jelly", cfg, m[0]
     cfg, m = scenes.small_sand(r=0.06, h=0.15)
     yield "sand_dp", "slip", cfg, m[0]
+    for kind in ("von_mises", "nacc", "linear"):
+        cfg, m = scenes.material_cube(kind)
+        yield kind, "jelly", cfg, m[0]
 
 
 # Adaptive-dt fixture: the reference's own Simulate picks every dt (CFL on the
@@ -60,11 +63,16 @@ def checksum(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()[:16]
 
 
-def main(outdir: str) -> None:
+def main(outdir: str, only: list[str] | None = None) -> None:
+    """Write the fixtures of every scene, or only of the named ones (merged into
+    an existing golden.json)."""
     out = Path(outdir)
     out.mkdir(parents=True, exist_ok=True)
-    meta = {}
+    meta_path = out / "golden.json"
+    meta = json.loads(meta_path.read_text()) if (only and meta_path.exists()) else {}
     for name, family, cfg, model in golden_scenes():
+        if only and name not in only:
+            continue
         runs = []
         for _ in range(2):
             _, d = ref_runner.run(family, model, FPS, FRAMES, DT, 0)
@@ -83,6 +91,9 @@ def main(outdir: str) -> None:
                       "mass": model.particle_mass, "volume": model.particle_volume,
                       "counts": [int(len(runs[0][k])) for k in range(FRAMES)]}
         print(name, meta[name]["n"], "spread", max(spread), flush=True)
+    if only and ADAPTIVE["name"] not in only:
+        meta_path.write_text(json.dumps(meta, indent=1))
+        return
     cfg, model = adaptive_scene()
     a = ADAPTIVE
     runs = []
@@ -96,8 +107,9 @@ def main(outdir: str) -> None:
                        "frames": a["frames"], "kept_frames": list(range(a["frames"])), "adaptive": True,
                        "reference_run_to_run_spread": spread, "counts": [int(len(r)) for r in runs[0]]}
     print(a["name"], meta[a["name"]]["n"], "spread", max(spread), flush=True)
-    (out / "golden.json").write_text(json.dumps(meta, indent=1))
+    meta_path.write_text(json.dumps(meta, indent=1))
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else str(Path(__file__).resolve().parent))
+    # python tests/golden/make_golden.py [outdir] [scene names ...]
+    main(sys.argv[1] if len(sys.argv) > 1 else str(Path(__file__).resolve().parent), sys.argv[2:] or None)

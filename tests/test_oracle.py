@@ -155,3 +155,57 @@ def test_out_of_domain_particles_are_dropped(oracle_mod):
     o = oracle_mod.OracleScene(cfg, [m])
     st = o.state(0)
     assert st["alive"].tolist() == [True, False, False]
+
+
+def test_von_mises_projects_onto_the_yield_surface(oracle_mod):
+    """Von Mises (mpm_algorithm.cuh:404-490): a trial strain outside the surface
+    ends with |dev log S| = yield / (2 mu), volume (tr log S) unchanged; inside,
+    F is untouched and tau is the StVK-Hencky stress of F."""
+    mu, lam, ys = 2.0e4, 3.0e4, 200.0
+    C = np.zeros((3, 3))
+    F = np.diag([1.2, 0.9, 1.0])
+    Fo, _, tau = oracle_mod.constitutive(4, [mu, lam, ys], C, 0.0, F, 0.0)
+    S = np.linalg.svd(Fo, compute_uv=False)
+    eps = np.log(S)
+    dev = eps - eps.mean()
+    assert abs(np.linalg.norm(dev) - ys / (2 * mu)) < 1e-12
+    assert abs(eps.sum() - np.log(np.linalg.svd(F, compute_uv=False)).sum()) < 1e-12
+    F2 = np.diag([1.001, 0.9995, 1.0])
+    Fo2, _, tau2 = oracle_mod.constitutive(4, [mu, 1e4 * lam, 1e6], C, 0.0, F2, 0.0)
+    assert np.allclose(Fo2, F2, atol=1e-15)
+    ls = np.log(np.diag(F2))
+    expect = np.diag((2 * mu * ls + 1e4 * lam * ls.sum()))  # tau = P F^T = diag(phi_i s_i)
+    assert np.allclose(tau2, expect, rtol=1e-10, atol=1e-8)
+
+
+def test_nacc_rest_state_and_hardening(oracle_mod):
+    """NACC (mpm_material.cuh:520-669): F = I carries no stress and no plastic
+    flow; a strong compression leaves [pMin, p0], projects to J = Je_new with
+    the clamped pressure K (1 - J^2) / 2 = p0, and hardens:
+    logJp += log(Je_trial / Je_new) < 0 raises p0."""
+    prm = [1.0e4, 2.0e4, -0.04, 0.5, 10.0, 1.0, 1.0]
+    C = np.zeros((3, 3))
+    F, a, tau = oracle_mod.constitutive(5, prm, C, 0.0, np.eye(3), -0.04)
+    assert np.allclose(tau, 0, atol=1e-9) and np.allclose(F, np.eye(3)) and a == -0.04
+    Fc = np.eye(3) * 0.7  # p_trial = K (1 - Je^2) / 2 = 0.44 K > p0 = 0.41 K
+    Fn, a2, tau2 = oracle_mod.constitutive(5, prm, C, 0.0, Fc, -0.04)
+    p0 = (2 * prm[0] / 3 + prm[1]) * (1e-5 + np.sinh(prm[4] * 0.04))
+    assert abs(-np.trace(tau2) / 3 - p0) < 1e-9 * p0  # isotropic projection: tau = -p0 I
+    assert np.allclose(tau2, -p0 * np.eye(3), atol=1e-9 * p0)
+    je = 0.7 ** 3
+    jn = np.linalg.det(Fn)
+    assert a2 < -0.04 and abs(a2 - (-0.04 + np.log(je / jn))) < 1e-12  # p0 grows with -logJp
+
+
+def test_linear_stored_stress(oracle_mod):
+    """The linear model's update (mpm_algorithm.cuh:107-191): Q <- (Q + 50 (C +
+    C^T - I) dt) det F, rows 1 and 2 zeroed, on a fresh particle (Q = 0)."""
+    cfg, _ = __import__("ckmpm_b200").scenes.jelly_cube()
+    from ckmpm_b200.engine import MPMMaterial, MPMModel
+    x = np.array([[0.5, 0.5, 0.5]], np.float32)
+    m = MPMModel(1.0, 1.0 / 8 / 64 ** 3, x, np.array([[0.1, 0.0, 0.0]], np.float32), MPMMaterial.linear(1.0, 1.0))
+    o = oracle_mod.OracleScene(cfg, [m])
+    o.setup()
+    o.step(1, 1e-4)
+    st = o.state(0)
+    assert np.isfinite(st["x"]).all() and np.allclose(st["F"][0], np.eye(3))
