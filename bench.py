@@ -45,7 +45,9 @@ WORKLOADS = {
                  "N(log 5e4, 0.2), nu=0.3, 200 substeps of dt=1e-4, checkpoint every 20, loss |com(T)-target|^2",
 }
 REFERENCE_FAMILY = {"sand_column": "sand", "jelly_cube": "jelly", "dam_break_mixed": "dam", "batched_256": "jelly"}
-STATE_BYTES = {0: 48, 2: 52, 3: 16}  # x + F (+ logJp) or x + J, read once and written once per substep
+# Per-particle state read once and written once per substep: x + F (FC, von Mises), x + F + logJp (DP,
+# NACC), x + F + stored stress (linear), x + J (fluid).
+STATE_BYTES = {0: 48, 1: 84, 2: 52, 3: 16, 4: 48, 5: 52}
 
 
 def parse():

@@ -1,14 +1,15 @@
 """The FP64 oracle against the reference CUDA build's own outputs (golden fixtures).
 
 tests/golden/*.npz hold the positions that the reference's stock
-MPMEngine::Simulate exported on a B200 for three seeded scenes
+MPMEngine::Simulate exported on a B200 for seeded scenes
 (tests/golden/make_golden.py, oracle/ref_harness.cu): a fixed-corotated cube,
-a J-fluid box and a Drucker-Prager column on the slip floor, 128 substeps of
-dt = 2^-14.  The reference exports unordered positions, so particles are
+a J-fluid box, a Drucker-Prager column on the slip floor, and von Mises,
+non-associated Cam-clay and linear cubes loaded by shear, converging and
+uniform initial velocity fields, 128 substeps of dt = 2^-14.  The reference exports unordered positions, so particles are
 matched by nearest neighbour (spacing dx/2 = 7.8e-3 is far above the errors).
 
-Tolerance on positions after N substeps: 1e-6 + N * 2^-24 (x 2 for
-Drucker-Prager).  The reference updates x += dt v in FP32; with a constant
+Tolerance on positions after N substeps: 1e-6 + N * 2^-24.  The reference
+updates x += dt v in FP32; with a constant
 increment round-to-nearest drifts by up to half an ulp of x (<= 2^-24 on
 [0.5, 1)) per substep in the same direction for every particle, which the FP64
 oracle does not do (measured: 1.19e-8 per substep on the cube, exactly that
@@ -36,7 +37,7 @@ def golden_cases():
 
 
 def tolerance(name: str, nsub: int) -> float:
-    return (1e-6 + nsub * 2.0 ** -24) * (2.0 if name.startswith("sand") else 1.0)
+    return 1e-6 + nsub * 2.0 ** -24
 
 
 def nn_error(x: np.ndarray, ref: np.ndarray) -> float:
