@@ -45,28 +45,43 @@ inline std::array<float, 2> ComputeLameParameters(float E, float nu) {
   return {E * nu / ((1 + nu) * (1 - 2 * nu)), E / (2 * (1 + nu))};
 }
 
-// MPMConstitutiveModel (include/mpm_material.cuh:10-18), the subset on this path.
+// MPMConstitutiveModel (include/mpm_material.cuh:10-18).
 enum class MPMConstitutiveModel : int32_t {
   kFixedCorotated = CKMPM_FIXED_COROTATED,
+  kLinear = CKMPM_LINEAR,
   kDruckerPragerStvkhencky = CKMPM_DRUCKER_PRAGER,
   kFluid = CKMPM_FLUID,
+  kVonMises = CKMPM_VON_MISES,
+  kNonAssociatedCamClay = CKMPM_NACC,
 };
 
-// MPMMaterial<k>::MaterialParameter_ collapsed into one run-time value type.
+// MPMMaterial<k>::MaterialParameter_ collapsed into one run-time value type;
+// p holds each model's parameters in its field order (include/mpm_material.cuh:24-257).
 struct MPMMaterial {
   MPMConstitutiveModel kind = MPMConstitutiveModel::kFixedCorotated;
-  float p[4] = {0, 0, 0, 0};
-  static MPMMaterial FixedCorotated(float lambda, float mu) { return {MPMConstitutiveModel::kFixedCorotated, {lambda, mu, 0, 0}}; }
+  float p[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  static MPMMaterial FixedCorotated(float lambda, float mu) {
+    return {MPMConstitutiveModel::kFixedCorotated, {lambda, mu}};
+  }
+  static MPMMaterial Linear(float lambda, float mu) { return {MPMConstitutiveModel::kLinear, {lambda, mu}}; }
   static MPMMaterial DruckerPrager(float lambda, float mu) {
-    return {MPMConstitutiveModel::kDruckerPragerStvkhencky, {lambda, mu, 0, 0}};
+    return {MPMConstitutiveModel::kDruckerPragerStvkhencky, {lambda, mu}};
   }
   static MPMMaterial Fluid(float bulk, float gamma, float viscosity, float J0 = 1.0f) {
     return {MPMConstitutiveModel::kFluid, {bulk, gamma, viscosity, J0}};
   }
+  static MPMMaterial VonMises(float mu, float lambda, float yieldStress) {
+    return {MPMConstitutiveModel::kVonMises, {mu, lambda, yieldStress}};
+  }
+  static MPMMaterial NonAssociatedCamClay(float mu, float lambda, float alpha0, float beta, float hardeningFactor,
+                                          float m, bool hardeningOn) {
+    return {MPMConstitutiveModel::kNonAssociatedCamClay,
+            {mu, lambda, alpha0, beta, hardeningFactor, m, hardeningOn ? 1.f : 0.f}};
+  }
   ckmpm_material c() const {
     ckmpm_material m{};
     m.kind = static_cast<int32_t>(kind);
-    for (int i = 0; i < 4; ++i) m.p[i] = p[i];
+    for (int i = 0; i < 8; ++i) m.p[i] = p[i];
     return m;
   }
 };

@@ -49,3 +49,22 @@ def test_header_compiles_as_c():
     out = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", str(ROOT / "include"), "-x", "c", "-",
                           "-fsyntax-only"], input=src, capture_output=True, text=True)
     assert out.returncode == 0, out.stderr
+
+
+def test_cpp_shim_compiles_with_every_material():
+    """include/ckmpm/mpm_engine.hpp (the reference-shaped C++ API) builds with a
+    plain host compiler and maps each MPMMaterial factory onto ckmpm_material."""
+    src = """#include "ckmpm/mpm_engine.hpp"
+int main() {
+  using ckmpm::MPMMaterial;
+  const MPMMaterial all[] = {MPMMaterial::FixedCorotated(1, 2), MPMMaterial::Linear(1, 2),
+                             MPMMaterial::DruckerPrager(1, 2), MPMMaterial::Fluid(1, 7.15f, 0.1f),
+                             MPMMaterial::VonMises(2, 1, 3), MPMMaterial::NonAssociatedCamClay(2, 1, -0.01f, 0.5f, 0.8f, 2.36f, true)};
+  const int kinds[] = {CKMPM_FIXED_COROTATED, CKMPM_LINEAR, CKMPM_DRUCKER_PRAGER, CKMPM_FLUID, CKMPM_VON_MISES, CKMPM_NACC};
+  for (int i = 0; i < 6; ++i) if (all[i].c().kind != kinds[i]) return 1;
+  return all[5].c().p[6] == 1.f ? 0 : 1;
+}
+"""
+    out = subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I", str(ROOT / "include"), "-x", "c++", "-",
+                          "-fsyntax-only"], input=src, capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
