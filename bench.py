@@ -48,6 +48,7 @@ REFERENCE_FAMILY = {"sand_column": "sand", "jelly_cube": "jelly", "dam_break_mix
 # Per-particle state read once and written once per substep: x + F (FC, von Mises), x + F + logJp (DP,
 # NACC), x + F + stored stress (linear), x + J (fluid).
 STATE_BYTES = {0: 48, 1: 84, 2: 52, 3: 16, 4: 48, 5: 52}
+AUTOTUNE_MAX_PARTICLES = 64_000_000
 
 
 def parse():
@@ -63,6 +64,8 @@ def parse():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sand_column")
     ap.add_argument("--ncu-case", action="store_true",
                     help="profiling driver: set up the workload, run warmup + steps substeps, no timing or baselines")
+    ap.add_argument("--ncu-scenes", type=int, default=256,
+                    help="profiling driver, batched workload: profile the first K of the 256 scenes")
     return ap.parse_args()
 
 
@@ -530,6 +533,13 @@ def run_ours(args, rank, world, local_rank):
     for m in models:
         s.add_model(m)
     s.setup()
+    # Launch shape from the autotuner (it restores the state it advanced).  The
+    # 241M-particle dam break fills every SM at the default shape and its
+    # checkpoint alone would hold tens of GB, so it keeps the default.
+    if n_total <= AUTOTUNE_MAX_PARTICLES:
+        tuning, _ = s.autotune(16, dt)
+    else:
+        tuning = s.tuning()
     s.step(args.warmup, dt)
     n_live = sum(s.count(i) for i in range(len(models)))
     sampler = ClockSampler(device_uuid(local_rank))
@@ -576,6 +586,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- end to end through the public API with host buffers
     s2 = Scene(cfg)
     s2.set_stream(stream.cuda_stream)
+    s2.set_tuning(tuning["threads"], tuning["ctas_per_sm"], tuning["graph_chunk"])
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -618,6 +629,7 @@ def run_ours(args, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jittered lattice, numpy PCG64 seed 0)",
         "config": {"workload": WORKLOADS[args.workload], "particles": n_live, "grid_blocks": grid_blocks, "dt": dt,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "tuning": {k: tuning[k] for k in ("threads", "ctas_per_sm", "graph_chunk")},
                    "l2": "particle state ~190 MB > 126 MB L2: no flush"},
         "roofline": roofline, "e2e": e2e, "clocks": clocks,
         "gpu_launches": 1 + args.steps * (3 * len(models) + 2),
@@ -666,12 +678,51 @@ def run_reference(args, rank, world):
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def ncu_case_other(args):
+    """Profiling driver for the batched and the differentiable forms: the batch
+    (first --ncu-scenes scenes) set up and stepped warmup + steps substeps, or
+    warmup + steps forward + adjoint rollouts of the differentiable cube."""
+    import torch
+    if args.workload == "batched_256":
+        from ckmpm_b200.batch import SceneBatch
+        cfg, models = workload(args.workload)
+        models = models[:max(1, args.ncu_scenes)]
+        b = SceneBatch(cfg, models)
+        b.setup()
+        b.step(args.warmup, cfg.dt)
+        b.step(args.steps, cfg.dt)
+        b.status_check()
+        print(json.dumps({"ncu_case": WORKLOADS[args.workload], "scenes": len(models), "particles": b.count(0),
+                          "substeps": args.warmup + args.steps}))
+        b.close()
+        return
+    from ckmpm_b200 import scenes
+    from ckmpm_b200.diff import DiffRollout, rollout
+    d = scenes.diff_cube()
+    sim = DiffRollout(d["config"], len(d["x0"]), d["mass"], d["volume"], d["nu"], d["nsteps"], d["dt"],
+                      d["checkpoint_every"])
+    x0 = torch.tensor(d["x0"], device="cuda")
+    target = torch.tensor(d["target"], device="cuda")
+    for _ in range(args.warmup + args.steps):
+        v = torch.tensor(d["v0"], device="cuda").requires_grad_()
+        e = torch.tensor(d["logE"], device="cuda").requires_grad_()
+        xT, _ = rollout(sim, x0, v, e)
+        ((xT.mean(0) - target) ** 2).sum().backward()
+    torch.cuda.synchronize()
+    print(json.dumps({"ncu_case": WORKLOADS["diff_cube"], "particles": len(d["x0"]), "substeps": d["nsteps"],
+                      "rollouts": args.warmup + args.steps}))
+    sim.close()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.ncu_case:
+        if args.workload in ("batched_256", "diff_cube"):
+            ncu_case_other(args)
+            return
         from ckmpm_b200 import Scene
         cfg, models = workload(args.workload)
         cfg.device = local_rank

@@ -17,15 +17,22 @@ ROOT = PKG.parent
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libckmpm_b200.so"
 SOURCES = [PKG / "csrc" / "library.cu"]
-# Every source and header the library's single translation unit pulls in.
+# Every source and header the library's single translation unit pulls in, and
+# this file (its flags).
 DEPS = SOURCES + sorted((PKG / "csrc").glob("*.cu")) + sorted((PKG / "csrc").glob("*.cuh")) + \
-    sorted((ROOT / "include").glob("*.h"))
+    sorted((ROOT / "include").glob("*.h")) + [Path(__file__).resolve()]
 
+# Single-precision division and square root use the hardware approximations
+# (at most 2 ulp, full range) instead of the IEEE-rounded sequences: the SVD's
+# Jacobi angles, the D inverses and the return maps divide a dozen times per
+# particle, and the fused substep measured 12 % faster this way on the sand
+# column (bitwise deterministic either way).
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC", "-shared",
     "--expt-relaxed-constexpr",
+    "--prec-div=false", "--prec-sqrt=false",
 ]
 
 
