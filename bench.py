@@ -47,7 +47,7 @@ WORKLOADS = {
 REFERENCE_FAMILY = {"sand_column": "sand", "jelly_cube": "jelly", "dam_break_mixed": "dam", "batched_256": "jelly"}
 # Per-particle state read once and written once per substep: x + F (FC, von Mises), x + F + logJp (DP,
 # NACC), x + F + stored stress (linear), x + J (fluid).
-STATE_BYTES = {0: 48, 1: 84, 2: 52, 3: 16, 4: 48, 5: 52}
+STATE_BYTES = {0: 48, 1: 84, 2: 52, 3: 16, 4: 52, 5: 52}
 AUTOTUNE_MAX_PARTICLES = 64_000_000
 
 

@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(kThreads) particle_kernel(Dev d, const float* 
 
 // Adjoint of one substep for every particle.  xb / Fb hold the adjoints of the
 // substep's outputs on entry and of its inputs on exit.
-__global__ void __launch_bounds__(kThreads) particle_adjoint_kernel(
+__global__ void __launch_bounds__(kThreads, 3) particle_adjoint_kernel(
     Dev d, const float* __restrict__ x, const float* __restrict__ F, const float* __restrict__ lam,
     const float* __restrict__ mu, const float4* __restrict__ vel, float dt, float ndt, const float4* __restrict__ gadj,
     float* __restrict__ xb, float* __restrict__ Fb, float* __restrict__ mub, float* __restrict__ lamb,

@@ -35,9 +35,11 @@
 #if defined(__CUDACC__)
 #define CKD __host__ __device__ __forceinline__
 #define CKD_UNROLL _Pragma("unroll")
+#define CKD_ROLLED _Pragma("unroll 1")
 #else
 #define CKD inline
 #define CKD_UNROLL
+#define CKD_ROLLED
 #endif
 
 #include <cmath>
@@ -453,10 +455,13 @@ CKD void particle_adjoint(const Particle<T>& p, const Fwd<T>& f, const T* U, con
     Fnb[k] = Fnbar_in[k];
     Ab[k] = T(0);
   }
-  // P2G at x' (gather of the grid adjoint).
+  // P2G at x' (gather of the grid adjoint).  The two node loops of the adjoint
+  // stay rolled: unrolled, the kernel's code outgrew the instruction cache
+  // (ncu: a third of the stall samples waiting for instructions), and rolled
+  // with 3 CTAs per SM the adjoint substep measured 8 % faster.
   CKD_UNROLL
   for (int g = 0; g < 2; ++g)
-    CKD_UNROLL
+    CKD_ROLLED
     for (int n = 0; n < 8; ++n) {
       T gw[3];
       const T w = node_weight(f.stn, g, n, inv_dx, gw);
@@ -537,7 +542,7 @@ CKD void particle_adjoint(const Particle<T>& p, const Fwd<T>& f, const T* U, con
   // G2P at x: v = 1/2 sum w v_i, B = sum w v_i r^T
   CKD_UNROLL
   for (int g = 0; g < 2; ++g)
-    CKD_UNROLL
+    CKD_ROLLED
     for (int n = 0; n < 8; ++n) {
       T gw[3];
       const T w = node_weight(f.st, g, n, inv_dx, gw);

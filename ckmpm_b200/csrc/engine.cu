@@ -3,6 +3,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -75,6 +76,8 @@ struct ckmpm_scene {
   cudaGraphExec_t graph_chunk = nullptr;
   cudaGraphExec_t graph_one = nullptr;
   uint64_t host_step = 0;
+  uint32_t rigid_count = 0;       // leading rigid particles of every von Mises model
+  float rigid_v[3] = {0.f, 0.f, 0.f};
 };
 
 namespace {
@@ -241,6 +244,7 @@ bool valid_material(const ckmpm_material& m, std::string* why) {
 
 // Initial aux value: J0 for the fluid, alpha0 (the initial logJp) for NACC, else 0.
 float initial_aux(const ckmpm_material& m) {
+  if (m.kind == CKMPM_VON_MISES) return 1.f;  // the rigid flag: deformable
   return m.kind == CKMPM_FLUID ? m.p[3] : (m.kind == CKMPM_NACC ? m.p[2] : 0.f);
 }
 
@@ -588,8 +592,9 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     lost_at_setup += n - m.n_valid;
     const float aux0 = initial_aux(m.mat);
     if (m.n_valid > 0)
-      setup_gather_kernel<<<(m.n_valid + 255) / 256, 256, 0, s->stream>>>(d, s->nstack, m.n_valid, v_out, dx_in,
-                                                                           dv_in, m.nv, aux0);
+      setup_gather_kernel<<<(m.n_valid + 255) / 256, 256, 0, s->stream>>>(
+          d, s->nstack, m.n_valid, v_out, dx_in, dv_in, m.nv, aux0,
+          (s->sc.rigid && m.mat.kind == CKMPM_VON_MISES) ? s->rigid_count : 0u);
     // Identity previous-step structures in list 1.
     CK_CUDA(s, cudaMemcpyAsync(d.bl[1].table, d.bl[0].table, sizeof(int32_t) * nbd, cudaMemcpyDeviceToDevice,
                                s->stream));
@@ -629,6 +634,7 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
   h.cur_dt = 0.f;
   h.next_dt = 0.f;
   h.lost = lost_at_setup;
+  for (int a = 0; a < 3; ++a) h.rigid_v[a] = s->rigid_v[a];
   CK_CUDA(s, cudaMemcpyAsync(s->scal, &h, sizeof(Scalars), cudaMemcpyHostToDevice, s->stream));
   CK_CUDA(s, cudaStreamSynchronize(s->stream));
   s->setup_done = true;
@@ -637,6 +643,32 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
   Scalars r{};
   CK_CUDA(s, cudaMemcpy(&r, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost));
   return status_from(s, r);
+}
+
+ckmpm_status ckmpm_set_rigid(ckmpm_scene* s, uint32_t rigid_count, const float* velocity) {
+  if (!s || !velocity) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  if (s->setup_done) return fail(s, CKMPM_ERR_INVALID, "rigid particles are set before ckmpm_setup");
+  if (s->nstack > 1) return fail(s, CKMPM_ERR_INVALID, "a batch has no rigid particles");
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(velocity[a])) return fail(s, CKMPM_ERR_INVALID, "rigid velocity must be finite");
+  s->sc.rigid = 1;
+  s->rigid_count = rigid_count;
+  for (int a = 0; a < 3; ++a) s->rigid_v[a] = velocity[a];
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_set_rigid_velocity(ckmpm_scene* s, const float* velocity) {
+  if (!s || !velocity) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  if (!s->sc.rigid) return fail(s, CKMPM_ERR_INVALID, "rigid particles are off (ckmpm_set_rigid)");
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(velocity[a])) return fail(s, CKMPM_ERR_INVALID, "rigid velocity must be finite");
+  for (int a = 0; a < 3; ++a) s->rigid_v[a] = velocity[a];
+  if (!s->setup_done) return CKMPM_OK;
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  // Stream-ordered: substeps already enqueued keep the old velocity.  The
+  // pageable source is staged before the call returns.
+  CK_CUDA(s, cudaMemcpyAsync(s->scal->rigid_v, s->rigid_v, sizeof(s->rigid_v), cudaMemcpyHostToDevice, s->stream));
+  return CKMPM_OK;
 }
 
 ckmpm_status ckmpm_set_stream(ckmpm_scene* s, void* cuda_stream) {

@@ -62,6 +62,7 @@ struct SceneDev {
   uint32_t nstack;       // stacked domains (1 for a single scene, the scene count for a batch)
   uint32_t nblocks_domain;  // table entries over all stacked domains
   float grid_unit;       // single scene: mass of one fixed-point unit (heaviest model's mass x 2^-36)
+  int32_t rigid;         // rigid particles on (the velocity is Scalars::rigid_v)
 };
 
 // Per-scene material of a batch (one model per stacked domain).
@@ -88,6 +89,7 @@ struct Scalars {
   double frame_end;    // adaptive dt: end of the current frame
   double cur_dt_d;     // cur_dt / next_dt in double, as the reference keeps its clock
   double next_dt_d;
+  float rigid_v[3];    // velocity of rigid particles (when SceneDev::rigid)
 };
 
 struct BlockListDev {
@@ -111,8 +113,18 @@ struct StateDev {
 
 // Which per-particle arrays a material keeps.
 __host__ __device__ __forceinline__ bool material_has_F(int kind) { return kind != kFluid; }
+// aux: logJp (Drucker-Prager, NACC), J (fluid) or the rigid flag (von Mises:
+// 1 deformable, 0 rigid; include/mpm_algorithm.cuh:1063-1069).
 __host__ __device__ __forceinline__ bool material_has_aux(int kind) {
-  return kind == kDruckerPrager || kind == kFluid || kind == kNacc;
+  return kind == kDruckerPrager || kind == kFluid || kind == kNacc || kind == kVonMises;
+}
+
+// With rigid particles on, the reference's G2P2G treats a particle as rigid
+// when its bucket attribute 3 is exactly zero (include/mpm_algorithm.cuh:1540-1543,
+// 1611): that attribute is F00 for fixed-corotated, Drucker-Prager and linear,
+// J for the fluid, logJp for NACC and the rigid flag for von Mises.
+__host__ __device__ __forceinline__ float rigid_attribute(int kind, const float* F, float aux) {
+  return (kind == kFluid || kind == kVonMises || kind == kNacc) ? aux : F[0];
 }
 
 struct ModelDev {
@@ -672,8 +684,22 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
       bool inside = true;
       float v[3], C[9], Dold[6];
       g2p(vtile, xs, key, dx, v, C, inside, Dold);
+      float adv[3] = {v[0], v[1], v[2]};
+      if (sc.rigid && rigid_attribute(kind, F, aux) == 0.f) {
+        // Rigid: moves with the scene's rigid velocity and carries no velocity,
+        // no affine field and no G2P D (include/mpm_algorithm.cuh:1609-1618).
 #pragma unroll
-      for (int a = 0; a < 3; ++a) x[a] += dt * v[a];
+        for (int k = 0; k < 9; ++k) C[k] = 0.f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) Dold[k] = 0.f;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          v[a] = 0.f;
+          adv[a] = scal->rigid_v[a];
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) x[a] += dt * adv[a];
 
       float tau[9];
       if (kind == kFluid) {
@@ -1155,11 +1181,13 @@ __global__ void setup_bin_kernel(SceneDev sc, uint32_t n, const float* __restric
   vals[i] = i;
 }
 
-// Sorted initial state: x from the input, F = I, aux = logJp0 (0) or J0,
-// id = input index, velocities gathered for the rasterisation
+// Sorted initial state: x from the input, F = I, aux = logJp0 (0), alpha0,
+// J0 or the rigid flag (0 for the first rigid_count input particles, else
+// aux0 = 1), id = input index, velocities gathered for the rasterisation
 // (include/mpm_algorithm.cuh:974-1081).
 __global__ void setup_gather_kernel(ModelDev md, uint32_t nstack, uint32_t n, const uint32_t* __restrict__ perm,
-                                    const float* __restrict__ x, const float* __restrict__ v, uint32_t nv, float aux0) {
+                                    const float* __restrict__ x, const float* __restrict__ v, uint32_t nv, float aux0,
+                                    uint32_t rigid_count) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t s = perm[i];
@@ -1171,7 +1199,7 @@ __global__ void setup_gather_kernel(ModelDev md, uint32_t nstack, uint32_t n, co
 #pragma unroll
     for (int k = 0; k < 9; ++k) st.F[k][i] = (k & 3) ? 0.f : 1.f;
   }
-  if (st.aux) st.aux[i] = md.smat ? md.smat[scene_of(md.sstart, nstack, s)].aux0 : aux0;
+  if (st.aux) st.aux[i] = md.smat ? md.smat[scene_of(md.sstart, nstack, s)].aux0 : (s < rigid_count ? 0.f : aux0);
   if (st.Q[0]) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) st.Q[k][i] = 0.f;
@@ -1256,6 +1284,11 @@ __global__ void __launch_bounds__(NT) probe_kernel(SceneDev sc, ModelDev md, Gri
         float v[3], C[9], D6[6];
         bool inside = true;
         g2p(vtile, xs, key, sc.dx, v, C, inside, D6);
+        if (sc.rigid) {  // rigid particles report zero velocity (include/mpm_algorithm.cuh:1316-1325)
+          const float f0 = (material_has_F(kind) && sin.F[0]) ? sin.F[0][iin] : 1.f;
+          const float a = (material_has_aux(kind) && sin.aux) ? sin.aux[iin] : 1.f;
+          if (rigid_attribute(kind, &f0, a) == 0.f) v[0] = v[1] = v[2] = 0.f;
+        }
         ov[3 * o] = v[0];
         ov[3 * o + 1] = v[1];
         ov[3 * o + 2] = v[2];

@@ -283,7 +283,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   const uint32_t n_valid = counts[1];
   const float aux0 = material->kind == CKMPM_FLUID ? material->p[3] : 0.f;
   if (n_valid > 0)
-    setup_gather_kernel<<<(n_valid + 255) / 256, 256, 0, st>>>(d, 1, n_valid, sort_vals_out, x, v, nv, aux0);
+    setup_gather_kernel<<<(n_valid + 255) / 256, 256, 0, st>>>(d, 1, n_valid, sort_vals_out, x, v, nv, aux0, 0u);
   NA_CUDA(cudaMemcpyAsync(d.bl[1].table, d.bl[0].table, sizeof(int32_t) * nbd, cudaMemcpyDeviceToDevice, st));
   NA_CUDA(cudaMemcpyAsync(d.bl[1].start, d.bl[0].start, sizeof(uint32_t) * d.cap_slots, cudaMemcpyDeviceToDevice, st));
   NA_CUDA(cudaMemcpyAsync(d.bl[1].count, d.bl[0].count, sizeof(uint32_t) * d.cap_slots, cudaMemcpyDeviceToDevice, st));

@@ -176,6 +176,13 @@ class MPMConfig:
     device: int = 0
     block_size: int = 4
     particles_per_cell_cap: int = 64
+    # Rigid particles (GetExistRigidParticle / GetRigidParticleCount /
+    # GetRigidParticleVelocity(frame), include/mpm_config.h:92-106): the first
+    # rigid_particle_count particles of every von Mises model are rigid;
+    # rigid_particle_velocity is (vx, vy, vz) or a callable frame -> (vx, vy, vz).
+    exist_rigid_particle: bool = False
+    rigid_particle_count: int = 0
+    rigid_particle_velocity: object = (0.0, 0.0, 0.0)
 
     # MPMConfigBase getter names (include/mpm_config.h:17-123)
     def GetDx(self) -> float:
@@ -214,6 +221,17 @@ class MPMConfig:
     def GetMassClamp(self) -> float:
         return self.mass_clamp
 
+    def GetExistRigidParticle(self) -> bool:
+        return self.exist_rigid_particle
+
+    def GetRigidParticleCount(self) -> int:
+        return self.rigid_particle_count
+
+    def GetRigidParticleVelocity(self, frame: int = 0) -> tuple[float, float, float]:
+        v = self.rigid_particle_velocity
+        v = v(frame) if callable(v) else v
+        return tuple(float(c) for c in v)
+
     def to_c(self) -> capi.SceneDesc:
         d = capi.SceneDesc()
         d.dx = self.dx
@@ -248,6 +266,19 @@ class Scene:
         desc = config.to_c()
         capi.check(L.ckmpm_create(C.byref(desc), C.byref(self._h)), "ckmpm_create", None)
         self.models: list[MPMModel] = []
+        if config.exist_rigid_particle:
+            self.set_rigid(config.rigid_particle_count, config.GetRigidParticleVelocity(0))
+
+    def set_rigid(self, count: int, velocity) -> None:
+        """Rigid particles on (before setup): the first `count` particles of
+        every von Mises model start rigid and move with `velocity`."""
+        v = np.ascontiguousarray(velocity, np.float32).reshape(3)
+        capi.check(capi.lib().ckmpm_set_rigid(self._h, int(count), capi.fptr(v)), "ckmpm_set_rigid", self._h)
+
+    def set_rigid_velocity(self, velocity) -> None:
+        """Velocity of the rigid particles for the substeps enqueued from now on."""
+        v = np.ascontiguousarray(velocity, np.float32).reshape(3)
+        capi.check(capi.lib().ckmpm_set_rigid_velocity(self._h, capi.fptr(v)), "ckmpm_set_rigid_velocity", self._h)
 
     def add_model(self, model: MPMModel) -> int:
         L = capi.lib()
@@ -438,6 +469,8 @@ class MPMEngine:
         assert self.scene is not None
         start = self.scene.counters()["steps"]
         for frame in range(config.GetTotalSimulatedFrameCount()):
+            if config.GetExistRigidParticle():  # the hook is evaluated per frame (mpm_algorithm.cuh:1614)
+                self.scene.set_rigid_velocity(config.GetRigidParticleVelocity(frame))
             if fixed_substeps_per_frame:
                 self.scene.step(fixed_substeps_per_frame, self.dt_)
             else:

@@ -125,6 +125,21 @@ ckmpm_status ckmpm_status_check(ckmpm_scene* s);
 ckmpm_status ckmpm_step_adaptive(ckmpm_scene* s, uint32_t nsteps, float dt_max, float cfl, double frame_time,
                                  double* elapsed);
 
+/* Rigid particles, the reference's scene hooks GetExistRigidParticle,
+ * GetRigidParticleCount and GetRigidParticleVelocity(frame)
+ * (include/mpm_config.h:92-106) as used by its particle initialisation
+ * (include/mpm_algorithm.cuh:1063-1069) and G2P2G (:1540-1543, :1609-1624).
+ * ckmpm_set_rigid, before ckmpm_setup, turns them on: the first rigid_count
+ * input particles of every von Mises model start rigid (aux = 0).  As in the
+ * reference, every particle whose bucket attribute 3 is exactly zero is then
+ * rigid (F00 for fixed-corotated, Drucker-Prager and linear, J for the fluid,
+ * logJp for NACC, the flag for von Mises): it moves by dt * velocity, deposits
+ * its mass with zero momentum and zero affine field, and reports v = 0.  Not
+ * for a batch.  ckmpm_set_rigid_velocity changes the velocity for the
+ * substeps enqueued after it (the reference evaluates its hook per frame). */
+ckmpm_status ckmpm_set_rigid(ckmpm_scene* s, uint32_t rigid_count, const float* velocity3);
+ckmpm_status ckmpm_set_rigid_velocity(ckmpm_scene* s, const float* velocity3);
+
 /* Use a caller-provided cudaStream_t (passed as void*) for all work of this
  * scene; NULL selects the scene's own stream. */
 ckmpm_status ckmpm_set_stream(ckmpm_scene* s, void* cuda_stream);
@@ -136,7 +151,8 @@ ckmpm_status ckmpm_get_count(ckmpm_scene* s, int32_t model, uint32_t* n_live);
  * D2H (include/mpm_algorithm.cuh:1977-2020, include/mpm_engine.cuh:386-454).
  * Arrays hold n_live entries (x, v: 3 floats; F: 9 floats row-major, the
  * identity for the fluid; aux: J for the fluid, logJp for Drucker-Prager and
- * NACC, 0 otherwise; id: input index).  With
+ * NACC, the rigid flag for von Mises (1 deformable, 0 rigid), 0 otherwise;
+ * id: input index).  With
  * CKMPM_FLAG_TRACK_IDS the arrays are in input order and id is the identity
  * over live particles; without it they are in block order.  v is the velocity
  * the next G2P interpolates at each particle (the reference's conservation

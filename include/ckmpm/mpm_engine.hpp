@@ -126,6 +126,11 @@ struct MPMConfig {
   uint32_t maxParticleCountPerBlock = 4096;
   bool trackIds = true;
   int32_t device = 0;
+  // Rigid particles (GetExistRigidParticle / GetRigidParticleCount /
+  // GetRigidParticleVelocity(frame), include/mpm_config.h:92-106).
+  bool existRigidParticle = false;
+  uint32_t rigidParticleCount = 0;
+  std::function<Vector3(int)> rigidParticleVelocity = [](int) { return Vector3{0.f, 0.f, 0.f}; };
 
   float GetDx() const { return dx; }
   float GetInvDx() const { return 1.f / dx; }
@@ -138,6 +143,9 @@ struct MPMConfig {
   uint32_t GetTotalSimulatedFrameCount() const { return totalFrames; }
   float GetGravity() const { return gravity; }
   float GetMassClamp() const { return massClamp; }
+  bool GetExistRigidParticle() const { return existRigidParticle; }
+  uint32_t GetRigidParticleCount() const { return rigidParticleCount; }
+  Vector3 GetRigidParticleVelocity(int frame) const { return rigidParticleVelocity(frame); }
 
   ckmpm_scene_desc c() const {
     ckmpm_scene_desc d{};
@@ -169,6 +177,10 @@ class MPMEngine {
     const ckmpm_scene_desc d = config.c();
     check(ckmpm_create(&d, &scene_), nullptr, "ckmpm_create");
     dt_ = std::min(config.GetDt(), 1.0f / static_cast<float>(config.GetFps()));
+    if (config.GetExistRigidParticle()) {
+      const Vector3 v = config.GetRigidParticleVelocity(0);
+      check(ckmpm_set_rigid(scene_, config.GetRigidParticleCount(), v.data()), scene_, "ckmpm_set_rigid");
+    }
   }
 
   // InitializeParticle: one engine model per MPMModel; dt shrinks by the CFL
@@ -198,6 +210,10 @@ class MPMEngine {
   double Simulate(const MPMConfig& config, const std::function<void(uint32_t, MPMEngine&)>& exportFrame = {}) {
     double total = 0.0;
     for (uint32_t f = 0; f < config.GetTotalSimulatedFrameCount(); ++f) {
+      if (config.GetExistRigidParticle()) {  // the hook is evaluated per frame (include/mpm_algorithm.cuh:1614)
+        const Vector3 v = config.GetRigidParticleVelocity(static_cast<int>(f));
+        check(ckmpm_set_rigid_velocity(scene_, v.data()), scene_, "ckmpm_set_rigid_velocity");
+      }
       double elapsed = 0.0;
       check(ckmpm_step_adaptive(scene_, 1u << 30, dt_, config.GetCfl(), 1.0 / config.GetFps(), &elapsed), scene_,
             "ckmpm_step_adaptive");

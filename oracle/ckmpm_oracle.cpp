@@ -61,7 +61,7 @@ struct Model {
   double p[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   double mass = 0, vol = 0;
   int n = 0;
-  std::vector<double> x, F, aux;  // aux: J (fluid) or logJp (DP, NACC)
+  std::vector<double> x, F, aux;  // aux: J (fluid), logJp (DP, NACC) or the rigid flag (von Mises)
   std::vector<double> Q;          // the linear model's stored stress (9 per particle)
   std::vector<double> v0;         // initial velocities (n or 1 entries of 3)
   std::vector<double> plam, pmu;  // optional per-particle Lame parameters (fixed-corotated)
@@ -77,7 +77,26 @@ struct Scene {
   int64_t steps = 0;
   int64_t lost = 0, window_skips = 0;
   std::vector<double> dt_log;
+  // Rigid particles (mpm_config.h:92-106 GetExistRigidParticle / GetRigidParticleCount /
+  // GetRigidParticleVelocity): the first rigid_count particles of every von Mises
+  // model start rigid (mpm_algorithm.cuh:1063-1069).
+  bool rigid = false;
+  int rigid_count = 0;
+  double rigid_v[3] = {0, 0, 0};
 };
+
+// The attribute the reference's G2P2G tests for rigidity when rigid particles
+// are on: bucket attribute 3 (mpm_algorithm.cuh:1540-1543), which is F00 for
+// fixed-corotated, Drucker-Prager and linear, J for the fluid, logJp for NACC
+// and the rigid flag for von Mises.
+inline double attribute3(const Model& m, int p) {
+  return (m.kind == 3 || m.kind == 4 || m.kind == 5) ? m.aux[p] : m.F[9 * p];
+}
+
+inline void init_rigid_flags(const Scene& s, Model& m) {
+  if (m.kind != 4) return;
+  for (int p = 0; p < m.n; ++p) m.aux[p] = (s.rigid && p < s.rigid_count) ? 0.0 : 1.0;
+}
 
 inline int64_t flat_key(const Scene& s, int bx, int by, int bz) {
   return (static_cast<int64_t>(bx) * s.d.dims[1] + by) * s.d.dims[2] + bz;
@@ -571,10 +590,16 @@ void substep(Scene& s, double next_dt) {
       particle_block(x, invdx, K);
       double v[3], C[9];
       g2p(s, x, dt, v, C);
+      // A rigid particle moves with the scene's rigid velocity and carries no
+      // velocity, no affine field and no G2P D (mpm_algorithm.cuh:1609-1618).
+      const bool rigid = s.rigid && attribute3(m, p) == 0.0;
+      if (rigid)
+        for (int k = 0; k < 9; ++k) C[k] = 0.0;
       double xn[3], xold[3];
       for (int a = 0; a < 3; ++a) {
         xold[a] = x[a];
-        xn[a] = x[a] + dt * v[a];
+        if (rigid) v[a] = 0.0;
+        xn[a] = x[a] + dt * (rigid ? s.rigid_v[a] : v[a]);
       }
       double tau[9];
       if (m.kind == 3) {
@@ -622,7 +647,7 @@ void substep(Scene& s, double next_dt) {
       double D[9], Dold[9], Di[9], halfD[9];
       d_matrix(xn, invdx, dx, D);
       d_matrix(xold, invdx, dx, Dold);
-      for (int k = 0; k < 9; ++k) halfD[k] = 0.5 * (D[k] + Dold[k]);
+      for (int k = 0; k < 9; ++k) halfD[k] = 0.5 * (D[k] + (rigid ? 0.0 : Dold[k]));
       inv3(halfD, Di);
       double DT[9];
       matmul3(Di, tau, DT);
@@ -669,6 +694,7 @@ int oracle_add_model(void* h, int kind, const double* params, int n, const float
   m.F.assign(9 * static_cast<size_t>(n), 0.0);
   for (int p = 0; p < n; ++p) m.F[9 * p] = m.F[9 * p + 4] = m.F[9 * p + 8] = 1.0;
   m.aux.assign(n, kind == 3 ? params[3] : (kind == 5 ? params[2] : 0.0));
+  init_rigid_flags(*s, m);
   if (kind == 1) m.Q.assign(9 * static_cast<size_t>(n), 0.0);
   m.v0.assign(v, v + 3 * static_cast<size_t>(nv));
   m.alive.assign(n, 1);
@@ -709,6 +735,27 @@ int oracle_set_velocity(void* h, int model, const double* v, int nv) {
   Model& m = s->models[model];
   if (nv != 1 && nv != m.n) return -1;
   m.v0.assign(v, v + 3 * static_cast<size_t>(nv));
+  return 0;
+}
+
+// Rigid particles on (enable != 0) with rigid_count leading rigid particles per
+// von Mises model and the rigid velocity v; call before oracle_setup.
+int oracle_set_rigid(void* h, int enable, int rigid_count, const double* v) {
+  Scene* s = static_cast<Scene*>(h);
+  if (rigid_count < 0 || !v) return -1;
+  s->rigid = enable != 0;
+  s->rigid_count = rigid_count;
+  for (int a = 0; a < 3; ++a) s->rigid_v[a] = v[a];
+  for (Model& m : s->models) init_rigid_flags(*s, m);
+  return 0;
+}
+
+// The rigid velocity of the following substeps (the reference evaluates its
+// hook once per frame, mpm_algorithm.cuh:1614).
+int oracle_set_rigid_velocity(void* h, const double* v) {
+  Scene* s = static_cast<Scene*>(h);
+  if (!v) return -1;
+  for (int a = 0; a < 3; ++a) s->rigid_v[a] = v[a];
   return 0;
 }
 
@@ -792,6 +839,7 @@ int oracle_get_state(void* h, int model, double* x, double* v, double* F, double
     if (v) {
       double C[9];
       g2p(*s, &m.x[3 * p], s->current_dt, &v[3 * p], C);
+      if (s->rigid && attribute3(m, p) == 0.0) v[3 * p] = v[3 * p + 1] = v[3 * p + 2] = 0.0;  // :1316-1325
     }
   }
   return m.n;

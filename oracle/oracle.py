@@ -37,6 +37,8 @@ def lib() -> C.CDLL:
         L.oracle_setup.argtypes = [C.c_void_p]
         L.oracle_set_lame.argtypes = [C.c_void_p, C.c_int, d, d]
         L.oracle_set_velocity.argtypes = [C.c_void_p, C.c_int, d, C.c_int]
+        L.oracle_set_rigid.argtypes = [C.c_void_p, C.c_int, C.c_int, d]
+        L.oracle_set_rigid_velocity.argtypes = [C.c_void_p, d]
         L.oracle_step.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.oracle_step_frame.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]
         L.oracle_get_state.argtypes = [C.c_void_p, C.c_int, d, d, d, d, C.POINTER(C.c_uint8)]
@@ -101,6 +103,16 @@ class OracleScene:
         """Initial velocities in double precision (1 or n rows); call before setup()."""
         v = np.ascontiguousarray(v, np.float64).reshape(-1, 3)
         assert lib().oracle_set_velocity(self._h, model, _d(v), len(v)) == 0
+
+    def set_rigid(self, count: int, velocity) -> None:
+        """Rigid particles on: the first `count` particles of every von Mises
+        model are rigid and move with `velocity`; call before setup()."""
+        v = np.ascontiguousarray(velocity, np.float64).reshape(3)
+        assert lib().oracle_set_rigid(self._h, 1, int(count), _d(v)) == 0
+
+    def set_rigid_velocity(self, velocity) -> None:
+        v = np.ascontiguousarray(velocity, np.float64).reshape(3)
+        assert lib().oracle_set_rigid_velocity(self._h, _d(v)) == 0
 
     def setup(self):
         lib().oracle_setup(self._h)

@@ -13,6 +13,10 @@
 //   CKMPM_HARNESS_SCENE_SAND  : dx = 1/256, 64^3 blocks, g = -9.8, slip floor at 8 cells
 //   CKMPM_HARNESS_SCENE_SLIP  : dx = 1/64,  16^3 blocks, g = -9.8, slip floor at 8 cells
 //   CKMPM_HARNESS_SCENE_DAM   : dx = 1/512, 128^3 blocks, g = -9.8, sticky walls
+//   CKMPM_HARNESS_SCENE_RIGID : the JELLY grid with rigid particles on (GetExistRigidParticle):
+//                               the first 2048 particles of every von Mises model are rigid and
+//                               move with (2, 0.5 frame - 1, -1) in frame `frame` (every value
+//                               exact in float)
 // The slip floor is installed through the reference's irregular-boundary hook
 // (GetExistIrregularBoundary / ProcessGridCellVelocity, include/mpm_algorithm.cuh:795-799):
 // sticky x/z walls and ceiling two blocks deep, v_y >= 0 in cells below the floor.
@@ -59,6 +63,12 @@ constexpr int kBlocks = 16;
 constexpr bool kSlipFloor = false;
 constexpr uint32_t kMaxBlocks = 4096;
 #endif
+#if defined(CKMPM_HARNESS_SCENE_RIGID)
+constexpr bool kRigid = true;
+#else
+constexpr bool kRigid = false;
+#endif
+constexpr uint32_t kRigidCount = 2048;
 constexpr float kGravity = -9.8f;
 constexpr float kFloorCells = 8.f;
 
@@ -92,11 +102,14 @@ class Config : public mpm::MPMConfigBase<Config> {
   MPM_FORCE_INLINE auto GetTotalSimulatedFrameCountImpl() const -> uint32_t { return g_frames; }
   constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetGravityImpl() const -> float { return kGravity; }
   constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetMassClampImpl() const -> float { return 0.f; }
-  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetExistRigidParticleImpl() const -> bool { return false; }
-  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetRigidParticleCountImpl() const -> uint32_t { return 0; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetExistRigidParticleImpl() const -> bool { return kRigid; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetRigidParticleCountImpl() const -> uint32_t {
+    return kRigid ? kRigidCount : 0u;
+  }
   template <typename Scalar>
-  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetRigidParticleVelocityImpl(int) const -> mpm::Vector<Scalar, 3> {
-    return mpm::Vector<Scalar, 3>{0.f, 0.f, 0.f};
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetRigidParticleVelocityImpl(int frame) const
+      -> mpm::Vector<Scalar, 3> {
+    return mpm::Vector<Scalar, 3>{Scalar(2), Scalar(0.5) * Scalar(frame) - Scalar(1), Scalar(-1)};
   }
   constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetExistIrregularBoundaryImpl() const -> bool { return kSlipFloor; }
   MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto ProcessGridCellVelocityImpl(const mpm::Vector<int, 3>& cell,

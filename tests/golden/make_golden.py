@@ -11,7 +11,9 @@ them), the largest nearest-neighbour distance between the two runs (the
 reference's own run-to-run spread, from its float atomics), and the inputs'
 checksum.  dt is a power of two and fps = 1 / (16 dt), so each frame is exactly
 16 substeps and the reference's frame clipping never changes dt; the first
-substep advects with dt = 0 as in the reference.
+substep advects with dt = 0 as in the reference.  The rigid-particle fixture
+runs on the harness's RIGID family, whose scene hooks make the first 2048
+particles rigid with a per-frame velocity (rigid_velocity below).
 """
 from __future__ import annotations
 
@@ -59,6 +61,26 @@ def adaptive_scene():
     return cfg, m[0]
 
 
+# Rigid-particle fixture: the von Mises cube on the harness's RIGID family
+# (oracle/ref_harness.cu), where the reference's rigid-particle hooks are on:
+# its first RIGID_COUNT particles move with rigid_velocity(frame).
+RIGID = {"name": "vm_rigid", "family": "rigid"}
+RIGID_COUNT = 2048
+
+
+def rigid_velocity(frame: int) -> tuple[float, float, float]:
+    return (2.0, 0.5 * frame - 1.0, -1.0)
+
+
+def rigid_scene():
+    cfg, m = scenes.material_cube("von_mises")
+    cfg.exist_rigid_particle = True
+    cfg.rigid_particle_count = RIGID_COUNT
+    cfg.rigid_particle_velocity = rigid_velocity
+    cfg.dt, cfg.fps, cfg.total_frames = DT, FPS, FRAMES
+    return cfg, m[0]
+
+
 def checksum(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()[:16]
 
@@ -91,6 +113,22 @@ def main(outdir: str, only: list[str] | None = None) -> None:
                       "mass": model.particle_mass, "volume": model.particle_volume,
                       "counts": [int(len(runs[0][k])) for k in range(FRAMES)]}
         print(name, meta[name]["n"], "spread", max(spread), flush=True)
+    if not only or RIGID["name"] in only:
+        cfg, model = rigid_scene()
+        runs = []
+        for _ in range(2):
+            _, d = ref_runner.run(RIGID["family"], model, FPS, FRAMES, DT, 0)
+            runs.append(ref_runner.frames_out(d, FRAMES))
+        spread = [float(ref_runner.match_nn(runs[0][k], runs[1][k])[1].max()) for k in range(FRAMES)]
+        np.savez_compressed(out / f"{RIGID['name']}.npz", **{f"frame{k}": runs[0][k] for k in KEEP})
+        meta[RIGID["name"]] = {"family": RIGID["family"], "n": int(len(model.particle_position)),
+                               "input_sha": checksum(model.particle_position), "dt": DT, "fps": FPS,
+                               "frames": FRAMES, "substeps_per_frame": SUBSTEPS_PER_FRAME,
+                               "kept_frames": list(KEEP), "rigid_count": RIGID_COUNT,
+                               "rigid_velocity": [list(rigid_velocity(k)) for k in range(FRAMES)],
+                               "reference_run_to_run_spread": spread,
+                               "counts": [int(len(r)) for r in runs[0]]}
+        print(RIGID["name"], meta[RIGID["name"]]["n"], "spread", max(spread), flush=True)
     if only and ADAPTIVE["name"] not in only:
         meta_path.write_text(json.dumps(meta, indent=1))
         return

@@ -53,7 +53,8 @@ def test_header_compiles_as_c():
 
 def test_cpp_shim_compiles_with_every_material():
     """include/ckmpm/mpm_engine.hpp (the reference-shaped C++ API) builds with a
-    plain host compiler and maps each MPMMaterial factory onto ckmpm_material."""
+    plain host compiler, maps each MPMMaterial factory onto ckmpm_material and
+    carries the rigid-particle hooks."""
     src = """#include "ckmpm/mpm_engine.hpp"
 int main() {
   using ckmpm::MPMMaterial;
@@ -62,6 +63,11 @@ int main() {
                              MPMMaterial::VonMises(2, 1, 3), MPMMaterial::NonAssociatedCamClay(2, 1, -0.01f, 0.5f, 0.8f, 2.36f, true)};
   const int kinds[] = {CKMPM_FIXED_COROTATED, CKMPM_LINEAR, CKMPM_DRUCKER_PRAGER, CKMPM_FLUID, CKMPM_VON_MISES, CKMPM_NACC};
   for (int i = 0; i < 6; ++i) if (all[i].c().kind != kinds[i]) return 1;
+  ckmpm::MPMConfig cfg;  // the rigid-particle hooks as run-time fields
+  cfg.existRigidParticle = true;
+  cfg.rigidParticleCount = 16;
+  cfg.rigidParticleVelocity = [](int frame) { return ckmpm::Vector3{1.f, 0.f, static_cast<float>(frame)}; };
+  if (!cfg.GetExistRigidParticle() || cfg.GetRigidParticleVelocity(2)[2] != 2.f) return 1;
   return all[5].c().p[6] == 1.f ? 0 : 1;
 }
 """

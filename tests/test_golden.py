@@ -107,3 +107,30 @@ def test_oracle_matches_reference_build(oracle_mod):
             err = nn_error(x, ref)
             print(f"{name} frame {k} ({target} substeps): oracle vs reference {err:.3e}")
             assert err <= tolerance(name, target), (name, k, err)
+
+
+def test_oracle_matches_reference_rigid(oracle_mod):
+    """Rigid particles: the reference with its rigid-particle hooks on (harness
+    family RIGID: the von Mises cube's first 2048 particles move with a velocity
+    that changes every frame) against the oracle driven frame by frame."""
+    _, mg = golden_cases()
+    meta = load_meta()["vm_rigid"]
+    cfg, model = mg.rigid_scene()
+    assert meta["input_sha"] == mg.checksum(model.particle_position)
+    assert max(meta["reference_run_to_run_spread"]) <= tolerance("vm_rigid", 128)
+    fx = np.load(GOLDEN / "vm_rigid.npz")
+    o = oracle_mod.OracleScene(cfg, [model])
+    o.set_rigid(cfg.GetRigidParticleCount(), cfg.GetRigidParticleVelocity(0))
+    o.setup()
+    for k in range(meta["frames"]):
+        o.set_rigid_velocity(cfg.GetRigidParticleVelocity(k))
+        o.step(meta["substeps_per_frame"], meta["dt"])
+        if k not in meta["kept_frames"]:
+            continue
+        st = o.state(0)
+        x = st["x"][st["alive"]]
+        ref = fx[f"frame{k}"]
+        assert len(x) == len(ref) == meta["counts"][k]
+        err = nn_error(x, ref)
+        print(f"vm_rigid frame {k}: oracle vs reference {err:.3e}")
+        assert err <= tolerance("vm_rigid", (k + 1) * meta["substeps_per_frame"]), (k, err)

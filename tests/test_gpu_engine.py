@@ -248,3 +248,47 @@ def test_other_materials_parity(engine_lib, oracle_mod, kind):
     s = run_engine(cfg, models, 40, 1e-4)
     o = run_oracle(oracle_mod, cfg, models, 40, 1e-4)
     compare(s, o, check_aux=(kind == "nacc"), f_left=(kind == "nacc"))
+
+
+def test_rigid_particles_parity(engine_lib, oracle_mod):
+    """Rigid particles (include/mpm_algorithm.cuh:1063-1069, 1540-1543,
+    1609-1624): the first 2048 particles of the von Mises cube are rigid and
+    their velocity changes every 10 substeps; engine and oracle agree on every
+    particle (rigid ones: x exactly advected, F = I, v = 0, aux = 0)."""
+    cfg, models = scenes.material_cube("von_mises")
+    R = 2048
+    vel = [(2.0, -1.0, 0.5), (0.0, 1.5, -1.0), (-1.0, 0.0, 0.0), (0.5, 0.5, 0.5)]
+    s = Scene(cfg)
+    s.set_rigid(R, vel[0])
+    s.add_model(models[0])
+    s.setup()
+    o = oracle_mod.OracleScene(cfg, models)
+    o.set_rigid(R, vel[0])
+    o.setup()
+    for v in vel:
+        s.set_rigid_velocity(v)
+        o.set_rigid_velocity(v)
+        s.step(10, 1e-4)
+        o.step(10, 1e-4)
+    compare(s, o, check_aux=True)
+    g = s.state(0)
+    rigid = g.id < R
+    assert rigid.sum() == R and np.all(g.aux[rigid] == 0.0) and np.all(g.aux[~rigid] == 1.0)
+    assert np.abs(g.v[rigid]).max() == 0.0
+    assert np.abs(g.F[rigid] - np.eye(3, dtype=np.float32)).max() == 0.0
+
+
+def test_rigid_particles_api(engine_lib):
+    cfg, models = scenes.material_cube("von_mises")
+    s = Scene(cfg)
+    with pytest.raises(capi.CkmpmError, match="rigid particles are off"):
+        s.set_rigid_velocity((1.0, 0.0, 0.0))
+    with pytest.raises(capi.CkmpmError, match="finite"):
+        s.set_rigid(4, (float("nan"), 0.0, 0.0))
+    s.add_model(models[0])
+    s.setup()
+    with pytest.raises(capi.CkmpmError, match="before ckmpm_setup"):
+        s.set_rigid(4, (1.0, 0.0, 0.0))
+    # Rigid particles off: the von Mises flag stays 1 and no particle is rigid.
+    s.step(4, 1e-4)
+    assert np.all(s.state(0).aux == 1.0)

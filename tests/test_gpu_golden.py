@@ -65,3 +65,27 @@ def test_engine_simulate_matches_reference_adaptive(engine_lib):
         err = nn_error(frames[k], fx[f"frame{k}"])
         print(f"jelly_adaptive frame {k}: engine vs reference {err:.3e} ({n} substeps in total)")
         assert err <= tolerance("jelly_adaptive", n), (k, err)
+
+
+def test_engine_rigid_matches_reference_build(engine_lib):
+    """Rigid particles through the reference-shaped MPMEngine (the rigid hooks of
+    MPMConfig, velocity set per frame by Simulate) against the reference with
+    its own rigid hooks on."""
+    sys.path.insert(0, str(GOLDEN))
+    import make_golden
+    from test_golden import nn_error, tolerance
+    from ckmpm_b200 import MPMEngine
+    meta = json.loads((GOLDEN / "golden.json").read_text())["vm_rigid"]
+    cfg, model = make_golden.rigid_scene()
+    fx = np.load(GOLDEN / "vm_rigid.npz")
+    frames = {}
+    eng = MPMEngine()
+    eng.Initialize(cfg)
+    eng.InitializeParticle(cfg, [model])
+    eng.InitialSetup(cfg)
+    eng.Simulate(cfg, export_callback=lambda f, scene: frames.__setitem__(f, scene.state(0).x.copy()),
+                 fixed_substeps_per_frame=meta["substeps_per_frame"])
+    for k in meta["kept_frames"]:
+        err = nn_error(frames[k], fx[f"frame{k}"])
+        print(f"vm_rigid frame {k}: engine vs reference {err:.3e}")
+        assert err <= tolerance("vm_rigid", (k + 1) * meta["substeps_per_frame"]), (k, err)

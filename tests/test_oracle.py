@@ -209,3 +209,35 @@ def test_linear_stored_stress(oracle_mod):
     o.step(1, 1e-4)
     st = o.state(0)
     assert np.isfinite(st["x"]).all() and np.allclose(st["F"][0], np.eye(3))
+
+
+def test_rigid_particles(oracle_mod):
+    """Rigid particles (include/mpm_algorithm.cuh:1063-1069, 1609-1624): the first
+    R particles of a von Mises model move by dt * velocity (the first substep
+    advects with dt = 0), keep F = I and report v = 0; they deposit mass with
+    zero momentum, so the deformable rest of the cube moves differently from a
+    run without them.  The rigid flag is aux (1 deformable, 0 rigid)."""
+    cfg, models = scenes.material_cube("von_mises")
+    R, dt, n = 2048, 1e-4, 12
+    vr = np.array([2.0, -1.0, 0.5])
+    o = oracle_mod.OracleScene(cfg, models)
+    o.set_rigid(R, vr)
+    o.setup()
+    x0 = o.state(0)["x"].copy()
+    o.step(n, dt)
+    st = o.state(0)
+    assert np.array_equal(st["aux"][:R], np.zeros(R)) and np.all(st["aux"][R:] == 1.0)
+    np.testing.assert_allclose(st["x"][:R] - x0[:R], np.tile((n - 1) * dt * vr, (R, 1)), rtol=0, atol=1e-12)
+    assert np.abs(st["F"][:R] - np.eye(3)).max() == 0.0
+    assert np.abs(st["v"][:R]).max() == 0.0
+    free = oracle_mod.OracleScene(cfg, models)
+    free.setup()
+    free.step(n, dt)
+    ref = free.state(0)
+    assert np.all(ref["aux"] == 1.0)
+    # The deformable particles next to the rigid slab feel its zero-momentum mass.
+    assert np.abs(st["x"][R:] - ref["x"][R:]).max() > 1e-7
+    # A velocity change applies to the following substeps only.
+    o.set_rigid_velocity(-vr)
+    o.step(3, dt)
+    np.testing.assert_allclose(o.state(0)["x"][:R] - st["x"][:R], np.tile(-3 * dt * vr, (R, 1)), rtol=0, atol=1e-12)
