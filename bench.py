@@ -145,14 +145,16 @@ def measured_peak() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def committed_traffic() -> float | None:
-    """DRAM bytes per fused launch from the committed ncu summary, scaled to this workload."""
+def committed_traffic(workload: str) -> float | None:
+    """DRAM bytes per particle of one fused launch from the committed ncu summary
+    of this workload (profiles/traffic.json); the caller scales it by the
+    particles of its launch."""
     p = ROOT / "profiles" / "traffic.json"
     if not p.exists():
         return None
     try:
-        d = json.loads(p.read_text())
-        return float(d["dram_bytes_per_particle"]) if "dram_bytes_per_particle" in d else None
+        d = json.loads(p.read_text()).get(workload)
+        return float(d["dram_bytes_per_particle"]) if d else None
     except Exception:
         return None
 
@@ -428,8 +430,10 @@ def run_batched(args, rank, world, local_rank):
     alg_bytes = 7168 * grid_blocks + sum(int((kinds == k).sum()) * (2 * STATE_BYTES[k] + 8) for k in STATE_BYTES)
     peak, peak_kind = measured_peak()
     achieved = alg_bytes / (avg_fused / 1e3) / 1e9
+    tpp = committed_traffic(args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "g2p2g_kernel<kMixed> (all scenes of the shard in one launch)",
+                "traffic": (tpp * n_live) if tpp else None,
+                "kernel": "g2p2g_kernel<kMixed> (all scenes of the shard in one launch)",
                 "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_fused,
                 "peak_source": f"{peak_kind} hbm_gbs", "fused_share": fused_ms / max(fused_ms + other_ms, 1e-9)}
     b.close()
@@ -575,7 +579,7 @@ def run_ours(args, rank, world, local_rank):
         alg_bytes += s.count(i) * (2 * STATE_BYTES[m.material.kind_code] + 8)
     peak, peak_kind = measured_peak()
     achieved = alg_bytes / (avg_fused / 1e3) / 1e9
-    tpp = committed_traffic() if args.workload == "sand_column" else None
+    tpp = committed_traffic(args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (tpp * n_live) if tpp else None,
                 "kernel": "g2p2g_kernel (fused grid update + G2P + SVD/return map + rebin + P2G), all models",
