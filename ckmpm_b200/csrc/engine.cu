@@ -111,23 +111,28 @@ void free_graphs(ckmpm_scene* s) {
   s->graph_chunk = s->graph_one = nullptr;
 }
 
-template <int KIND, int NT>
+template <int KIND, int NT, bool RIGID>
 cudaError_t launch_fused(ckmpm_scene* s, const ModelHost& m) {
-  g2p2g_kernel<KIND, NT><<<s->fused_ctas, NT, kSmemFused, s->stream>>>(s->sc, m.dev, s->grid, s->scal);
+  g2p2g_kernel<KIND, NT, RIGID><<<s->fused_ctas, NT, kSmemFused, s->stream>>>(s->sc, m.dev, s->grid, s->scal);
   return cudaGetLastError();
+}
+
+template <int NT, bool RIGID>
+cudaError_t launch_fused_kind(ckmpm_scene* s, const ModelHost& m) {
+  switch (m.mat.kind) {
+    case CKMPM_FIXED_COROTATED: return launch_fused<kFixedCorotated, NT, RIGID>(s, m);
+    case CKMPM_LINEAR: return launch_fused<kLinear, NT, RIGID>(s, m);
+    case CKMPM_DRUCKER_PRAGER: return launch_fused<kDruckerPrager, NT, RIGID>(s, m);
+    case CKMPM_VON_MISES: return launch_fused<kVonMises, NT, RIGID>(s, m);
+    case CKMPM_NACC: return launch_fused<kNacc, NT, RIGID>(s, m);
+    default: return launch_fused<kFluid, NT, RIGID>(s, m);
+  }
 }
 
 template <int NT>
 cudaError_t launch_fused_nt(ckmpm_scene* s, const ModelHost& m) {
-  switch (m.mat.kind) {
-    case CKMPM_FIXED_COROTATED: return launch_fused<kFixedCorotated, NT>(s, m);
-    case CKMPM_LINEAR: return launch_fused<kLinear, NT>(s, m);
-    case CKMPM_DRUCKER_PRAGER: return launch_fused<kDruckerPrager, NT>(s, m);
-    case CKMPM_VON_MISES: return launch_fused<kVonMises, NT>(s, m);
-    case CKMPM_NACC: return launch_fused<kNacc, NT>(s, m);
-    case kMixedKind: return launch_fused<kMixed, NT>(s, m);
-    default: return launch_fused<kFluid, NT>(s, m);
-  }
+  if (m.mat.kind == kMixedKind) return launch_fused<kMixed, NT, false>(s, m);  // batches have no rigid particles
+  return s->sc.rigid ? launch_fused_kind<NT, true>(s, m) : launch_fused_kind<NT, false>(s, m);
 }
 
 cudaError_t launch_fused_any(ckmpm_scene* s, const ModelHost& m) {
@@ -136,13 +141,19 @@ cudaError_t launch_fused_any(ckmpm_scene* s, const ModelHost& m) {
 
 template <int NT>
 cudaError_t set_fused_attributes(int* occ) {
-  const void* fns[7] = {reinterpret_cast<const void*>(g2p2g_kernel<kFixedCorotated, NT>),
-                        reinterpret_cast<const void*>(g2p2g_kernel<kLinear, NT>),
-                        reinterpret_cast<const void*>(g2p2g_kernel<kDruckerPrager, NT>),
-                        reinterpret_cast<const void*>(g2p2g_kernel<kFluid, NT>),
-                        reinterpret_cast<const void*>(g2p2g_kernel<kVonMises, NT>),
-                        reinterpret_cast<const void*>(g2p2g_kernel<kNacc, NT>),
-                        reinterpret_cast<const void*>(g2p2g_kernel<kMixed, NT>)};
+  const void* fns[13] = {reinterpret_cast<const void*>(g2p2g_kernel<kFixedCorotated, NT>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kLinear, NT>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kDruckerPrager, NT>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kFluid, NT>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kVonMises, NT>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kNacc, NT>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kMixed, NT>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kFixedCorotated, NT, true>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kLinear, NT, true>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kDruckerPrager, NT, true>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kFluid, NT, true>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kVonMises, NT, true>),
+                         reinterpret_cast<const void*>(g2p2g_kernel<kNacc, NT, true>)};
   int lowest = 1 << 30;
   for (const void* fn : fns) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemFused));

@@ -401,26 +401,38 @@ __device__ __forceinline__ void g2p(const float4* __restrict__ vtile, const floa
   for (int r = 0; r < 3; ++r) v[r] = 0.5f * vs[r];
 }
 
-// Exact 64-bit integer add into shared memory with two native 32-bit
+// The P2G tile holds 4 channels x 1024 nodes of exact 64-bit sums as two
+// planes of 32-bit words: the low words first, the high words kTilePlane
+// words later.  With the halves in separate planes, the low-word atomics of a
+// warp spread over all 32 banks (interleaved 64-bit words would put every low
+// word in an even bank); measured 5 % faster on the sand column and 9 % on
+// small batched scenes.
+constexpr int kTilePlane = kTileNodes * 4;
+
+// Exact 64-bit integer add into the tile with two native 32-bit shared
 // atomics: the low word's returned old value gives the carry into the high
 // word.  Integer addition is associative, so the final 64-bit value is the
 // exact sum whatever order the adds arrive in (64-bit shared atomics are not
 // native on this part and measured 1.7x slower as a whole kernel).
-__device__ __forceinline__ void fixed_add(unsigned long long* p, long long v) {
-  unsigned* w = reinterpret_cast<unsigned*>(p);
+__device__ __forceinline__ void fixed_add(unsigned* lo_word, long long v) {
   const unsigned lo = static_cast<unsigned>(v);
-  const unsigned old = atomicAdd(w, lo);
-  atomicAdd(w + 1, static_cast<unsigned>(v >> 32) + ((old + lo < old) ? 1u : 0u));
+  const unsigned old = atomicAdd(lo_word, lo);
+  atomicAdd(lo_word + kTilePlane, static_cast<unsigned>(v >> 32) + ((old + lo < old) ? 1u : 0u));
+}
+
+// The 64-bit sum of tile word i (node index + channel * kTileNodes).
+__device__ __forceinline__ unsigned long long tile_sum(const unsigned* tile, int i) {
+  return static_cast<unsigned long long>(tile[i]) | (static_cast<unsigned long long>(tile[i + kTilePlane]) << 32);
 }
 
 // Scatter one particle's mass and momentum into the fixed-point tile.  The
-// tile is channel-major, [m, mvx, mvy, mvz][grid][8][8][8] as 64-bit sums, so
+// tile is channel-major, [m, mvx, mvy, mvz][grid][8][8][8] in each plane, so
 // lanes of a warp that update different nodes of one channel fall in
 // different banks (measured 17 % faster than node-major for the whole kernel).
 // Per unit particle mass: node mass w, node momentum w (v + Ah (d - o)) with
 // Ah = A dx / m (A the reference's affine contribution).  Integer atomics make
 // the tile sum independent of the order in which particles arrive.
-__device__ __forceinline__ void p2g_scatter(unsigned long long* __restrict__ ptile, const AxisStencil (&st)[2][3],
+__device__ __forceinline__ void p2g_scatter(unsigned* __restrict__ ptile, const AxisStencil (&st)[2][3],
                                             const int (&lbase)[2][3], const float* v, const float* Ah) {
 #pragma unroll
   for (int g = 0; g < 2; ++g) {
@@ -431,7 +443,7 @@ __device__ __forceinline__ void p2g_scatter(unsigned long long* __restrict__ pti
     const float wx[2] = {st[g][0].w0 * kFixScale, (1.f - st[g][0].w0) * kFixScale};
     const float wy[2] = {st[g][1].w0, 1.f - st[g][1].w0};
     const float wz[2] = {st[g][2].w0, 1.f - st[g][2].w0};
-    unsigned long long* base = ptile + ((g * 8 + lbase[g][0]) * 64 + lbase[g][1] * 8 + lbase[g][2]);
+    unsigned* base = ptile + ((g * 8 + lbase[g][0]) * 64 + lbase[g][1] * 8 + lbase[g][2]);
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
       const int dxn = (n >> 2) & 1, dyn = (n >> 1) & 1, dzn = n & 1;
@@ -444,7 +456,7 @@ __device__ __forceinline__ void p2g_scatter(unsigned long long* __restrict__ pti
         if (dyn) val[r] += Ah[r * 3 + 1];
         if (dzn) val[r] += Ah[r * 3 + 2];
       }
-      unsigned long long* node = base + (dxn * 64 + dyn * 8 + dzn);
+      unsigned* node = base + (dxn * 64 + dyn * 8 + dzn);
       const long long fx[4] = {__float2ll_rn(w), __float2ll_rn(w * val[0]), __float2ll_rn(w * val[1]),
                                __float2ll_rn(w * val[2])};
 #pragma unroll
@@ -463,7 +475,7 @@ __device__ __forceinline__ void p2g_scatter(unsigned long long* __restrict__ pti
 // stamped before the launch; ratio rescales a model's per-unit-mass sums to
 // the grid's unit (1 when the scene has one particle mass).
 template <int NT>
-__device__ __forceinline__ void flush_tile(const SceneDev& sc, int4 key, const unsigned long long* __restrict__ ptile,
+__device__ __forceinline__ void flush_tile(const SceneDev& sc, int4 key, const unsigned* __restrict__ ptile,
                                            double ratio, long long* __restrict__ gout) {
   int64_t fb[8];
 #pragma unroll
@@ -481,8 +493,10 @@ __device__ __forceinline__ void flush_tile(const SceneDev& sc, int4 key, const u
     const int w = i & 127;
     const int gi = w >> 6, cell = w & 63;
     const int lx = (e >> 2) * 4 + (cell >> 4), ly = ((e >> 1) & 1) * 4 + ((cell >> 2) & 3), lz = (e & 1) * 4 + (cell & 3);
-    const unsigned long long* src = ptile + ((gi * 8 + lx) * 64 + ly * 8 + lz);
-    unsigned long long v[4] = {src[0], src[kTileNodes], src[2 * kTileNodes], src[3 * kTileNodes]};
+    const int node = (gi * 8 + lx) * 64 + ly * 8 + lz;
+    unsigned long long v[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) v[c] = tile_sum(ptile, node + c * kTileNodes);
     if ((v[0] | v[1] | v[2] | v[3]) == 0ull) continue;
     if (ratio != 1.0) {
 #pragma unroll
@@ -581,7 +595,7 @@ struct SharedSmall {
 };
 
 constexpr size_t kSmemVTile = sizeof(float4) * 344;                      // 5.5 KB (341 nodes)
-constexpr size_t kSmemPTile = sizeof(unsigned long long) * kTileNodes * 4;  // 32 KB
+constexpr size_t kSmemPTile = sizeof(unsigned) * 2 * kTilePlane;            // 32 KB, two planes
 constexpr size_t kSmemCodes = kMaxParticlesPerBlock;                     // 4 KB
 constexpr size_t kSmemFused = kSmemVTile + kSmemPTile + kSmemCodes;
 
@@ -593,19 +607,21 @@ constexpr size_t kSmemFused = kSmemVTile + kSmemPTile + kSmemCodes;
 // (:739-869), the advection record (mpm_particle.cuh:333-371) and the
 // per-block list build (:629-649, :1868-1918).  KIND is the material, or
 // kMixed for a batch, where each work item reads its scene's material (one
-// scene per stacked domain, so the kind is uniform across the CTA).  Register
+// scene per stacked domain, so the kind is uniform across the CTA).  RIGID
+// compiles the rigid-particle test in (scenes with rigid particles on; the
+// test alone cost 1.7 % on the sand column).  Register
 // budget: 64 per thread at 256 threads (4 CTAs per SM); at 128 threads the
 // shared-memory footprint allows 5 CTAs per SM, so up to 102 registers.
 template <int NT>
 constexpr int fused_min_ctas() { return NT == 128 ? 5 : 1024 / NT; }
 
-template <int KIND, int NT>
+template <int KIND, int NT, bool RIGID = false>
 __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
     g2p2g_kernel(SceneDev sc, ModelDev md, GridDev gd, Scalars* __restrict__ scal) {
   static_assert(NT % 32 == 0 && NT / 32 <= 8 && NT >= 64, "block size");
   extern __shared__ __align__(16) unsigned char smem[];
   float4* vtile = reinterpret_cast<float4*>(smem);
-  unsigned long long* ptile = reinterpret_cast<unsigned long long*>(smem + kSmemVTile);
+  unsigned* ptile = reinterpret_cast<unsigned*>(smem + kSmemVTile);
   uint8_t* dcode = smem + kSmemVTile + kSmemPTile;
   __shared__ SharedSmall sh;
 
@@ -652,7 +668,8 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
     else if (threadIdx.x < 40)
       window_blocks(sc, stin, read_epoch, key, sh.blk, threadIdx.x - 32);
     for (int i = threadIdx.x; i < 8 * 28; i += NT) (&sh.wcnt[0][0])[i] = 0u;
-    for (int i = threadIdx.x; i < kTileNodes * 4; i += NT) ptile[i] = 0ull;
+    for (int i = threadIdx.x; i < 2 * kTilePlane / 4; i += NT)
+      reinterpret_cast<uint4*>(ptile)[i] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
     load_velocity_tile<NT>(sc, gin, sh.blk, key, unit, dt, vtile);
     __syncthreads();
@@ -685,7 +702,7 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
       float v[3], C[9], Dold[6];
       g2p(vtile, xs, key, dx, v, C, inside, Dold);
       float adv[3] = {v[0], v[1], v[2]};
-      if (sc.rigid && rigid_attribute(kind, F, aux) == 0.f) {
+      if (RIGID && rigid_attribute(kind, F, aux) == 0.f) {
         // Rigid: moves with the scene's rigid velocity and carries no velocity,
         // no affine field and no G2P D (include/mpm_algorithm.cuh:1609-1618).
 #pragma unroll
@@ -878,7 +895,7 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
 template <int NT>
 __global__ void __launch_bounds__(NT, 2) rasterize_kernel(SceneDev sc, ModelDev md, GridDev gd, Scalars* scal) {
   extern __shared__ __align__(16) unsigned char smem[];
-  unsigned long long* ptile = reinterpret_cast<unsigned long long*>(smem + kSmemVTile);
+  unsigned* ptile = reinterpret_cast<unsigned*>(smem + kSmemVTile);
   __shared__ SharedSmall sh;
   const BlockListDev cur = md.bl[0];
   const StateDev s0 = md.st[0];
@@ -893,7 +910,8 @@ __global__ void __launch_bounds__(NT, 2) rasterize_kernel(SceneDev sc, ModelDev 
     const int4 key = cur.keys[item];
     const uint32_t start = cur.start[item];
     const uint32_t n = cur.count[item];
-    for (int i = threadIdx.x; i < kTileNodes * 4; i += NT) ptile[i] = 0ull;
+    for (int i = threadIdx.x; i < 2 * kTilePlane / 4; i += NT)
+      reinterpret_cast<uint4*>(ptile)[i] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
     const int kk[3] = {key.x, key.y, key.z};
     for (uint32_t q = threadIdx.x; q < n; q += NT) {
