@@ -355,6 +355,36 @@ def run_diff(args, rank, world, local_rank):
             fd = (oracle_loss(vp) - oracle_loss(vm)) / (2 * eps)
             ad = float(grad[:, a].sum())
             gradcheck[f"v0_{name}"] = {"fd_fp64": fd, "adjoint_fp32": ad, "rel_err": abs(fd - ad) / max(abs(fd), 1e-30)}
+    # Roofline of the forward substep (grid_kernel + particle_kernel, event-timed
+    # per rollout graph): particle state read + written (x, F: 48 B each way)
+    # plus the per-particle log E and index traffic (8 B); the node arrays stay
+    # in L2 at this size.
+    peak, peak_kind = measured_peak()
+    sub_ms = fwd / nsteps
+    alg = n * (2 * 48 + 8)
+    roofline = {"bound": "hbm", "achieved": alg / (sub_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": alg / (sub_ms / 1e3) / 1e9 / peak, "traffic": None,
+                "kernel": "forward substep of the rollout graph (grid_kernel + particle_kernel)",
+                "algorithmic_bytes_per_launch": alg, "avg_launch_ms": sub_ms, "peak_source": f"{peak_kind} hbm_gbs",
+                "note": "latency-bound: 50.6k particles fill under one wave of 148 SMs (profiles/diff_cube.md)"}
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        E = np.exp(d["logE"].astype(np.float64))
+        lam_p, mu_p = E * d["nu"] / ((1 + d["nu"]) * (1 - 2 * d["nu"])), E / (2 * (1 + d["nu"]))
+        m = MPMModel(d["mass"], d["volume"], d["x0"], d["v0"], MPMMaterial.fixed_corotated(1.0, 1.0))
+        o = O.OracleScene(cfg, [m])
+        o.set_lame(0, lam_p, mu_p)
+        o.setup()
+        o.step(1, d["dt"])
+        t0 = time.perf_counter()
+        k = 8
+        o.step(k, d["dt"])
+        t = time.perf_counter() - t0
+        o.close()
+        cpu = {"value": n * k / t, "unit": METRIC, "cores": 1, "kind": "port",
+               "sample": f"FP64 serial oracle forward (oracle/ckmpm_oracle.cpp), {k} substeps of the {n}-particle "
+                         f"cube with per-particle Lame parameters, {t:.1f} s; no adjoint on the CPU"}
     line = {
         "metric": METRIC, "value": n * nsteps / (fwd / 1e3), "unit": METRIC, "n_gpus": world, "steps": steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -367,7 +397,8 @@ def run_diff(args, rank, world, local_rank):
         "fwd_adj_over_fwd": (fwd + bwd) / fwd,
         "plain_forward_ms": plain_ms, "fwd_adj_over_plain_forward": (fwd + bwd) / plain_ms,
         "train_step_particle_substeps_per_s": n * nsteps / (ms / 1e3),
-        "gradcheck": gradcheck, "loss": float(loss.item()), "clocks": clocks,
+        "gradcheck": gradcheck, "loss": float(loss.item()), "clocks": clocks, "roofline": roofline,
+        "cpu_baseline": cpu,
         "gpu_launches": 4 + 2 * nsteps + 1 + (2 * nsteps + 2 * nsteps) + 4,
         "e2e": {"value": n * nsteps / (ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 8, "includes": "torch tensors already on the device; loss read back per step"},
