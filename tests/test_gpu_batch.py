@@ -158,3 +158,24 @@ def test_batch_argument_errors(engine_lib):
     b.setup()
     with pytest.raises(CkmpmError):
         b.blocks_in(3)
+
+
+def test_batch_with_every_material_equals_scenes_alone(engine_lib):
+    """von Mises, NACC and linear scenes (the kinds the batched workload does not
+    draw) next to fixed-corotated, fluid and Drucker-Prager scenes in one batch:
+    every scene bitwise equal to the same scene run alone."""
+    cfg, models = small_batch(n=6, seed=5)
+    for kind in ("von_mises", "nacc", "linear"):
+        c2, m2 = scenes.material_cube(kind)
+        assert c2.dx == cfg.dx and tuple(c2.domain_blocks) == tuple(cfg.domain_blocks)
+        models.append(m2[0])
+    b = run_batch(cfg, models, 24)
+    st = b.state()
+    kinds = set()
+    for i, m in enumerate(models):
+        alone = run_alone(cfg, m, 24)
+        assert_same_state(b.scene_state(i, st), alone.state(0), f"scene {i} ({m.material.kind})")
+        kinds.add(m.material.kind)
+        alone.close()
+    assert {"von_mises", "nacc", "linear"} <= kinds
+    assert b.counters()["status"] == 0

@@ -292,3 +292,21 @@ def test_rigid_particles_api(engine_lib):
     # Rigid particles off: the von Mises flag stays 1 and no particle is rigid.
     s.step(4, 1e-4)
     assert np.all(s.state(0).aux == 1.0)
+
+
+def test_model_entirely_outside_the_domain(engine_lib):
+    """A model whose particles all lie outside the domain is dropped at setup
+    (counted as lost, zero live particles, empty state) and leaves the other
+    model's simulation bitwise unchanged."""
+    cfg, models = scenes.jelly_cube(lo=(0.44, 0.44, 0.44), hi=(0.56, 0.56, 0.56))
+    m = models[0]
+    out = MPMModel(m.particle_mass, m.particle_volume, (m.particle_position + 2.0).astype(np.float32),
+                   m.particle_velocity, m.material)
+    s = run_engine(cfg, [m, out], 12, 1e-4)
+    alone = run_engine(cfg, [m], 12, 1e-4)
+    assert s.count(1) == 0 and s.counters()["lost"] == len(out.particle_position)
+    empty = s.state(1)
+    assert empty.x.shape == (0, 3) and empty.id.shape == (0,)
+    a, b = s.state(0), alone.state(0)
+    for name in ("id", "x", "v", "F"):
+        assert np.array_equal(getattr(a, name), getattr(b, name)), name
