@@ -667,19 +667,23 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
       incoming_groups(sc, prev, key, sh.off, sh.idx, sh.src);
     else if (threadIdx.x < 40)
       window_blocks(sc, stin, read_epoch, key, sh.blk, threadIdx.x - 32);
-    for (int i = threadIdx.x; i < 8 * 28; i += NT) (&sh.wcnt[0][0])[i] = 0u;
+    for (int i = threadIdx.x; i < static_cast<int>(sizeof(sh.wcnt) / sizeof(uint32_t)); i += NT)
+      (&sh.wcnt[0][0])[i] = 0u;
     for (int i = threadIdx.x; i < 2 * kTilePlane / 4; i += NT)
       reinterpret_cast<uint4*>(ptile)[i] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
     load_velocity_tile<NT>(sc, gin, sh.blk, key, unit, dt, vtile);
     __syncthreads();
+    // The block's output slots [start, start + n) must lie in the state arrays;
+    // counts that say otherwise are flagged and clamped, never written past.
+    const uint32_t room = start < md.cap_particles ? md.cap_particles - start : 0u;
     if (threadIdx.x == 0) {
       uint32_t flags = 0;
-      if (sh.off[27] != n) flags |= kStatusConsistency;
+      if (sh.off[27] != n || n > room) flags |= kStatusConsistency;
       if (n > maxp) flags |= kStatusCapacity;
       if (flags) set_status(scal, flags);
     }
-    n = min(min(n, sh.off[27]), maxp);
+    n = min(min(min(n, sh.off[27]), maxp), room);
 
     for (uint32_t q = threadIdx.x; q < n; q += NT) {
       const int d = find_group(sh.off, q);
@@ -1273,7 +1277,7 @@ __global__ void __launch_bounds__(NT) probe_kernel(SceneDev sc, ModelDev md, Gri
     if (ov) load_velocity_tile<NT>(sc, gd.grid[parity], sh.blk, key, md.smat ? md.smat[key.w].unit : sc.grid_unit, dt,
                                    vtile);
     __syncthreads();
-    const uint32_t nn = min(n, sh.off[27]);
+    const uint32_t nn = min(min(n, sh.off[27]), start < md.cap_particles ? md.cap_particles - start : 0u);
     for (uint32_t q = threadIdx.x; q < nn; q += NT) {
       const int d = find_group(sh.off, q);
       const uint32_t ii = sh.idx[d] + (q - sh.off[d]);
