@@ -246,8 +246,8 @@ ckmpm_status ckmpm_get_blocks_in(ckmpm_scene* s, uint32_t scene, int32_t model, 
 
 /* ---- Launch shape of the fused substep kernel.  No counterpart in the
  * reference (fixed launch shapes, include/mpm_engine.cuh:519-866).  Results do
- * not depend on it: the P2G sums are exact integers and the grid flushes are
- * ordered by block colour. */
+ * not depend on it: the P2G tile and the grid hold exact integer sums, so the
+ * order in which blocks deposit never changes a bit. */
 typedef struct ckmpm_tuning {
   uint32_t threads;      /* CTA size: 128 or 256 */
   uint32_t ctas_per_sm;  /* resident persistent CTAs per SM, 1..occupancy */

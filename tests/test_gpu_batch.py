@@ -2,8 +2,8 @@
 
 A batch advances every scene in the same launches; each scene must come out
 exactly as the same scene run alone: the per-particle arithmetic is the same,
-P2G sums are exact integers and grid flushes are ordered by block colour, so
-the comparison is bitwise (x, v, F, aux, ids, block sets).  Launch shape
+P2G tile and the grid hold exact integer sums, so the order in which blocks
+deposit does not matter and the comparison is bitwise (x, v, F, aux, ids, block sets).  Launch shape
 (ckmpm_set_tuning, ckmpm_autotune) and checkpoint save/restore must not change
 any bit either.  Three scenes are also checked against the FP64 oracle with
 the tolerances of the plain-path parity tests.
