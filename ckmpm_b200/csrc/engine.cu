@@ -260,7 +260,7 @@ float initial_aux(const ckmpm_material& m) {
 }
 
 ckmpm_status status_from(ckmpm_scene* s, const Scalars& h) {
-  if (h.status & kStatusTimeout) return fail(s, CKMPM_ERR_TIMEOUT, "a bounded device wait gave up (flush ordering)");
+  if (h.status & kStatusTimeout) return fail(s, CKMPM_ERR_TIMEOUT, "a bounded device wait gave up");
   if (h.status & kStatusCapacity)
     return fail(s, CKMPM_ERR_CAPACITY, "block capacity exceeded (particles per block or block table)");
   if (h.status & kStatusNumeric) return fail(s, CKMPM_ERR_NUMERIC, "non-finite or out-of-range P2G contribution");

@@ -1,7 +1,7 @@
 // Device kernels of the CK-MPM substep.
 //
 // Data layout (per scene; a batch stacks `nstack` identical domains, scene w
-// owning table entries [w * blocks, (w + 1) * blocks), and no stencil, wait or
+// owning table entries [w * blocks, (w + 1) * blocks), and no stencil, flush or
 // rebin ever crosses from one stacked domain into another):
 //  * grid[2]: dense over every 4^3 block of the domain, 4 KB per block of
 //    exact 64-bit fixed-point sums (2^-36 of a particle mass per unit):
@@ -13,11 +13,12 @@
 //  * stamp[2]: per block, the epoch for which it was last zeroed; a block whose
 //    stamp is stale reads as empty.  Only the blocks a substep deposits into
 //    are zeroed, by zero_windows_kernel before that substep.
-//  * per model, particle state SoA (x[3], F[9], aux, id) double-buffered and
-//    sorted by particle block; the block list (keys, start, count) in
-//    colour-major key order; a dense block table; 28 outgoing-direction prefix
-//    counts per block and a u16 per-particle index list that records, for each
-//    block, which of its particles leave in which of the 27 directions.
+//  * per model, particle state SoA (x[3], F[9], aux, Q[9] for the linear
+//    model, id) double-buffered and sorted by particle block; the block list
+//    (keys, start, count) in colour-major key order; a dense block table; 28
+//    outgoing-direction prefix counts per block and a u16 per-particle index
+//    list that records, for each block, which of its particles leave in which
+//    of the 27 directions.
 //
 // Every substep is: one fused kernel per model (grid update + G2P + F update,
 // SVD, return map + rebin record + P2G, flushed as exact integer sums), then
@@ -44,9 +45,8 @@ constexpr float kFixMaxValue = 131072.0f;          // |contribution| bound per u
 enum StatusBits : uint32_t {
   kStatusCapacity = 1u,
   kStatusNumeric = 2u,
-  kStatusTimeout = 4u,
+  kStatusTimeout = 4u,  // no device code waits any more; kept so status words keep their meaning
   kStatusConsistency = 8u,
-  kStatusEscape = 16u,
   kStatusOutsideBlock = 32u,
 };
 
@@ -83,7 +83,7 @@ struct Scalars {
   uint32_t status;     // StatusBits
   uint32_t lost;       // particles that left the domain
   uint32_t window_skips;
-  uint32_t timeouts;
+  uint32_t timeouts;    // always 0: the substep has no bounded waits (kept for the counters ABI)
   uint32_t maxv2_bits; // max |v|^2 on the grid (float bits), adaptive dt
   double time;         // simulated time: sum of the dt each substep advanced with
   double frame_end;    // adaptive dt: end of the current frame
