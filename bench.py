@@ -715,6 +715,7 @@ def run_reference(args, rank, world):
             secs += r["seconds"]
         value = work / secs
         cpu = {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
+               "runs_on": "one B200: the reference's implementation of this path is CUDA code",
                "sample": f"reference CUDA build (oracle/_ref/ref_{family}) via MPMEngine::Simulate in profile mode, "
                          f"one process per scene, every 8th scene ({len(sample)} of {len(models)}), "
                          f"{args.warmup + args.steps} substeps each; host timer around each frame loop, summed"}
@@ -722,7 +723,8 @@ def run_reference(args, rank, world):
         from oracle import ref_runner
         res = ref_runner.time_reference(family, cfg, models, args.steps, args.warmup)
         value = res["value"]
-        cpu = {"value": value, "unit": METRIC, "cores": 1, "kind": "reference", "sample": res["sample"]}
+        cpu = {"value": value, "unit": METRIC, "cores": 1, "kind": "reference", "sample": res["sample"],
+               "runs_on": "one B200: the reference's implementation of this path is CUDA code"}
     else:
         cpu = cpu_baseline_oracle(cfg, models, args.cpu_seconds)
         cpu["kind"] = "port"
