@@ -46,7 +46,7 @@ EXPORTED = (
     "ckmpm_version", "ckmpm_simulate_noalloc", "ckmpm_create_batch", "ckmpm_add_batch", "ckmpm_get_blocks_in",
     "ckmpm_set_tuning", "ckmpm_get_tuning", "ckmpm_autotune", "ckmpm_checkpoint_bytes", "ckmpm_checkpoint_save",
     "ckmpm_checkpoint_restore", "ckmpm_diff_create", "ckmpm_diff_forward", "ckmpm_diff_backward", "ckmpm_diff_timing",
-    "ckmpm_diff_last_error", "ckmpm_diff_destroy", "ckmpm_set_rigid", "ckmpm_set_rigid_velocity",
+    "ckmpm_diff_last_error", "ckmpm_diff_destroy", "ckmpm_set_rigid", "ckmpm_set_rigid_velocity", "ckmpm_get_time",
 )
 
 MAX_BATCH_SCENES = 65536
@@ -116,6 +116,7 @@ def lib() -> C.CDLL:
         L.ckmpm_set_stream.argtypes = [P, P]
         L.ckmpm_set_rigid.argtypes = [P, C.c_uint32, C.POINTER(C.c_float)]
         L.ckmpm_set_rigid_velocity.argtypes = [P, C.POINTER(C.c_float)]
+        L.ckmpm_get_time.argtypes = [P, C.POINTER(C.c_double)]
         L.ckmpm_get_count.argtypes = [P, C.c_int32, u32p]
         L.ckmpm_get_state.argtypes = [P, C.c_int32, f32p, f32p, f32p, f32p, u32p, C.c_uint32, u32p]
         L.ckmpm_get_blocks.argtypes = [P, C.c_int32, C.c_int32, i32p, u32p, C.c_uint32, u32p]

@@ -733,15 +733,17 @@ ckmpm_status ckmpm_step(ckmpm_scene* s, uint32_t nsteps, float dt) {
 ckmpm_status ckmpm_step_adaptive(ckmpm_scene* s, uint32_t nsteps, float dt_max, float cfl, double frame_time,
                                  double* elapsed) {
   if (!s || !s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
-  if (!(dt_max > 0.f) || !(cfl > 0.f) || !(frame_time > 0.0))
-    return fail(s, CKMPM_ERR_INVALID, "dt_max, cfl and frame_time must be positive");
+  if (!(dt_max > 0.f) || !(cfl > 0.f) || !(frame_time >= 0.0))
+    return fail(s, CKMPM_ERR_INVALID, "dt_max and cfl must be positive, frame_time non-negative");
   if (s->nstack > 1) return fail(s, CKMPM_ERR_INVALID, "a batch steps with a fixed dt (ckmpm_step)");
   CK_CUDA(s, cudaSetDevice(s->desc.device));
   Scalars h{};
   CK_CUDA(s, cudaMemcpyAsync(&h, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
   CK_CUDA(s, cudaStreamSynchronize(s->stream));
-  const double t0 = h.time, t_end = h.time + frame_time;
-  set_frame_end_kernel<<<1, 32, 0, s->stream>>>(s->scal, frame_time);
+  // frame_time == 0 continues the frame an earlier call opened (a caller that
+  // steps one substep at a time, e.g. to record per-substep diagnostics).
+  const double t0 = h.time, t_end = frame_time > 0.0 ? h.time + frame_time : h.frame_end;
+  if (frame_time > 0.0) set_frame_end_kernel<<<1, 32, 0, s->stream>>>(s->scal, frame_time);
   const int maxv_ctas = s->sm_count * 8;
   float mass_floor = 0.f;
   for (const auto& m : s->models) mass_floor = (mass_floor == 0.f) ? m.mass : std::min(mass_floor, m.mass);
@@ -975,6 +977,16 @@ ckmpm_status ckmpm_get_counters(ckmpm_scene* s, uint64_t* out5) {
   out5[2] = h.window_skips;
   out5[3] = h.status;
   out5[4] = h.timeouts;
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_get_time(ckmpm_scene* s, double* out2) {
+  if (!s || !out2) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  Scalars h{};
+  CK_CUDA(s, cudaMemcpyAsync(&h, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
+  CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  out2[0] = h.time;
+  out2[1] = h.frame_end;
   return CKMPM_OK;
 }
 

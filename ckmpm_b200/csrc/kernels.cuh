@@ -1170,8 +1170,11 @@ __global__ void adaptive_dt_kernel(Scalars* scal, float dx, float cfl, float dt_
   const float v2 = __uint_as_float(scal->maxv2_bits);
   scal->maxv2_bits = 0u;
   if (isinf(v2)) scal->status |= kStatusNumeric;
-  const float vmax = sqrtf(v2);
-  if (vmax > 0.f) next = fmin(next, static_cast<double>(dx * cfl / vmax));
+  // IEEE-rounded square root and division (the library builds with the
+  // approximate ones): the reference takes this bound on the host in FP32
+  // (include/mpm_engine.cuh:540,556), and the dt sequence should match it.
+  const float vmax = __fsqrt_rn(v2);
+  if (vmax > 0.f) next = fmin(next, static_cast<double>(__fdiv_rn(dx * cfl, vmax)));
   if (next < 0.0) next = 0.0;
   scal->next_dt_d = next;
   scal->next_dt = static_cast<float>(next);

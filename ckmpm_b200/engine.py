@@ -313,6 +313,27 @@ class Scene:
                    "ckmpm_step_adaptive", self._h)
         return el.value
 
+    def time(self) -> tuple[float, float]:
+        """(simulated time, end of the current adaptive frame), both in double."""
+        out = (C.c_double * 2)()
+        capi.check(capi.lib().ckmpm_get_time(self._h, out), "ckmpm_get_time", self._h)
+        return out[0], out[1]
+
+    def conservation_metric(self, model: int = 0) -> np.ndarray:
+        """The reference's conservation metric of one model (CollectConservationMetric,
+        include/mpm_algorithm.cuh:1252-1360, written per substep by Simulate,
+        include/mpm_engine.cuh:573-603): rows Eulerian linear and angular
+        momentum (left at zero, as the reference leaves them), Lagrangian linear
+        momentum sum(v) and angular momentum sum(x cross v), per unit particle mass,
+        with v the velocity the next G2P interpolates (zero for rigid particles).
+        Summed in double here; the reference adds floats with atomics."""
+        st = self.state(model)
+        x, v = st.x.astype(np.float64), st.v.astype(np.float64)
+        out = np.zeros((4, 3))
+        out[2] = v.sum(axis=0)
+        out[3] = np.cross(x, v).sum(axis=0)
+        return out
+
     def step_profiled(self, nsteps: int, dt: float) -> tuple[float, float, int]:
         out = (C.c_double * 3)()
         capi.check(capi.lib().ckmpm_step_profiled(self._h, nsteps, dt, out), "ckmpm_step_profiled", self._h)
@@ -456,7 +477,7 @@ class MPMEngine:
         return out
 
     def Simulate(self, config: MPMConfig, export_callback=None, fixed_substeps_per_frame: int | None = None,
-                 export_root: str | Path | None = None) -> int:
+                 export_root: str | Path | None = None, collect_conservation_metric: bool = False) -> int:
         """Run GetTotalSimulatedFrameCount() frames; returns the substeps taken.
 
         As the reference's Simulate (include/mpm_engine.cuh:457-909): every
@@ -465,20 +486,57 @@ class MPMEngine:
         exactly on its boundary.  With fixed_substeps_per_frame every substep
         uses dt_ instead.  export_callback(frame_index, scene) runs after every
         frame (the reference's ExportParticleToModel point, :880-883).
+
+        collect_conservation_metric records the conservation metric of every
+        model before every substep (:573-603), stepping one substep at a time
+        (same results, slower): `self.conservation_records[i]` holds rows of 13
+        values (time, then the four vectors of Scene.conservation_metric), and
+        with export_root they are also written, float32, to
+        <root>/conservationMetric_model_<i>.bin as the reference writes them.
         """
         assert self.scene is not None
         start = self.scene.counters()["steps"]
+        nmodels = len(self.scene.models)
+        if collect_conservation_metric:
+            self.conservation_records = [[] for _ in range(nmodels)]
+
+        def record():
+            t = self.scene.time()[0]
+            for i in range(nmodels):
+                self.conservation_records[i].append(np.concatenate([[t], self.scene.conservation_metric(i).ravel()]))
+
         for frame in range(config.GetTotalSimulatedFrameCount()):
             if config.GetExistRigidParticle():  # the hook is evaluated per frame (mpm_algorithm.cuh:1614)
                 self.scene.set_rigid_velocity(config.GetRigidParticleVelocity(frame))
-            if fixed_substeps_per_frame:
-                self.scene.step(fixed_substeps_per_frame, self.dt_)
+            if not collect_conservation_metric:
+                if fixed_substeps_per_frame:
+                    self.scene.step(fixed_substeps_per_frame, self.dt_)
+                else:
+                    self.scene.step_adaptive(1 << 30, self.dt_, config.GetCfl(), 1.0 / config.GetFps())
+            elif fixed_substeps_per_frame:
+                for _ in range(fixed_substeps_per_frame):
+                    record()
+                    self.scene.step(1, self.dt_)
             else:
-                self.scene.step_adaptive(1 << 30, self.dt_, config.GetCfl(), 1.0 / config.GetFps())
+                # One substep per call; frame_time 0 continues the frame the first call opened.
+                frame_time = 1.0 / config.GetFps()
+                while True:
+                    if frame_time == 0.0:
+                        t, frame_end = self.scene.time()
+                        if not frame_end - t > 0.0:
+                            break
+                    record()
+                    self.scene.step_adaptive(1, self.dt_, config.GetCfl(), frame_time)
+                    frame_time = 0.0
             if export_root is not None:
                 self.ExportParticleToModel(export_root, frame)
             if export_callback is not None:
                 export_callback(frame, self.scene)
+        if collect_conservation_metric and export_root is not None:
+            root = Path(export_root)
+            root.mkdir(parents=True, exist_ok=True)
+            for i, rows in enumerate(self.conservation_records):
+                np.asarray(rows, np.float32).reshape(-1, 13).tofile(root / f"conservationMetric_model_{i}.bin")
         return self.scene.counters()["steps"] - start
 
 

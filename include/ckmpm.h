@@ -121,7 +121,8 @@ ckmpm_status ckmpm_status_check(ckmpm_scene* s);
 /* Adaptive step, the reference's CFL rule (include/mpm_engine.cuh:552-557):
  * next dt = min(dt_max, frame_remaining, dx * cfl / max|v_grid|), computed on
  * the device from the grid of the previous substep.  Advances nsteps substeps
- * and returns the simulated time in *elapsed (may be NULL). */
+ * and returns the simulated time in *elapsed (may be NULL).  frame_time = 0
+ * continues the frame an earlier call opened (stepping one substep at a time). */
 ckmpm_status ckmpm_step_adaptive(ckmpm_scene* s, uint32_t nsteps, float dt_max, float cfl, double frame_time,
                                  double* elapsed);
 
@@ -177,6 +178,11 @@ ckmpm_status ckmpm_get_counters(ckmpm_scene* s, uint64_t* out5);
 
 /* Current dt pair: [0] the dt the next substep advects with, [1] the dt it deposits stress with. */
 ckmpm_status ckmpm_get_dt(ckmpm_scene* s, float* out2);
+
+/* Simulated time in double, as the reference keeps its clock (currentTimestamp_,
+ * include/mpm_engine.cuh:514-552): [0] the sum of the dt every substep advanced
+ * with, [1] the end of the frame the last ckmpm_step_adaptive opened. */
+ckmpm_status ckmpm_get_time(ckmpm_scene* s, double* out2);
 
 /* Run nsteps substeps without graphs, timing every kernel with CUDA events on
  * the scene's stream.  ms_out[0]: total of the fused G2P2G launches, [1]: total

@@ -310,3 +310,56 @@ def test_model_entirely_outside_the_domain(engine_lib):
     a, b = s.state(0), alone.state(0)
     for name in ("id", "x", "v", "F"):
         assert np.array_equal(getattr(a, name), getattr(b, name)), name
+
+
+def test_conservation_metric(engine_lib, oracle_mod, tmp_path):
+    """The reference's conservation metric (Lagrangian sum(v) and sum(x cross v)
+    before every substep, include/mpm_engine.cuh:573-603): written as 13 float32
+    per substep; collecting it steps one substep at a time without changing a
+    bit of the simulation; its x and z momentum of a free-flying cube stay at
+    N v0 (APIC transfers conserve momentum; gravity acts on y only); and it
+    matches the FP64 oracle's sums at the end."""
+    from ckmpm_b200 import MPMEngine
+    cfg, models = scenes.jelly_cube(lo=(0.44, 0.44, 0.44), hi=(0.56, 0.56, 0.56), v0=(0.3, -1.0, 0.2))
+    cfg.dt, cfg.fps, cfg.total_frames = 2.0 ** -14, 1024, 4
+    n = len(models[0].particle_position)
+    finals = {}
+    for mode in ("fixed", "adaptive"):
+        for collect in (False, True):
+            eng = MPMEngine()
+            eng.Initialize(cfg)
+            eng.InitializeParticle(cfg, models)
+            eng.InitialSetup(cfg)
+            root = tmp_path / f"{mode}_{collect}"
+            eng.Simulate(cfg, fixed_substeps_per_frame=16 if mode == "fixed" else None,
+                         export_root=root if collect else None, collect_conservation_metric=collect)
+            finals[(mode, collect)] = eng.scene.state(0).x.copy()
+            if collect:
+                rec = np.fromfile(root / "conservationMetric_model_0.bin", np.float32).reshape(-1, 13)
+                assert rec.shape[0] == 64 and np.all(np.diff(rec[:, 0]) >= 0)
+                assert np.all(rec[:, 1:7] == 0.0)  # the Eulerian rows stay zero, as in the reference
+                np.testing.assert_allclose(rec[:, 7], n * 0.3, rtol=1e-5)
+                np.testing.assert_allclose(rec[:, 9], n * 0.2, rtol=1e-5)
+                last = eng.scene.conservation_metric(0)
+        assert np.array_equal(finals[(mode, False)], finals[(mode, True)]), mode
+    o = run_oracle(oracle_mod, cfg, models, 64, cfg.dt)
+    r = o.state(0)
+    ref = np.array([r["v"].sum(axis=0), np.cross(r["x"], r["v"]).sum(axis=0)])
+    s = run_engine(cfg, models, 64, cfg.dt)
+    got = s.conservation_metric(0)[2:]
+    assert np.abs(got - ref).max() <= 5e-5 * np.abs(ref).max(), (got, ref)
+
+
+def test_momentum_conserved_on_the_full_sand_column(engine_lib):
+    """Size-independent property at the benchmark's full size (1.69M particles):
+    the column starts at rest and nothing acts on it along x or z but its own
+    stress (the slip floor only limits v_y, the walls are far), so the
+    Lagrangian x and z momentum stay at zero up to FP32 noise."""
+    cfg, models = scenes.sand_column(track_ids=False)
+    s = run_engine(cfg, models, 200, cfg.dt)
+    st = s.state(0)
+    n, vmax = len(st.v), float(np.abs(st.v).max())
+    m = s.conservation_metric(0)[2]
+    assert vmax > 1e-3
+    assert abs(m[0]) <= 1e-4 * n * vmax and abs(m[2]) <= 1e-4 * n * vmax, (m, n, vmax)
+    assert s.counters()["lost"] == 0
