@@ -321,7 +321,7 @@ class Scene:
 
     def conservation_metric(self, model: int = 0) -> np.ndarray:
         """The reference's conservation metric of one model (CollectConservationMetric,
-        include/mpm_algorithm.cuh:1252-1360, written per substep by Simulate,
+        include/mpm_algorithm.cuh:1082-1361, written per substep by Simulate,
         include/mpm_engine.cuh:573-603): rows Eulerian linear and angular
         momentum (left at zero, as the reference leaves them), Lagrangian linear
         momentum sum(v) and angular momentum sum(x cross v), per unit particle mass,
