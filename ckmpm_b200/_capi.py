@@ -34,6 +34,8 @@ MATERIAL_PARAMS = 8
 
 BOUNDARY_STICKY_BLOCKS = 0
 BOUNDARY_SLIP_FLOOR = 1
+BOUNDARY_FIELD = 2
+CELL_FREE, CELL_FIXED, CELL_SLIP, CELL_VELOCITY, CELL_SEPARATE = 0, 1, 2, 3, 4
 
 FLAG_TRACK_IDS = 1
 
@@ -47,6 +49,7 @@ EXPORTED = (
     "ckmpm_set_tuning", "ckmpm_get_tuning", "ckmpm_autotune", "ckmpm_checkpoint_bytes", "ckmpm_checkpoint_save",
     "ckmpm_checkpoint_restore", "ckmpm_diff_create", "ckmpm_diff_forward", "ckmpm_diff_backward", "ckmpm_diff_timing",
     "ckmpm_diff_last_error", "ckmpm_diff_destroy", "ckmpm_set_rigid", "ckmpm_set_rigid_velocity", "ckmpm_get_time",
+    "ckmpm_set_boundary_field",
 )
 
 MAX_BATCH_SCENES = 65536
@@ -117,6 +120,7 @@ def lib() -> C.CDLL:
         L.ckmpm_set_rigid.argtypes = [P, C.c_uint32, C.POINTER(C.c_float)]
         L.ckmpm_set_rigid_velocity.argtypes = [P, C.POINTER(C.c_float)]
         L.ckmpm_get_time.argtypes = [P, C.POINTER(C.c_double)]
+        L.ckmpm_set_boundary_field.argtypes = [P, C.POINTER(C.c_uint8), C.POINTER(C.c_float)]
         L.ckmpm_get_count.argtypes = [P, C.c_int32, u32p]
         L.ckmpm_get_state.argtypes = [P, C.c_int32, f32p, f32p, f32p, f32p, u32p, C.c_uint32, u32p]
         L.ckmpm_get_blocks.argtypes = [P, C.c_int32, C.c_int32, i32p, u32p, C.c_uint32, u32p]

@@ -280,7 +280,8 @@ ckmpm_status create_impl(const ckmpm_scene_desc* desc, uint32_t nstack, ckmpm_sc
       return fail(nullptr, CKMPM_ERR_INVALID, "domain_blocks out of range");
   const uint64_t nbd = static_cast<uint64_t>(desc->domain_blocks[0]) * desc->domain_blocks[1] * desc->domain_blocks[2];
   if (nbd * nstack > (1ull << 28)) return fail(nullptr, CKMPM_ERR_INVALID, "domain too large for the dense block table");
-  if (desc->boundary != CKMPM_BOUNDARY_STICKY_BLOCKS && desc->boundary != CKMPM_BOUNDARY_SLIP_FLOOR)
+  if (desc->boundary != CKMPM_BOUNDARY_STICKY_BLOCKS && desc->boundary != CKMPM_BOUNDARY_SLIP_FLOOR &&
+      desc->boundary != CKMPM_BOUNDARY_FIELD)
     return fail(nullptr, CKMPM_ERR_INVALID, "unknown boundary kind");
   if (desc->max_particles_per_block > static_cast<uint32_t>(kMaxParticlesPerBlock))
     return fail(nullptr, CKMPM_ERR_INVALID, "max_particles_per_block > 4096");
@@ -324,6 +325,19 @@ ckmpm_status create_impl(const ckmpm_scene_desc* desc, uint32_t nstack, ckmpm_sc
   }
   if (dalloc(s, &s->scal, 1) != cudaSuccess) return bail(fail(s, CKMPM_ERR_CUDA, "scalar allocation failed"));
   cudaMemsetAsync(s->scal, 0, sizeof(Scalars), s->stream);
+  if (desc->boundary == CKMPM_BOUNDARY_FIELD) {
+    // Per-cell rules (all FREE until ckmpm_set_boundary_field); a batch's
+    // scenes share the one field of their common domain extent.
+    const size_t cells = static_cast<size_t>(nbd) * 64;
+    uint8_t* rule = nullptr;
+    float* param = nullptr;
+    if (dalloc(s, &rule, cells) != cudaSuccess || dalloc(s, &param, 3 * cells) != cudaSuccess)
+      return bail(fail(s, CKMPM_ERR_CUDA, "boundary field allocation failed"));
+    cudaMemsetAsync(rule, 0, cells, s->stream);
+    cudaMemsetAsync(param, 0, sizeof(float) * 3 * cells, s->stream);
+    sc.brule = rule;
+    sc.bparam = param;
+  }
 
   if (set_fused_attributes<128>(&s->occ[0]) != cudaSuccess || set_fused_attributes<256>(&s->occ[1]) != cudaSuccess ||
       cudaFuncSetAttribute(reinterpret_cast<const void*>(rasterize_kernel<kFusedThreads>),
@@ -654,6 +668,31 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
   Scalars r{};
   CK_CUDA(s, cudaMemcpy(&r, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost));
   return status_from(s, r);
+}
+
+ckmpm_status ckmpm_set_boundary_field(ckmpm_scene* s, const uint8_t* rule, const float* param) {
+  if (!s || !rule) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  if (s->desc.boundary != CKMPM_BOUNDARY_FIELD || !s->sc.brule)
+    return fail(s, CKMPM_ERR_INVALID, "the scene's boundary kind is not CKMPM_BOUNDARY_FIELD");
+  const size_t cells = static_cast<size_t>(s->desc.domain_blocks[0]) * s->desc.domain_blocks[1] *
+                       s->desc.domain_blocks[2] * 64;
+  bool needs_param = false;
+  for (size_t c = 0; c < cells; ++c) {
+    if (rule[c] > CKMPM_CELL_SEPARATE) return fail(s, CKMPM_ERR_INVALID, "unknown cell rule");
+    needs_param |= rule[c] >= CKMPM_CELL_SLIP;
+  }
+  if (needs_param && !param) return fail(s, CKMPM_ERR_INVALID, "SLIP, VELOCITY and SEPARATE cells need param");
+  if (param)
+    for (size_t k = 0; k < 3 * cells; ++k)
+      if (!std::isfinite(param[k])) return fail(s, CKMPM_ERR_INVALID, "boundary parameters must be finite");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  // Stream-ordered: substeps already enqueued keep the old field.  Pageable
+  // sources are staged before the calls return.
+  CK_CUDA(s, cudaMemcpyAsync(const_cast<uint8_t*>(s->sc.brule), rule, cells, cudaMemcpyHostToDevice, s->stream));
+  if (param)
+    CK_CUDA(s, cudaMemcpyAsync(const_cast<float*>(s->sc.bparam), param, sizeof(float) * 3 * cells,
+                               cudaMemcpyHostToDevice, s->stream));
+  return CKMPM_OK;
 }
 
 ckmpm_status ckmpm_set_rigid(ckmpm_scene* s, uint32_t rigid_count, const float* velocity) {

@@ -63,6 +63,8 @@ struct SceneDev {
   uint32_t nblocks_domain;  // table entries over all stacked domains
   float grid_unit;       // single scene: mass of one fixed-point unit (heaviest model's mass x 2^-36)
   int32_t rigid;         // rigid particles on (the velocity is Scalars::rigid_v)
+  const uint8_t* brule;  // boundary == 2: per-cell rule (ckmpm_cell_rule), x-major over the domain's cells
+  const float* bparam;   // boundary == 2: per-cell normal or velocity, 3 floats per cell
 };
 
 // Per-scene material of a batch (one model per stacked domain).
@@ -202,7 +204,7 @@ __device__ __forceinline__ float4 node_velocity(const SceneDev& sc, const long l
   float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
   const float m = __ll2float_rn(__ldcg(blk + cell)) * unit;
   if (m > sc.mass_clamp) {
-    const float inv = 1.0f / m;
+    const float inv = __frcp_rn(m);  // IEEE-rounded 1/m, as the reference's invMass (the build approximates 1/x)
     v.x = __ll2float_rn(__ldcg(blk + 128 + cell)) * unit * inv;
     v.y = __ll2float_rn(__ldcg(blk + 256 + cell)) * unit * inv;
     v.z = __ll2float_rn(__ldcg(blk + 384 + cell)) * unit * inv;
@@ -211,6 +213,26 @@ __device__ __forceinline__ float4 node_velocity(const SceneDev& sc, const long l
       const bool out = (bx < 2 || bx + 2 >= sc.dims[0]) || (by < 2 || by + 2 >= sc.dims[1]) ||
                        (bz < 2 || bz + 2 >= sc.dims[2]);
       if (out) v = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else if (sc.boundary == 2) {
+      // Per-cell rule (the scene's irregular-boundary hook evaluated into data).
+      const int cx = bx * 4 + ((cell >> 4) & 3), cy = by * 4 + ((cell >> 2) & 3), cz = bz * 4 + (cell & 3);
+      const int64_t c = (static_cast<int64_t>(cx) * (sc.dims[1] * 4) + cy) * (sc.dims[2] * 4) + cz;
+      const int rule = sc.brule[c];
+      if (rule == 1) {
+        v = make_float4(0.f, 0.f, 0.f, 0.f);
+      } else if (rule >= 2 && rule <= 4) {
+        const float3 p = make_float3(__ldg(sc.bparam + 3 * c), __ldg(sc.bparam + 3 * c + 1), __ldg(sc.bparam + 3 * c + 2));
+        if (rule == 3) {
+          v = make_float4(p.x, p.y, p.z, 0.f);
+        } else {
+          const float d = p.x * v.x + p.y * v.y + p.z * v.z;
+          if (rule == 2 || d < 0.f) {
+            v.x -= d * p.x;
+            v.y -= d * p.y;
+            v.z -= d * p.z;
+          }
+        }
+      }
     } else {
       const bool out = (bx < 2 || bx + 2 >= sc.dims[0]) || (bz < 2 || bz + 2 >= sc.dims[2]) || (by + 2 >= sc.dims[1]);
       if (out) {

@@ -183,6 +183,10 @@ class MPMConfig:
     exist_rigid_particle: bool = False
     rigid_particle_count: int = 0
     rigid_particle_velocity: object = (0.0, 0.0, 0.0)
+    # boundary == "field": (rule, param) per grid cell, the irregular-boundary hook
+    # (GetExistIrregularBoundary / ProcessGridCellVelocity, include/mpm_config.h:108-117)
+    # evaluated into data; see ckmpm_b200.boundary.
+    boundary_field: object = None
 
     # MPMConfigBase getter names (include/mpm_config.h:17-123)
     def GetDx(self) -> float:
@@ -239,7 +243,8 @@ class MPMConfig:
             d.domain_blocks[i] = int(self.domain_blocks[i])
         d.gravity = self.gravity
         d.mass_clamp = self.mass_clamp
-        d.boundary = {"sticky_blocks": capi.BOUNDARY_STICKY_BLOCKS, "slip_floor": capi.BOUNDARY_SLIP_FLOOR}[self.boundary]
+        d.boundary = {"sticky_blocks": capi.BOUNDARY_STICKY_BLOCKS, "slip_floor": capi.BOUNDARY_SLIP_FLOOR,
+                      "field": capi.BOUNDARY_FIELD}[self.boundary]
         d.floor_cells = self.floor_cells
         d.max_particles_per_block = self.max_particles_per_block
         d.device = self.device
@@ -268,6 +273,17 @@ class Scene:
         self.models: list[MPMModel] = []
         if config.exist_rigid_particle:
             self.set_rigid(config.rigid_particle_count, config.GetRigidParticleVelocity(0))
+        if config.boundary == "field" and config.boundary_field is not None:
+            self.set_boundary_field(*config.boundary_field)
+
+    def set_boundary_field(self, rule, param=None) -> None:
+        """Per-cell boundary rules of a boundary="field" scene: rule (uint8, one per
+        cell, shape (Nx, Ny, Nz) or flat x-major) and param (3 floats per cell: the
+        normal of SLIP / SEPARATE cells, the velocity of VELOCITY cells)."""
+        r = np.ascontiguousarray(rule, np.uint8).ravel()
+        p = None if param is None else np.ascontiguousarray(param, np.float32).reshape(-1)
+        capi.check(capi.lib().ckmpm_set_boundary_field(self._h, r.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                                       capi.fptr(p)), "ckmpm_set_boundary_field", self._h)
 
     def set_rigid(self, count: int, velocity) -> None:
         """Rigid particles on (before setup): the first `count` particles of

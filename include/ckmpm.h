@@ -51,11 +51,28 @@ typedef enum ckmpm_material_kind {
  * (include/mpm_algorithm.cuh:765-768,802-805).  SLIP_FLOOR keeps sticky x/z
  * walls and ceiling, and clamps v_y >= 0 for cells below floor_cells (the
  * per-cell hook a scene installs through ProcessGridCellVelocity,
- * include/mpm_config.h:108-117). */
+ * include/mpm_config.h:108-117).  FIELD takes one rule per grid cell from
+ * ckmpm_set_boundary_field: the reference's irregular-boundary hook
+ * (GetExistIrregularBoundary / ProcessGridCellVelocity, include/mpm_algorithm.cuh:795-799)
+ * evaluated into data, so scene hooks such as slip walls, fixed regions or
+ * driven grips run without scene code on the device. */
 typedef enum ckmpm_boundary_kind {
   CKMPM_BOUNDARY_STICKY_BLOCKS = 0,
-  CKMPM_BOUNDARY_SLIP_FLOOR = 1
+  CKMPM_BOUNDARY_SLIP_FLOOR = 1,
+  CKMPM_BOUNDARY_FIELD = 2
 } ckmpm_boundary_kind;
+
+/* Per-cell rules of CKMPM_BOUNDARY_FIELD, applied to a grid node's velocity
+ * after gravity when its mass exceeds the clamp (both staggered grids of a cell
+ * take the cell's rule, as the reference's hook sees only the cell index).
+ * param is a unit normal n (SLIP, SEPARATE) or a velocity u (VELOCITY). */
+typedef enum ckmpm_cell_rule {
+  CKMPM_CELL_FREE = 0,      /* no constraint */
+  CKMPM_CELL_FIXED = 1,     /* v = 0 */
+  CKMPM_CELL_SLIP = 2,      /* v -= (n . v) n */
+  CKMPM_CELL_VELOCITY = 3,  /* v = u */
+  CKMPM_CELL_SEPARATE = 4   /* if n . v < 0: v -= (n . v) n */
+} ckmpm_cell_rule;
 
 /* Scene constants: the getters of MPMConfigBase (include/mpm_config.h:17-123)
  * and the block extent of MPMDomainRange (include/mpm_domain.h:17-30). */
@@ -140,6 +157,15 @@ ckmpm_status ckmpm_step_adaptive(ckmpm_scene* s, uint32_t nsteps, float dt_max, 
  * substeps enqueued after it (the reference evaluates its hook per frame). */
 ckmpm_status ckmpm_set_rigid(ckmpm_scene* s, uint32_t rigid_count, const float* velocity3);
 ckmpm_status ckmpm_set_rigid_velocity(ckmpm_scene* s, const float* velocity3);
+
+/* The per-cell boundary of a CKMPM_BOUNDARY_FIELD scene.  rule: one
+ * ckmpm_cell_rule byte per cell of the domain (4 * domain_blocks cells per
+ * axis, index (cx * Ny + cy) * Nz + cz); param: 3 floats per cell in the same
+ * order, or NULL when every rule is FREE or FIXED.  Host arrays.  Before
+ * ckmpm_setup, or later to change the boundary for the substeps enqueued after
+ * the call (the reference's hook also receives the frame index).  Not for a
+ * batch. */
+ckmpm_status ckmpm_set_boundary_field(ckmpm_scene* s, const uint8_t* rule, const float* param);
 
 /* Use a caller-provided cudaStream_t (passed as void*) for all work of this
  * scene; NULL selects the scene's own stream. */

@@ -131,6 +131,11 @@ struct MPMConfig {
   bool existRigidParticle = false;
   uint32_t rigidParticleCount = 0;
   std::function<Vector3(int)> rigidParticleVelocity = [](int) { return Vector3{0.f, 0.f, 0.f}; };
+  // boundary == CKMPM_BOUNDARY_FIELD: the irregular-boundary hook (GetExistIrregularBoundary /
+  // ProcessGridCellVelocity, include/mpm_config.h:108-117) as one ckmpm_cell_rule per cell
+  // (x-major over 4 * domainBlocks cells per axis) and 3 floats per cell.
+  std::vector<uint8_t> boundaryRule;
+  std::vector<float> boundaryParam;
 
   float GetDx() const { return dx; }
   float GetInvDx() const { return 1.f / dx; }
@@ -181,6 +186,10 @@ class MPMEngine {
       const Vector3 v = config.GetRigidParticleVelocity(0);
       check(ckmpm_set_rigid(scene_, config.GetRigidParticleCount(), v.data()), scene_, "ckmpm_set_rigid");
     }
+    if (config.boundary == CKMPM_BOUNDARY_FIELD && !config.boundaryRule.empty())
+      check(ckmpm_set_boundary_field(scene_, config.boundaryRule.data(),
+                                     config.boundaryParam.empty() ? nullptr : config.boundaryParam.data()),
+            scene_, "ckmpm_set_boundary_field");
   }
 
   // InitializeParticle: one engine model per MPMModel; dt shrinks by the CFL

@@ -46,8 +46,10 @@ struct SceneDesc {
   int32_t dims[3];       // domain extent in 4^3-cell blocks
   double gravity;        // acceleration on y
   double mass_clamp;     // grid nodes with m <= clamp get v = 0
-  int32_t boundary;      // 0: sticky blocks (reference default), 1: slip floor
+  int32_t boundary;      // 0: sticky blocks (reference default), 1: slip floor, 2: per-cell rules
   double floor_cells;    // slip floor height in cells (boundary == 1)
+  std::vector<uint8_t> rule;   // boundary == 2: rule per cell (0 free, 1 fixed, 2 slip, 3 velocity, 4 separate)
+  std::vector<double> param;   // boundary == 2: normal or velocity per cell (3 each)
 };
 
 struct GridBlock {
@@ -270,6 +272,23 @@ void node_velocity(const Scene& s, int gi, const int* c, double dt, double* v) {
     bool out = false;
     for (int a = 0; a < 3; ++a) out |= (K[a] < 2 || K[a] + 2 >= s.d.dims[a]);
     if (out) v[0] = v[1] = v[2] = 0.0;
+  } else if (s.d.boundary == 2) {
+    // Per-cell rules: the scene's irregular-boundary hook (mpm_algorithm.cuh:795-799)
+    // evaluated into data; both staggered grids of a cell take its rule.
+    const int64_t ci = (static_cast<int64_t>(c[0]) * (4 * s.d.dims[1]) + c[1]) * (4 * s.d.dims[2]) + c[2];
+    const int r = s.d.rule.empty() ? 0 : s.d.rule[ci];
+    if (r == 1) {
+      v[0] = v[1] = v[2] = 0.0;
+    } else if (r >= 2 && r <= 4) {
+      const double* p = &s.d.param[3 * ci];
+      if (r == 3) {
+        for (int k = 0; k < 3; ++k) v[k] = p[k];
+      } else {
+        const double d = p[0] * v[0] + p[1] * v[1] + p[2] * v[2];
+        if (r == 2 || d < 0.0)
+          for (int k = 0; k < 3; ++k) v[k] -= d * p[k];
+      }
+    }
   } else {
     // Slip floor: sticky walls on x, z and the ceiling, and v_y >= 0 below the floor.
     bool out = (K[0] < 2 || K[0] + 2 >= s.d.dims[0]) || (K[2] < 2 || K[2] + 2 >= s.d.dims[2]) ||
@@ -678,6 +697,18 @@ void* oracle_create(double dx, const int32_t* dims, double gravity, double mass_
 }
 
 void oracle_destroy(void* h) { delete static_cast<Scene*>(h); }
+
+// Per-cell boundary rules of a boundary-2 scene: rule[cells], param[3 cells]
+// (NULL: all zero), cells x-major over the domain's 4 * dims cells per axis.
+int oracle_set_boundary_field(void* h, const uint8_t* rule, const double* param) {
+  Scene* s = static_cast<Scene*>(h);
+  if (s->d.boundary != 2 || !rule) return -1;
+  const size_t cells = static_cast<size_t>(s->d.dims[0]) * s->d.dims[1] * s->d.dims[2] * 64;
+  s->d.rule.assign(rule, rule + cells);
+  s->d.param.assign(3 * cells, 0.0);
+  if (param) s->d.param.assign(param, param + 3 * cells);
+  return 0;
+}
 
 // kind: 0 fixed-corotated (params lambda, mu), 2 Drucker-Prager (lambda, mu),
 // 3 J-fluid (bulk, gamma, viscosity, J0).  v holds nv = 1 or n velocities.

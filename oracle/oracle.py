@@ -38,6 +38,7 @@ def lib() -> C.CDLL:
         L.oracle_set_lame.argtypes = [C.c_void_p, C.c_int, d, d]
         L.oracle_set_velocity.argtypes = [C.c_void_p, C.c_int, d, C.c_int]
         L.oracle_set_rigid.argtypes = [C.c_void_p, C.c_int, C.c_int, d]
+        L.oracle_set_boundary_field.argtypes = [C.c_void_p, C.POINTER(C.c_uint8), d]
         L.oracle_set_rigid_velocity.argtypes = [C.c_void_p, d]
         L.oracle_step.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.oracle_step_frame.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]
@@ -72,12 +73,20 @@ class OracleScene:
     def __init__(self, config, models=None):
         L = lib()
         dims = (C.c_int32 * 3)(*config.domain_blocks)
-        boundary = {"sticky_blocks": 0, "slip_floor": 1}[config.boundary]
+        boundary = {"sticky_blocks": 0, "slip_floor": 1, "field": 2}[config.boundary]
         self._h = C.c_void_p(L.oracle_create(config.dx, dims, config.gravity, config.mass_clamp, boundary,
                                              config.floor_cells))
         self.n = []
+        if config.boundary == "field" and getattr(config, "boundary_field", None) is not None:
+            self.set_boundary_field(*config.boundary_field)
         for m in models or []:
             self.add_model(m)
+
+    def set_boundary_field(self, rule, param=None) -> None:
+        """Per-cell boundary rules (x-major over the domain's cells) of a 'field' scene."""
+        r = np.ascontiguousarray(rule, np.uint8).ravel()
+        p = None if param is None else np.ascontiguousarray(param, np.float64).reshape(-1)
+        assert lib().oracle_set_boundary_field(self._h, r.ctypes.data_as(C.POINTER(C.c_uint8)), _d(p)) == 0
 
     def add_model(self, m) -> int:
         x = np.ascontiguousarray(m.particle_position, np.float32)

@@ -13,6 +13,10 @@
 //   CKMPM_HARNESS_SCENE_SAND  : dx = 1/256, 64^3 blocks, g = -9.8, slip floor at 8 cells
 //   CKMPM_HARNESS_SCENE_SLIP  : dx = 1/64,  16^3 blocks, g = -9.8, slip floor at 8 cells
 //   CKMPM_HARNESS_SCENE_DAM   : dx = 1/512, 128^3 blocks, g = -9.8, sticky walls
+//   CKMPM_HARNESS_SCENE_FIELD : the JELLY grid with an irregular-boundary hook: v = 0 in the cell
+//                               box [24,32) x [0,14) x [24,32), elsewhere the slip walls of
+//                               tests/fluid_with_two_longs (cells within 8 of a face lose the
+//                               velocity component along the normalised sum of the face normals)
 //   CKMPM_HARNESS_SCENE_RIGID : the JELLY grid with rigid particles on (GetExistRigidParticle):
 //                               the first 2048 particles of every von Mises model are rigid and
 //                               move with (2, 0.5 frame - 1, -1) in frame `frame` (every value
@@ -68,6 +72,11 @@ constexpr bool kRigid = true;
 #else
 constexpr bool kRigid = false;
 #endif
+#if defined(CKMPM_HARNESS_SCENE_FIELD)
+constexpr bool kField = true;
+#else
+constexpr bool kField = false;
+#endif
 constexpr uint32_t kRigidCount = 2048;
 constexpr float kGravity = -9.8f;
 constexpr float kFloorCells = 8.f;
@@ -111,10 +120,36 @@ class Config : public mpm::MPMConfigBase<Config> {
       -> mpm::Vector<Scalar, 3> {
     return mpm::Vector<Scalar, 3>{Scalar(2), Scalar(0.5) * Scalar(frame) - Scalar(1), Scalar(-1)};
   }
-  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetExistIrregularBoundaryImpl() const -> bool { return kSlipFloor; }
+  constexpr MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto GetExistIrregularBoundaryImpl() const -> bool {
+    return kSlipFloor || kField;
+  }
   MPM_FORCE_INLINE MPM_HOST_DEV_FUNC auto ProcessGridCellVelocityImpl(const mpm::Vector<int, 3>& cell,
                                                                       mpm::Vector<float, 3>& velocity, int) const
       -> void {
+    if (kField) {
+      const bool fixed = cell[0] >= 24 && cell[0] < 32 && cell[1] < 14 && cell[2] >= 24 && cell[2] < 32;
+      if (fixed) {
+        velocity[0] = velocity[1] = velocity[2] = 0.f;
+        return;
+      }
+      mpm::Vector<float, 3> n{0.f, 0.f, 0.f};
+      bool wall = false;
+      for (int a = 0; a < 3; ++a) {
+        if (cell[a] < 8) {
+          n[a] = 1.f;
+          wall = true;
+        } else if (cell[a] >= kBlocks * 4 - 8) {
+          n[a] = -1.f;
+          wall = true;
+        }
+      }
+      if (wall) {
+        n = n / n.Norm();
+        const float d = n.Dot(velocity);
+        velocity -= d * n;
+      }
+      return;
+    }
     const int bx = cell[0] / 4, by = cell[1] / 4, bz = cell[2] / 4;
     const bool wall = bx < 2 || bx + 2 >= kBlocks || bz < 2 || bz + 2 >= kBlocks || by + 2 >= kBlocks;
     if (wall) {

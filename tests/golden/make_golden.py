@@ -11,7 +11,9 @@ them), the largest nearest-neighbour distance between the two runs (the
 reference's own run-to-run spread, from its float atomics), and the inputs'
 checksum.  dt is a power of two and fps = 1 / (16 dt), so each frame is exactly
 16 substeps and the reference's frame clipping never changes dt; the first
-substep advects with dt = 0 as in the reference.  The rigid-particle fixture
+substep advects with dt = 0 as in the reference.  The fluid_walls fixture runs on
+the harness's FIELD family, whose irregular-boundary hook (slip walls and a
+fixed box of cells) the engine receives as a per-cell boundary field.  The rigid-particle fixture
 runs on the harness's RIGID family, whose scene hooks make the first 2048
 particles rigid with a per-frame velocity (rigid_velocity below).
 """
@@ -48,6 +50,17 @@ def golden_scenes():
     for kind in ("von_mises", "nacc", "linear"):
         cfg, m = scenes.material_cube(kind)
         yield kind, "jelly", cfg, m[0]
+    yield ("fluid_walls", "field") + wall_scene()
+
+
+def wall_scene():
+    """A J-fluid box thrown into the slip walls and over a fixed box of cells:
+    the harness's FIELD family hook, and the same rules as a boundary field."""
+    from ckmpm_b200.boundary import BoundaryField
+    cfg, m = scenes.fluid_box(lo=(0.13, 0.13, 0.3), hi=(0.45, 0.3, 0.55), v0=(-2.0, -3.0, 1.0))
+    cfg.boundary = "field"
+    cfg.boundary_field = BoundaryField(cfg).slip_walls(8).fixed_box((24, 0, 24), (32, 14, 32)).arrays()
+    return cfg, m[0]
 
 
 # Adaptive-dt fixture: the reference's own Simulate picks every dt (CFL on the

@@ -54,7 +54,7 @@ def test_header_compiles_as_c():
 def test_cpp_shim_compiles_with_every_material():
     """include/ckmpm/mpm_engine.hpp (the reference-shaped C++ API) builds with a
     plain host compiler, maps each MPMMaterial factory onto ckmpm_material and
-    carries the rigid-particle hooks."""
+    carries the rigid-particle and boundary hooks."""
     src = """#include "ckmpm/mpm_engine.hpp"
 int main() {
   using ckmpm::MPMMaterial;
@@ -68,6 +68,9 @@ int main() {
   cfg.rigidParticleCount = 16;
   cfg.rigidParticleVelocity = [](int frame) { return ckmpm::Vector3{1.f, 0.f, static_cast<float>(frame)}; };
   if (!cfg.GetExistRigidParticle() || cfg.GetRigidParticleVelocity(2)[2] != 2.f) return 1;
+  cfg.boundary = CKMPM_BOUNDARY_FIELD;  // the irregular-boundary hook as per-cell rules
+  cfg.boundaryRule.assign(64 * 64 * 64, static_cast<uint8_t>(CKMPM_CELL_SLIP));
+  cfg.boundaryParam.assign(3 * 64 * 64 * 64, 0.f);
   return all[5].c().p[6] == 1.f ? 0 : 1;
 }
 """
