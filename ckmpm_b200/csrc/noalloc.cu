@@ -65,16 +65,21 @@ cudaError_t na_base(int device, unsigned char** base, int* ctas) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    int sms = 0, occ = 0, occ2 = 0, occ3 = 0;
+    int sms = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, g2p2g_kernel<kFixedCorotated, kFusedThreads>, kFusedThreads,
-                                                  kSmemFused);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, g2p2g_kernel<kDruckerPrager, kFusedThreads>, kFusedThreads,
-                                                  kSmemFused);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, g2p2g_kernel<kFluid, kFusedThreads>, kFusedThreads,
-                                                  kSmemFused);
-    g_na_ctas[device] = std::max(1, std::min(occ, std::min(occ2, occ3))) * sms;
+    const void* fns[5] = {reinterpret_cast<const void*>(g2p2g_kernel<kFixedCorotated, kFusedThreads>),
+                          reinterpret_cast<const void*>(g2p2g_kernel<kDruckerPrager, kFusedThreads>),
+                          reinterpret_cast<const void*>(g2p2g_kernel<kFluid, kFusedThreads>),
+                          reinterpret_cast<const void*>(g2p2g_kernel<kVonMises, kFusedThreads>),
+                          reinterpret_cast<const void*>(g2p2g_kernel<kNacc, kFusedThreads>)};
+    int lowest = 1 << 30;
+    for (const void* fn : fns) {
+      int occ = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kFusedThreads, kSmemFused);
+      lowest = std::min(lowest, occ);
+    }
+    g_na_ctas[device] = std::max(1, lowest) * sms;
     g_na_base[device] = static_cast<unsigned char*>(p);
   }
   *base = g_na_base[device];
@@ -155,8 +160,8 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   if (desc->max_particles_per_block > static_cast<uint32_t>(kMaxParticlesPerBlock))
     return na_fail(message, CKMPM_ERR_INVALID, "max_particles_per_block > 4096");
   if (material->kind != CKMPM_FIXED_COROTATED && material->kind != CKMPM_DRUCKER_PRAGER &&
-      material->kind != CKMPM_FLUID)
-    return na_fail(message, CKMPM_ERR_INVALID, "unsupported material kind");
+      material->kind != CKMPM_FLUID && material->kind != CKMPM_VON_MISES && material->kind != CKMPM_NACC)
+    return na_fail(message, CKMPM_ERR_INVALID, "unsupported material kind (the linear model keeps a stored stress)");
   if (!(mass > 0.f) || !(volume > 0.f)) return na_fail(message, CKMPM_ERR_INVALID, "mass and volume must be positive");
   if (!(dt >= 0.f)) return na_fail(message, CKMPM_ERR_INVALID, "dt must be non-negative");
 
@@ -281,7 +286,9 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   NA_CUDA(cudaMemcpyAsync(&counts[1], d.bl[0].nparticles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   NA_CUDA(cudaStreamSynchronize(st));
   const uint32_t n_valid = counts[1];
-  const float aux0 = material->kind == CKMPM_FLUID ? material->p[3] : 0.f;
+  const float aux0 = material->kind == CKMPM_FLUID ? material->p[3]
+                     : material->kind == CKMPM_NACC ? material->p[2]
+                     : material->kind == CKMPM_VON_MISES ? 1.f : 0.f;
   if (n_valid > 0)
     setup_gather_kernel<<<(n_valid + 255) / 256, 256, 0, st>>>(d, 1, n_valid, sort_vals_out, x, v, nv, aux0, 0u);
   NA_CUDA(cudaMemcpyAsync(d.bl[1].table, d.bl[0].table, sizeof(int32_t) * nbd, cudaMemcpyDeviceToDevice, st));
@@ -313,6 +320,12 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
         break;
       case CKMPM_DRUCKER_PRAGER:
         g2p2g_kernel<kDruckerPrager, kFusedThreads><<<ctas, kFusedThreads, kSmemFused, st>>>(sc, d, grid, scal);
+        break;
+      case CKMPM_VON_MISES:
+        g2p2g_kernel<kVonMises, kFusedThreads><<<ctas, kFusedThreads, kSmemFused, st>>>(sc, d, grid, scal);
+        break;
+      case CKMPM_NACC:
+        g2p2g_kernel<kNacc, kFusedThreads><<<ctas, kFusedThreads, kSmemFused, st>>>(sc, d, grid, scal);
         break;
       default:
         g2p2g_kernel<kFluid, kFusedThreads><<<ctas, kFusedThreads, kSmemFused, st>>>(sc, d, grid, scal);

@@ -238,8 +238,10 @@ ckmpm_status ckmpm_debug_constitutive(const ckmpm_material* material, uint32_t n
  * first call before any stream capture.  x, v (nv = 1 or n float3) and the
  * outputs x_out, v_out (3n), F_out (9n), aux_out (n) are DEVICE pointers in
  * input order (outputs may be NULL; particles lost at the domain edge read
- * NaN).  Every call reuses the same array and clears what it needs: calls that
- * overlap on the GPU race.  *message (may be NULL) receives a static string. */
+ * NaN).  Materials: every kind but the linear model (which keeps a stored
+ * stress); boundary kinds STICKY_BLOCKS and SLIP_FLOOR.  Every call reuses the
+ * same array and clears what it needs: calls that overlap on the GPU race.
+ * *message (may be NULL) receives a static string. */
 ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, const ckmpm_material* material, uint32_t n,
                                     const float* x, const float* v, uint32_t nv, float mass, float volume,
                                     uint32_t nsteps, float dt, void* cuda_stream, float* x_out, float* v_out,

@@ -75,6 +75,30 @@ def test_noalloc_matches_allocating_path_twice(engine_lib):
             assert used < (1 << 20), used
 
 
+@pytest.mark.parametrize("kind", ["von_mises", "nacc"])
+def test_noalloc_other_materials(engine_lib, kind):
+    """The von Mises and NACC cubes through the allocation-free entry point, against the
+    allocating path (NACC compared through F F^T, its F being fixed only up to a rotation)."""
+    torch = pytest.importorskip("torch")
+    cfg, models = scenes.material_cube(kind)
+    nsteps, dt = 24, 1e-4
+    s = Scene(cfg)
+    s.add_model(models[0])
+    s.setup()
+    s.step(nsteps, dt)
+    ref = s.state(0)
+    s.close()
+    code, msg, nlive, xo, vo, Fo, used = _noalloc(engine_lib, cfg, models[0], nsteps, dt, torch)
+    assert code == capi.CKMPM_OK, msg
+    assert nlive == len(ref.id)
+    assert np.abs(xo[ref.id] - ref.x).max() <= X_TOL
+    Fa, Fb = Fo[ref.id].astype(np.float64), ref.F.astype(np.float64)
+    if kind == "nacc":
+        Fa, Fb = Fa @ Fa.transpose(0, 2, 1), Fb @ Fb.transpose(0, 2, 1)
+    assert np.abs(Fa - Fb).max() <= F_TOL
+    assert np.abs(vo[ref.id] - ref.v).max() <= V_REL * float(np.abs(ref.v).max()) + 1e-6
+
+
 def test_noalloc_rejects_sizes_beyond_its_limits(engine_lib):
     torch = pytest.importorskip("torch")
     cfg, models = scenes.jelly_cube(lo=(0.44, 0.44, 0.44), hi=(0.56, 0.56, 0.56))
