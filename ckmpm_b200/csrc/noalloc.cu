@@ -245,7 +245,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   d.max_per_block = desc->max_particles_per_block ? desc->max_particles_per_block : kMaxParticlesPerBlock;
   d.track_ids = 1;
   d.mat.kind = material->kind;
-  for (int k = 0; k < 4; ++k) d.mat.p[k] = material->p[k];
+  for (int k = 0; k < kMaterialParams; ++k) d.mat.p[k] = material->p[k];
   d.mass = mass;
   d.vol = volume;
   d.flush_ratio = 1.0;
