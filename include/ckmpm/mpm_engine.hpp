@@ -244,6 +244,60 @@ class MPMEngine {
     return x;
   }
 
+  // Full per-particle state of a model in input order when ids are tracked:
+  // x, v (the velocity the next G2P interpolates), F (row-major 3x3) and aux
+  // (J, logJp or the rigid flag), as ckmpm_get_state returns them.
+  struct ParticleState {
+    std::vector<Vector3> x, v;
+    std::vector<std::array<float, 9>> F;
+    std::vector<float> aux;
+  };
+  ParticleState GetParticleState(int32_t model) {
+    uint32_t n = 0;
+    check(ckmpm_get_count(scene_, model, &n), scene_, "ckmpm_get_count");
+    ParticleState st;
+    st.x.resize(n);
+    st.v.resize(n);
+    st.F.resize(n);
+    st.aux.resize(n);
+    uint32_t out = 0;
+    if (n)
+      check(ckmpm_get_state(scene_, model, st.x[0].data(), st.v[0].data(), st.F[0].data(), st.aux.data(), nullptr, n,
+                            &out),
+            scene_, "ckmpm_get_state");
+    return st;
+  }
+
+  // The reference's conservation metric of one model (CollectConservationMetric,
+  // include/mpm_algorithm.cuh:1082-1361): rows Eulerian linear and angular
+  // momentum (zero, as the reference leaves them), Lagrangian sum(v) and
+  // sum(x cross v), per unit particle mass, summed in double.
+  std::array<Vector3, 4> GetConservationMetric(int32_t model) {
+    const ParticleState st = GetParticleState(model);
+    double l[3] = {0, 0, 0}, a[3] = {0, 0, 0};
+    for (size_t i = 0; i < st.x.size(); ++i) {
+      const auto& x = st.x[i];
+      const auto& v = st.v[i];
+      for (int k = 0; k < 3; ++k) l[k] += v[k];
+      a[0] += static_cast<double>(x[1]) * v[2] - static_cast<double>(x[2]) * v[1];
+      a[1] += static_cast<double>(x[2]) * v[0] - static_cast<double>(x[0]) * v[2];
+      a[2] += static_cast<double>(x[0]) * v[1] - static_cast<double>(x[1]) * v[0];
+    }
+    std::array<Vector3, 4> m{};
+    for (int k = 0; k < 3; ++k) {
+      m[2][k] = static_cast<float>(l[k]);
+      m[3][k] = static_cast<float>(a[k]);
+    }
+    return m;
+  }
+
+  // Simulated time (double) and the end of the current adaptive frame.
+  std::array<double, 2> GetTime() {
+    std::array<double, 2> t{};
+    check(ckmpm_get_time(scene_, t.data()), scene_, "ckmpm_get_time");
+    return t;
+  }
+
   float GetDt() const { return dt_; }
   ckmpm_scene* Handle() { return scene_; }
 

@@ -54,9 +54,16 @@ int main(int argc, char** argv) {
     simulator.InitializeParticle(config, models);
     simulator.InitialSetup(config);
     std::vector<ckmpm::Vector3> last;
+    std::array<ckmpm::Vector3, 4> metric{};
     simulator.Simulate(config, [&](uint32_t frame, ckmpm::MPMEngine& e) {
-      if (frame + 1 == frames) last = e.GetParticlePosition(0);
+      if (frame + 1 == frames) {
+        last = e.GetParticlePosition(0);
+        metric = e.GetConservationMetric(0);
+      }
     });
+    // The Lagrangian momentum of the last frame on stderr, for the test to compare.
+    std::fprintf(stderr, "metric %.9g %.9g %.9g %.9g %.9g %.9g\n", metric[2][0], metric[2][1], metric[2][2],
+                 metric[3][0], metric[3][1], metric[3][2]);
     std::ofstream out(argv[2], std::ios::binary);
     out.write(reinterpret_cast<const char*>(last.data()), static_cast<std::streamsize>(last.size() * 12));
   } catch (const ckmpm::Error& err) {

@@ -49,7 +49,7 @@ def python_run(model, rigid: int) -> np.ndarray:
     eng.InitializeParticle(cfg, [model])
     eng.InitialSetup(cfg)
     eng.Simulate(cfg, export_callback=lambda f, scene: frames.__setitem__(f, scene.state(0).x.copy()))
-    return frames[FRAMES - 1]
+    return frames[FRAMES - 1], eng.scene.conservation_metric(0)
 
 
 @pytest.mark.parametrize("rigid", [0, 1500])
@@ -67,6 +67,9 @@ def test_cpp_scene_matches_python_engine(scene_binary, tmp_path, rigid):
                           f"{lam:.9g}", f"{mu:.9g}", str(FRAMES), str(rigid)], capture_output=True, text=True)
     assert res.returncode == 0, res.stderr
     cpp = np.fromfile(of, np.float32).reshape(-1, 3)
-    py = python_run(model, rigid)
+    py, metric = python_run(model, rigid)
     assert cpp.shape == py.shape
     assert np.array_equal(cpp, py), np.abs(cpp - py).max()
+    line = [ln for ln in res.stderr.splitlines() if ln.startswith("metric ")][0]
+    cpp_metric = np.array([float(t) for t in line.split()[1:]]).reshape(2, 3)
+    np.testing.assert_allclose(cpp_metric, metric[2:].astype(np.float32), rtol=1e-6, atol=1e-6)
