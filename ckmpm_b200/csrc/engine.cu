@@ -66,7 +66,7 @@ struct ckmpm_scene {
   std::string err;
   int sm_count = 0;
   int fused_ctas = 0;
-  int occ[2] = {0, 0};     // resident fused CTAs per SM at 128 / 256 threads
+  int occ[3] = {0, 0, 0};  // resident fused CTAs per SM at 128 / 256 / 1024 threads
   uint32_t nstack = 1;     // stacked domains: 1, or the scene count of a batch
   ckmpm_tuning tune{};
   // Every device allocation with its size; the first n_state_allocs hold the
@@ -136,8 +136,15 @@ cudaError_t launch_fused_nt(ckmpm_scene* s, const ModelHost& m) {
 }
 
 cudaError_t launch_fused_any(ckmpm_scene* s, const ModelHost& m) {
-  return s->tune.threads == 128 ? launch_fused_nt<128>(s, m) : launch_fused_nt<256>(s, m);
+  switch (s->tune.threads) {
+    case 128: return launch_fused_nt<128>(s, m);
+    case 1024: return launch_fused_nt<1024>(s, m);
+    default: return launch_fused_nt<256>(s, m);
+  }
 }
+
+// Index of a CTA size in ckmpm_scene::occ (-1 for a size that has no kernel).
+int shape_index(uint32_t threads) { return threads == 128 ? 0 : threads == 256 ? 1 : threads == 1024 ? 2 : -1; }
 
 template <int NT>
 cudaError_t set_fused_attributes(int* occ) {
@@ -340,6 +347,7 @@ ckmpm_status create_impl(const ckmpm_scene_desc* desc, uint32_t nstack, ckmpm_sc
   }
 
   if (set_fused_attributes<128>(&s->occ[0]) != cudaSuccess || set_fused_attributes<256>(&s->occ[1]) != cudaSuccess ||
+      set_fused_attributes<1024>(&s->occ[2]) != cudaSuccess ||
       cudaFuncSetAttribute(reinterpret_cast<const void*>(rasterize_kernel<kFusedThreads>),
                            cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemFused)) != cudaSuccess)
     return bail(fail(s, CKMPM_ERR_CUDA, "cudaFuncSetAttribute failed"));
@@ -355,8 +363,8 @@ ckmpm_status create_impl(const ckmpm_scene_desc* desc, uint32_t nstack, ckmpm_sc
 }
 
 ckmpm_status apply_tuning(ckmpm_scene* s, const ckmpm_tuning& t) {
-  if (t.threads != 128 && t.threads != 256) return fail(s, CKMPM_ERR_INVALID, "threads must be 128 or 256");
-  const int occ = s->occ[t.threads == 128 ? 0 : 1];
+  if (shape_index(t.threads) < 0) return fail(s, CKMPM_ERR_INVALID, "threads must be 128, 256 or 1024");
+  const int occ = s->occ[shape_index(t.threads)];
   if (t.ctas_per_sm < 1 || t.ctas_per_sm > static_cast<uint32_t>(occ))
     return fail(s, CKMPM_ERR_INVALID, "ctas_per_sm must be between 1 and the kernel's occupancy");
   if (t.graph_chunk < 2 || t.graph_chunk > kMaxGraphChunk || (t.graph_chunk & 1))
@@ -959,8 +967,8 @@ ckmpm_status ckmpm_autotune(ckmpm_scene* s, uint32_t probe_steps, float dt, ckmp
   CK_CUDA(s, checkpoint_copy(s, static_cast<unsigned char*>(saved), true));
   const ckmpm_tuning before = s->tune;
   std::vector<ckmpm_tuning> cands;
-  for (uint32_t nt : {256u, 128u}) {
-    const int occ = s->occ[nt == 128 ? 0 : 1];
+  for (uint32_t nt : {256u, 128u, 1024u}) {
+    const int occ = s->occ[shape_index(nt)];
     for (int c = occ; c >= 1; --c)
       for (uint32_t chunk : {8u, 32u}) cands.push_back(ckmpm_tuning{nt, static_cast<uint32_t>(c), chunk, 0.f});
   }

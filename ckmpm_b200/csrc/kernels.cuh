@@ -616,7 +616,6 @@ __device__ __forceinline__ uint32_t o_slot(uint32_t start, uint32_t q) { return 
 
 struct SharedSmall {
   int64_t blk[8];
-  uint32_t wcnt[8][28];
   uint32_t item;
   uint32_t off[28];
   uint32_t idx[27];
@@ -640,19 +639,28 @@ constexpr size_t kSmemFused = kSmemVTile + kSmemPTile + kSmemCodes;
 // compiles the rigid-particle test in (scenes with rigid particles on; the
 // test alone cost 1.7 % on the sand column).  Register
 // budget: 64 per thread at 256 threads (4 CTAs per SM); at 128 threads the
-// shared-memory footprint allows 5 CTAs per SM, so up to 102 registers.
+// shared-memory footprint allows 5 CTAs per SM, so up to 102 registers; at
+// 1024 threads one CTA fills the SM (for small scenes, where a few hundred
+// blocks cannot fill 148 SMs and the fullest block sets the launch's length).
 template <int NT>
 constexpr int fused_min_ctas() { return NT == 128 ? 5 : 1024 / NT; }
+
+// Per-warp direction counts of the rebin ranking.
+template <int NT>
+struct RankCounts {
+  uint32_t wcnt[NT / 32][28];
+};
 
 template <int KIND, int NT, bool RIGID = false>
 __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
     g2p2g_kernel(SceneDev sc, ModelDev md, GridDev gd, Scalars* __restrict__ scal) {
-  static_assert(NT % 32 == 0 && NT / 32 <= 8 && NT >= 64, "block size");
+  static_assert(NT % 32 == 0 && NT / 32 <= 32 && NT >= 64, "block size");
   extern __shared__ __align__(16) unsigned char smem[];
   float4* vtile = reinterpret_cast<float4*>(smem);
   unsigned* ptile = reinterpret_cast<unsigned*>(smem + kSmemVTile);
   uint8_t* dcode = smem + kSmemVTile + kSmemPTile;
   __shared__ SharedSmall sh;
+  __shared__ RankCounts<NT> rk;
 
   const int32_t step = scal->step;
   const int parity = step & 1;
@@ -696,8 +704,8 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
       incoming_groups(sc, prev, key, sh.off, sh.idx, sh.src);
     else if (threadIdx.x < 40)
       window_blocks(sc, stin, read_epoch, key, sh.blk, threadIdx.x - 32);
-    for (int i = threadIdx.x; i < static_cast<int>(sizeof(sh.wcnt) / sizeof(uint32_t)); i += NT)
-      (&sh.wcnt[0][0])[i] = 0u;
+    for (int i = threadIdx.x; i < static_cast<int>(sizeof(rk.wcnt) / sizeof(uint32_t)); i += NT)
+      (&rk.wcnt[0][0])[i] = 0u;
     for (int i = threadIdx.x; i < 2 * kTilePlane / 4; i += NT)
       reinterpret_cast<uint4*>(ptile)[i] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
@@ -869,7 +877,7 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
         const uint32_t q = b + lane;
         const int code = q < q1 ? dcode[q] : 255;
         const uint32_t mask = __match_any_sync(0xffffffffu, code);
-        if (code < 28 && lane == 31 - __clz(mask)) sh.wcnt[wid][code] += __popc(mask);
+        if (code < 28 && lane == 31 - __clz(mask)) rk.wcnt[wid][code] += __popc(mask);
         __syncwarp();
       }
       __syncthreads();
@@ -878,8 +886,8 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
         if (lane < 28) {
 #pragma unroll
           for (int w = 0; w < kWarps; ++w) {
-            const uint32_t t = sh.wcnt[w][lane];
-            sh.wcnt[w][lane] = c;
+            const uint32_t t = rk.wcnt[w][lane];
+            rk.wcnt[w][lane] = c;
             c += t;
           }
         }
@@ -893,7 +901,7 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
         if (lane < 27) {
           const uint32_t pre = incl - cv;
 #pragma unroll
-          for (int w = 0; w < kWarps; ++w) sh.wcnt[w][lane] += pre;
+          for (int w = 0; w < kWarps; ++w) rk.wcnt[w][lane] += pre;
           cur.prefix28[item * 28 + lane] = pre;
           if (c > 0) {
             const int x = key.x - (lane / 9 - 1), y = key.y - ((lane / 3) % 3 - 1), z = key.z - (lane % 3 - 1);
@@ -909,11 +917,11 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
         const int code = q < q1 ? dcode[q] : 255;
         const uint32_t mask = __match_any_sync(0xffffffffu, code);
         if (code < 27) {
-          const uint32_t r = sh.wcnt[wid][code] + __popc(mask & lt);
+          const uint32_t r = rk.wcnt[wid][code] + __popc(mask & lt);
           if (start + r < md.cap_particles) cur.idx[start + r] = static_cast<uint16_t>(q);
         }
         __syncwarp();
-        if (code < 27 && lane == 31 - __clz(mask)) sh.wcnt[wid][code] += __popc(mask);
+        if (code < 27 && lane == 31 - __clz(mask)) rk.wcnt[wid][code] += __popc(mask);
         __syncwarp();
       }
     }

@@ -283,7 +283,7 @@ ckmpm_status ckmpm_get_blocks_in(ckmpm_scene* s, uint32_t scene, int32_t model, 
  * not depend on it: the P2G tile and the grid hold exact integer sums, so the
  * order in which blocks deposit never changes a bit. */
 typedef struct ckmpm_tuning {
-  uint32_t threads;      /* CTA size: 128 or 256 */
+  uint32_t threads;      /* CTA size: 128, 256 or 1024 (one CTA per SM; for small scenes) */
   uint32_t ctas_per_sm;  /* resident persistent CTAs per SM, 1..occupancy */
   uint32_t graph_chunk;  /* substeps per captured CUDA graph, even, 2..64 */
   float probe_ms;        /* ckmpm_autotune: measured ms per substep; 0 otherwise */
@@ -291,7 +291,8 @@ typedef struct ckmpm_tuning {
 
 ckmpm_status ckmpm_set_tuning(ckmpm_scene* s, const ckmpm_tuning* t);
 
-/* max_ctas_per_sm2 (may be NULL): occupancy limit at 128 and 256 threads. */
+/* max_ctas_per_sm2 (may be NULL): occupancy limit at 128 and 256 threads (at
+ * 1024 threads it is 1). */
 ckmpm_status ckmpm_get_tuning(ckmpm_scene* s, ckmpm_tuning* t, uint32_t* max_ctas_per_sm2);
 
 /* Autotuner: times probe_steps substeps (rounded up to whole graphs) of this
