@@ -662,13 +662,10 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     CK_CUDA(s, cudaMemsetAsync(m.dev.ticket, 0, sizeof(uint32_t), s->stream));
   }
   CK_CUDA(s, launch_zero(s, 0, 1, 1));
-  Scalars h{};
-  h.step = 0;
-  h.cur_dt = 0.f;
-  h.next_dt = 0.f;
-  h.lost = lost_at_setup;
-  for (int a = 0; a < 3; ++a) h.rigid_v[a] = s->rigid_v[a];
-  CK_CUDA(s, cudaMemcpyAsync(s->scal, &h, sizeof(Scalars), cudaMemcpyHostToDevice, s->stream));
+  // The scalars were zeroed at creation; setup's kernels may have raised status
+  // bits in them, which ckmpm_setup then reports.
+  finish_setup_kernel<<<1, 32, 0, s->stream>>>(s->scal, lost_at_setup, s->rigid_v[0], s->rigid_v[1], s->rigid_v[2]);
+  CK_CUDA(s, cudaGetLastError());
   CK_CUDA(s, cudaStreamSynchronize(s->stream));
   s->setup_done = true;
   s->host_step = 0;

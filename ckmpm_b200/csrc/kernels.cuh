@@ -1151,6 +1151,18 @@ __global__ void __launch_bounds__(kCompactThreads)
 
 // Advance the substep counter and roll the dt pair: currentDt = nextDt, then
 // the clock advances by it (include/mpm_engine.cuh:869-871).
+// End of setup: the particles dropped while binning and the rigid velocity.
+// The other fields keep what setup's kernels left (zero, and any status bits
+// they raised: a non-finite initial velocity, a full block).
+__global__ void finish_setup_kernel(Scalars* scal, uint32_t lost, float rx, float ry, float rz) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    scal->lost += lost;
+    scal->rigid_v[0] = rx;
+    scal->rigid_v[1] = ry;
+    scal->rigid_v[2] = rz;
+  }
+}
+
 __global__ void end_substep_kernel(Scalars* scal) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     scal->step += 1;

@@ -305,9 +305,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   rasterize_kernel<kFusedThreads><<<ctas, kFusedThreads, kSmemFused, st>>>(sc, d, grid, scal);
   NA_CUDA(cudaMemsetAsync(d.ticket, 0, sizeof(uint32_t), st));
   zero_windows_kernel<<<sms * 4, 256, 0, st>>>(sc, d.bl[0], grid.grid[1], grid.stamp[1], scal, 1);
-  Scalars h{};
-  h.lost = n - n_valid;
-  NA_CUDA(cudaMemcpyAsync(scal, &h, sizeof(Scalars), cudaMemcpyHostToDevice, st));
+  finish_setup_kernel<<<1, 32, 0, st>>>(scal, n - n_valid, 0.f, 0.f, 0.f);  // keeps setup's status bits
   NA_CUDA(cudaGetLastError());
 
   // Substeps: the launch sequence of ckmpm_step without graphs.

@@ -432,3 +432,26 @@ def test_boundary_field_api(engine_lib):
     s.setup()
     s.step(4, 1e-4)
     assert s.counters()["status"] == 0
+
+
+def test_non_finite_inputs(engine_lib):
+    """A non-finite or out-of-range initial velocity is an error status from
+    ckmpm_setup (the reference stops when the grid velocity turns infinite,
+    include/mpm_engine.cuh:545-549); a non-finite position drops the particle
+    at binning and counts it as lost."""
+    cfg, models = scenes.jelly_cube(lo=(0.44, 0.44, 0.44), hi=(0.56, 0.56, 0.56))
+    m = models[0]
+    for bad in (np.nan, np.inf, 1e6):
+        v = np.repeat(np.asarray([[0.0, -1.0, 0.0]], np.float32), len(m.particle_position), 0)
+        v[17, 1] = bad
+        s = Scene(cfg)
+        s.add_model(MPMModel(m.particle_mass, m.particle_volume, m.particle_position, v, m.material))
+        with pytest.raises(capi.CkmpmError, match="NUMERIC"):
+            s.setup()
+    x = m.particle_position.copy()
+    x[5, 0] = np.nan
+    s = Scene(cfg)
+    s.add_model(MPMModel(m.particle_mass, m.particle_volume, x, m.particle_velocity, m.material))
+    s.setup()
+    s.step(4, 1e-4)
+    assert s.counters()["lost"] == 1 and s.count(0) == len(x) - 1
