@@ -87,6 +87,8 @@ class SceneBatch(Scene):
             else np.repeat(m.particle_velocity, len(m.particle_position), 0) for m in scenes]), np.float32)
         capi.check(L.ckmpm_add_batch(self._h, len(scenes), arr, capi.fptr(x), capi.fptr(v)), "ckmpm_add_batch",
                    self._h)
+        if config.boundary == "field" and config.boundary_field is not None:
+            self.set_boundary_field(*config.boundary_field)  # one field, shared by every scene of the batch
 
     @property
     def n_scenes(self) -> int:

@@ -163,8 +163,8 @@ ckmpm_status ckmpm_set_rigid_velocity(ckmpm_scene* s, const float* velocity3);
  * axis, index (cx * Ny + cy) * Nz + cz); param: 3 floats per cell in the same
  * order, or NULL when every rule is FREE or FIXED.  Host arrays.  Before
  * ckmpm_setup, or later to change the boundary for the substeps enqueued after
- * the call (the reference's hook also receives the frame index).  Not for a
- * batch. */
+ * the call (the reference's hook also receives the frame index).  The scenes
+ * of a batch share one field. */
 ckmpm_status ckmpm_set_boundary_field(ckmpm_scene* s, const uint8_t* rule, const float* param);
 
 /* Use a caller-provided cudaStream_t (passed as void*) for all work of this

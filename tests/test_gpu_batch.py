@@ -179,3 +179,18 @@ def test_batch_with_every_material_equals_scenes_alone(engine_lib):
         alone.close()
     assert {"von_mises", "nacc", "linear"} <= kinds
     assert b.counters()["status"] == 0
+
+
+def test_batch_shares_a_boundary_field(engine_lib):
+    """A batch of boundary="field" scenes shares one per-cell field (slip walls
+    and a fixed box); each scene comes out bitwise as it does alone with it."""
+    from ckmpm_b200.boundary import BoundaryField
+    cfg, models = small_batch(n=4, seed=13)
+    cfg.boundary = "field"
+    cfg.boundary_field = BoundaryField(cfg).slip_walls(8).fixed_box((20, 0, 20), (44, 12, 44)).arrays()
+    b = run_batch(cfg, models, 16)
+    st = b.state()
+    for i, m in enumerate(models):
+        alone = run_alone(cfg, m, 16)
+        assert_same_state(b.scene_state(i, st), alone.state(0), f"scene {i}")
+        alone.close()
