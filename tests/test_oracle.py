@@ -241,3 +241,61 @@ def test_rigid_particles(oracle_mod):
     o.set_rigid_velocity(-vr)
     o.step(3, dt)
     np.testing.assert_allclose(o.state(0)["x"][:R] - st["x"][:R], np.tile(-3 * dt * vr, (R, 1)), rtol=0, atol=1e-12)
+
+
+def _field_cube(rule_kind, param=None, v0=(1.0, -0.5, 0.25)):
+    """Cube in a boundary field whose every cell carries one rule (oracle)."""
+    from ckmpm_b200.boundary import BoundaryField
+    cfg, models = scenes.jelly_cube(lo=(0.45, 0.45, 0.45), hi=(0.55, 0.55, 0.55), v0=v0, gravity=0.0)
+    cfg.boundary = "field"
+    bf = BoundaryField(cfg)
+    bf.rule[...] = rule_kind
+    if param is not None:
+        bf.param[...] = np.asarray(param, np.float32)
+    cfg.boundary_field = bf.arrays()
+    return cfg, models
+
+
+def test_boundary_field_rules(oracle_mod):
+    """The per-cell rules of a boundary field (the reference's irregular-boundary
+    hook as data, mpm_algorithm.cuh:795-799), one rule over the whole domain:
+    the velocity the next G2P reads is the rule applied to the free velocity."""
+    v0 = np.array([1.0, -0.5, 0.25])
+    n = np.array([0.0, 0.6, 0.8])  # a unit normal
+    u = np.array([0.3, 0.2, -0.1])
+    expect = {
+        0: v0,                            # free
+        1: np.zeros(3),                   # fixed
+        2: v0 - (n @ v0) * n,             # slip
+        3: u,                             # prescribed velocity
+        4: v0 if n @ v0 >= 0 else v0 - (n @ v0) * n,  # separate: n . v = -0.1 < 0, so projected
+    }
+    for kind, want in expect.items():
+        param = u if kind == 3 else n
+        cfg, models = _field_cube(kind, param)
+        o = oracle_mod.OracleScene(cfg, models)
+        o.setup()
+        v = o.state(0)["v"]
+        np.testing.assert_allclose(v, np.tile(want, (len(v), 1)), atol=1e-9, err_msg=f"rule {kind}")
+
+
+def test_boundary_field_helpers():
+    """BoundaryField builds the reference scenes' hook rules: slip walls with the
+    normalised sum of face normals, fixed and rotating boxes, a one-sided floor."""
+    from ckmpm_b200.boundary import FIXED, SEPARATE, SLIP, VELOCITY, BoundaryField
+    cfg, _ = scenes.jelly_cube()
+    bf = BoundaryField(cfg).slip_walls(8)
+    assert bf.shape == (64, 64, 64)
+    assert bf.rule[30, 30, 30] == 0 and bf.rule[3, 30, 30] == SLIP and bf.rule[60, 3, 30] == SLIP
+    np.testing.assert_allclose(bf.param[3, 30, 30], [1, 0, 0])
+    np.testing.assert_allclose(bf.param[60, 3, 30], np.array([-1, 1, 0]) / np.sqrt(2), rtol=1e-7)
+    np.testing.assert_allclose(bf.param[0, 63, 0], np.array([1, -1, 1]) / np.sqrt(3), rtol=1e-7)
+    bf.fixed_box((20, 0, 20), (24, 4, 24)).separate_below(2)
+    assert bf.rule[21, 3, 21] == FIXED and bf.rule[40, 1, 40] == SEPARATE
+    bf.rotating_box((10, 10, 10), (20, 20, 12), center=(0.25, 0.25, 0.0), axis=(0, 0, -1), factor=2.0)
+    c = (15, 10, 11)
+    r = np.array([c[0] / 64 - 0.25, c[1] / 64 - 0.25, 0.0])
+    v = bf.param[c]
+    assert bf.rule[c] == VELOCITY
+    np.testing.assert_allclose(np.linalg.norm(v), 2.0 * np.linalg.norm(r), rtol=1e-6)
+    assert abs(v @ r) < 1e-7  # tangential
