@@ -568,10 +568,18 @@ def load_scene_json(path: str | Path) -> tuple[MPMConfig, list[MPMModel]]:
     """JSON scene files (a project addition; the reference's importer at
     include/mpm_io.h:168-199 is commented out).  Schema:
       {"config": {MPMConfig fields}, "models": [{"material": {...}, "mass": m,
-       "volume": v, "positions": "file.npy" | "file.bin" | [[x,y,z],...], "velocity": [[vx,vy,vz]]}]}
+       "volume": v, "positions": "file.npy" | "file.bin" | [[x,y,z],...], "velocity": [[vx,vy,vz]]}],
+       "boundary_rules": [{"slip_walls": width} | {"sticky_walls": width} | {"fixed_box": [lo, hi]} |
+                          {"velocity_box": [lo, hi, velocity]} |
+                          {"rotating_box": [lo, hi, center, axis, factor]} |
+                          {"separate_below": [cell_y, normal]}, ...]}
     A ".bin" file is raw float32 xyz triples, the reference's asset format
     (asset/*.bin, read by the scenes' SetupModel, e.g.
-    tests/sand_armadillo/test_sand_armadillo.cuh:137-192).
+    tests/sand_armadillo/test_sand_armadillo.cuh:137-192).  boundary_rules
+    (with config "boundary": "field") build the per-cell boundary with
+    ckmpm_b200.boundary.BoundaryField, applying the rules in order.  A material
+    gives MPMMaterial's fields, or "E" and "nu" for lambda_ and mu_
+    (ComputeLameParameters, include/mpm_material.cuh:277-283).
     """
     path = Path(path)
     spec = json.loads(path.read_text())
@@ -579,9 +587,26 @@ def load_scene_json(path: str | Path) -> tuple[MPMConfig, list[MPMModel]]:
     if "domain_blocks" in cfgd:
         cfgd["domain_blocks"] = tuple(cfgd["domain_blocks"])
     cfg = MPMConfig(**cfgd)
+    if spec.get("boundary_rules"):
+        from .boundary import BoundaryField
+        if cfg.boundary != "field":
+            raise ValueError('boundary_rules need config "boundary": "field"')
+        bf = BoundaryField(cfg)
+        for rule in spec["boundary_rules"]:
+            (name, args), = rule.items()
+            if name not in ("slip_walls", "sticky_walls", "fixed_box", "velocity_box", "rotating_box",
+                            "separate_below"):
+                raise ValueError(f"unknown boundary rule {name!r}")
+            getattr(bf, name)(*(args if isinstance(args, list) else [args]))
+        cfg.boundary_field = bf.arrays()
     models = []
     for md in spec["models"]:
-        mat = MPMMaterial(**md["material"])
+        matd = dict(md["material"])
+        if "E" in matd:  # Young's modulus and Poisson ratio, as the reference's scenes give them
+            lam, mu = compute_lame_parameters(matd.pop("E"), matd.pop("nu"))
+            matd.setdefault("lambda_", lam)
+            matd.setdefault("mu_", mu)
+        mat = MPMMaterial(**matd)
         pos = md["positions"]
         if isinstance(pos, str):
             pos = load_raw_positions(path.parent / pos) if pos.endswith(".bin") else np.load(path.parent / pos)
