@@ -20,6 +20,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <functional>
 #include <stdexcept>
 #include <string>
@@ -229,6 +230,81 @@ class MPMEngine {
       total += elapsed;
       if (exportFrame) exportFrame(f, *this);
     }
+    return total;
+  }
+
+  // The reference's own signature, Simulate(config, exportRootPath,
+  // collectConservationMetric, exportParticlePositionAsBinary, profileMode)
+  // (include/mpm_engine.cuh:457-909), so scene code calls it unchanged:
+  //  * exportParticlePositionAsBinary: after every frame, each model's positions as
+  //    raw float32 xyz in <root>/model_<i>_particle_frame_<frame>.txt (:433-444);
+  //    without it the reference writes Partio .bgeo files, which are not written here;
+  //  * collectConservationMetric: before every substep, one record of 13 float32
+  //    (time, Eulerian linear and angular momentum (zero), Lagrangian sum(v) and
+  //    sum(x cross v)) per model in <root>/conservationMetric_model_<i>.bin (:494-603),
+  //    stepping one substep at a time;
+  //  * profileMode: no export.
+  // Returns the simulated time (the reference ends the process).
+  double Simulate(const MPMConfig& config, const std::string& exportRootPath, bool collectConservationMetric,
+                  bool exportParticlePositionAsBinary, bool profileMode) {
+    const bool metric = collectConservationMetric && !profileMode;
+    const bool binary = exportParticlePositionAsBinary && !profileMode;
+    const size_t nmodels = counts_.size();
+    std::vector<FILE*> metricFiles;
+    if (metric)
+      for (size_t i = 0; i < nmodels; ++i) {
+        const std::string path = exportRootPath + "/conservationMetric_model_" + std::to_string(i) + ".bin";
+        FILE* f = std::fopen(path.c_str(), "wb");
+        if (!f) {
+          for (FILE* g : metricFiles) std::fclose(g);
+          throw Error(CKMPM_ERR_INVALID, "cannot open " + path);
+        }
+        metricFiles.push_back(f);
+      }
+    auto record = [&]() {
+      const double t = GetTime()[0];
+      for (size_t i = 0; i < nmodels; ++i) {
+        const std::array<Vector3, 4> m = GetConservationMetric(static_cast<int32_t>(i));
+        float row[13] = {static_cast<float>(t)};
+        for (int r = 0; r < 4; ++r)
+          for (int k = 0; k < 3; ++k) row[1 + 3 * r + k] = m[r][k];
+        std::fwrite(row, sizeof(float), 13, metricFiles[i]);
+      }
+    };
+    double total = 0.0;
+    try {
+      for (uint32_t f = 0; f < config.GetTotalSimulatedFrameCount(); ++f) {
+        if (config.GetExistRigidParticle()) {
+          const Vector3 v = config.GetRigidParticleVelocity(static_cast<int>(f));
+          check(ckmpm_set_rigid_velocity(scene_, v.data()), scene_, "ckmpm_set_rigid_velocity");
+        }
+        double frameTime = 1.0 / config.GetFps();
+        for (;;) {
+          if (metric) record();
+          double elapsed = 0.0;
+          check(ckmpm_step_adaptive(scene_, metric ? 1u : (1u << 30), dt_, config.GetCfl(), frameTime, &elapsed),
+                scene_, "ckmpm_step_adaptive");
+          total += elapsed;
+          frameTime = 0.0;  // later calls continue this frame
+          const std::array<double, 2> t = GetTime();
+          if (!metric || !(t[1] - t[0] > 0.0)) break;
+        }
+        if (binary)
+          for (size_t i = 0; i < nmodels; ++i) {
+            const std::vector<Vector3> x = GetParticlePosition(static_cast<int32_t>(i));
+            const std::string path = exportRootPath + "/model_" + std::to_string(i) + "_particle_frame_" +
+                                     std::to_string(f) + ".txt";
+            FILE* out = std::fopen(path.c_str(), "wb");
+            if (!out) throw Error(CKMPM_ERR_INVALID, "cannot open " + path);
+            std::fwrite(x.data(), sizeof(float), 3 * x.size(), out);
+            std::fclose(out);
+          }
+      }
+    } catch (...) {
+      for (FILE* g : metricFiles) std::fclose(g);
+      throw;
+    }
+    for (FILE* g : metricFiles) std::fclose(g);
     return total;
   }
 

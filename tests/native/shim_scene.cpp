@@ -4,12 +4,14 @@
 // include/ckmpm/mpm_engine.hpp and the engine library, with a plain host
 // compiler.  Used by tests/test_gpu_cpp_shim.py.
 //
-// usage: shim_scene <x.bin> <out.bin> <mass> <volume> <lambda> <mu> <frames> [rigid_count]
+// usage: shim_scene <x.bin> <out.bin> <mass> <volume> <lambda> <mu> <frames> [rigid_count [export_dir]]
 //   x.bin: float32 xyz triples; the cube falls with v0 = (0, -1, 0) on the
 //   1/64 grid (16^3 blocks, sticky walls), dt = 2^-14, 1024 frames per second.
 //   With rigid_count > 0 the model is von Mises (mu, lambda, yield 100) and its
 //   first rigid_count particles are rigid with velocity (1, 0.5 frame, 0).
-//   out.bin: positions after the last frame (input order).
+//   out.bin: positions after the last frame (input order).  With export_dir the
+//   scene calls the reference's own Simulate signature, writing per-frame raw
+//   positions and the per-substep conservation metric there.
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -31,6 +33,7 @@ int main(int argc, char** argv) {
   const float lambda = std::strtof(argv[5], nullptr), mu = std::strtof(argv[6], nullptr);
   const uint32_t frames = static_cast<uint32_t>(std::strtoul(argv[7], nullptr, 10));
   const uint32_t rigid = argc > 8 ? static_cast<uint32_t>(std::strtoul(argv[8], nullptr, 10)) : 0u;
+  const char* exportDir = argc > 9 ? argv[9] : nullptr;
 
   ckmpm::MPMConfig config;
   config.dx = 1.f / 64.f;
@@ -53,6 +56,10 @@ int main(int argc, char** argv) {
     simulator.Initialize(config);
     simulator.InitializeParticle(config, models);
     simulator.InitialSetup(config);
+    if (exportDir) {  // the reference's call, as in its scene executables
+      simulator.Simulate(config, exportDir, true, true, false);
+      return 0;
+    }
     std::vector<ckmpm::Vector3> last;
     std::array<ckmpm::Vector3, 4> metric{};
     simulator.Simulate(config, [&](uint32_t frame, ckmpm::MPMEngine& e) {

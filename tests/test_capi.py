@@ -71,6 +71,10 @@ int main() {
   cfg.boundary = CKMPM_BOUNDARY_FIELD;  // the irregular-boundary hook as per-cell rules
   cfg.boundaryRule.assign(64 * 64 * 64, static_cast<uint8_t>(CKMPM_CELL_SLIP));
   cfg.boundaryParam.assign(3 * 64 * 64 * 64, 0.f);
+  auto referenceCall = [](ckmpm::MPMEngine& e, const ckmpm::MPMConfig& c) {  // the reference's Simulate signature
+    return e.Simulate(c, std::string("out"), true, true, false);
+  };
+  (void)referenceCall;
   return all[5].c().p[6] == 1.f ? 0 : 1;
 }
 """

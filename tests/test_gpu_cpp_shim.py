@@ -73,3 +73,41 @@ def test_cpp_scene_matches_python_engine(scene_binary, tmp_path, rigid):
     line = [ln for ln in res.stderr.splitlines() if ln.startswith("metric ")][0]
     cpp_metric = np.array([float(t) for t in line.split()[1:]]).reshape(2, 3)
     np.testing.assert_allclose(cpp_metric, metric[2:].astype(np.float32), rtol=1e-6, atol=1e-6)
+
+
+def test_cpp_scene_reference_simulate_signature(scene_binary, tmp_path):
+    """Simulate(config, exportRootPath, collectConservationMetric=true,
+    exportParticlePositionAsBinary=true, profileMode=false), the reference's own
+    call: per-frame raw position files and a per-substep conservation-metric file
+    equal to the Python engine's."""
+    from ckmpm_b200 import MPMEngine
+    _, models = scenes.jelly_cube(lo=(0.44, 0.44, 0.44), hi=(0.56, 0.56, 0.56))
+    m = models[0]
+    lam, mu = compute_lame_parameters(E, NU)
+    lam, mu = float(np.float32(lam)), float(np.float32(mu))
+    xf = tmp_path / "x.bin"
+    np.ascontiguousarray(m.particle_position, np.float32).tofile(xf)
+    out = tmp_path / "ref_style"
+    out.mkdir()
+    res = subprocess.run([str(scene_binary), str(xf), str(tmp_path / "unused.bin"), f"{m.particle_mass:.9g}",
+                          f"{m.particle_volume:.9g}", f"{lam:.9g}", f"{mu:.9g}", str(FRAMES), "0", str(out)],
+                         capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    cfg, _ = scenes.jelly_cube(lo=(0.44, 0.44, 0.44), hi=(0.56, 0.56, 0.56))
+    cfg.dt, cfg.fps, cfg.total_frames = 2.0 ** -14, 1024, FRAMES
+    model = MPMModel(m.particle_mass, m.particle_volume, m.particle_position,
+                     np.asarray([[0.0, -1.0, 0.0]], np.float32), MPMMaterial.fixed_corotated(lam, mu))
+    py_root = tmp_path / "py"
+    eng = MPMEngine()
+    eng.Initialize(cfg)
+    eng.InitializeParticle(cfg, [model])
+    eng.InitialSetup(cfg)
+    eng.Simulate(cfg, export_root=py_root, collect_conservation_metric=True)
+    for f in range(FRAMES):
+        a = np.fromfile(out / f"model_0_particle_frame_{f}.txt", np.float32)
+        b = np.fromfile(py_root / f"model_0_particle_frame_{f}.txt", np.float32)
+        assert np.array_equal(a, b), f
+    ma = np.fromfile(out / "conservationMetric_model_0.bin", np.float32).reshape(-1, 13)
+    mb = np.fromfile(py_root / "conservationMetric_model_0.bin", np.float32).reshape(-1, 13)
+    assert ma.shape == mb.shape and ma.shape[0] >= 16 * FRAMES
+    np.testing.assert_allclose(ma, mb, rtol=1e-6, atol=1e-6)
