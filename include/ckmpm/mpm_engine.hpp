@@ -7,7 +7,8 @@
 //   Initialize(config)            (:171)                      ->    Initialize(config)
 //   InitializeParticle(config, models) (:92)                  ->    InitializeParticle(config, models)
 //   InitialSetup(config)          (:216)                      ->    InitialSetup(config)
-//   Simulate(config, dir, conservation, binary, profile) (:457) ->  Simulate(config, export_fn) -- returns
+//   Simulate(config, dir, conservation, binary, profile) (:457) ->  the same call, or Simulate(config, export_fn);
+//                                                                  both return instead of exiting
 //   MPMModel<MPMMaterial<k>>(mass, volume, x, v, material)    ->    ckmpm::MPMModel(mass, volume, x, v, material)
 //   MPMConfigBase<Derived> getters (include/mpm_config.h)     ->    ckmpm::MPMConfig (run-time fields, same getters)
 //
