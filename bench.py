@@ -420,7 +420,9 @@ def run_diff(args, rank, world, local_rank):
         "train_step_particle_substeps_per_s": n * nsteps / (ms / 1e3),
         "gradcheck": gradcheck, "loss": float(loss.item()), "clocks": clocks, "roofline": roofline,
         "cpu_baseline": cpu,
-        "gpu_launches": 4 + 2 * nsteps + 1 + (2 * nsteps + 2 * nsteps) + 4,
+        # per training step: forward (init, box reset, raster, grid + particle per substep), backward
+        # (recomputed segments, grid and particle adjoint per substep, finish, layout copies)
+        "gpu_launches": steps * (6 * nsteps - 2 * (nsteps // d["checkpoint_every"]) + 9),
         "e2e": {"value": n * nsteps / (e2e_ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": n * (12 + 12 + 4),
                 "d2h_bytes_per_step": 4 + n * (12 + 4),
                 "includes": "per step: x0, v0, log E uploaded from pinned host memory, forward + adjoint rollout "
@@ -704,7 +706,7 @@ def run_ours(args, rank, world, local_rank):
                    "tuning": {k: tuning[k] for k in ("threads", "ctas_per_sm", "graph_chunk")},
                    "l2": "particle state ~190 MB > 126 MB L2: no flush"},
         "roofline": roofline, "e2e": e2e, "clocks": clocks,
-        "gpu_launches": 1 + args.steps * (3 * len(models) + 2),
+        "gpu_launches": 1 + args.steps * (4 * len(models) + 1),  # per model: fused, 2 compaction, zero; + end
     }
     return line
 
