@@ -51,6 +51,13 @@ def golden_scenes():
         cfg, m = scenes.material_cube(kind)
         yield kind, "jelly", cfg, m[0]
     yield ("fluid_walls", "field") + wall_scene()
+    # The reference scenes' own material constants: the sand of
+    # tests/sand_armadillo (E 1e4, nu 0.4) and the fluid of tests/fluid_dam_break
+    # (bulk 10, gamma 7.15, viscosity 0.1).
+    cfg, m = scenes.small_sand(r=0.06, h=0.15, E=1e4, nu=0.4)
+    yield "sand_scene_params", "slip", cfg, m[0]
+    cfg, m = scenes.fluid_box(lo=(0.32, 0.3, 0.34), hi=(0.44, 0.42, 0.46), v0=(0.5, 0.0, -0.25), bulk=10.0)
+    yield "fluid_scene_params", "jelly", cfg, m[0]
 
 
 def wall_scene():

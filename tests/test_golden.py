@@ -3,9 +3,12 @@
 tests/golden/*.npz hold the positions that the reference's stock
 MPMEngine::Simulate exported on a B200 for seeded scenes
 (tests/golden/make_golden.py, oracle/ref_harness.cu): a fixed-corotated cube,
-a J-fluid box, a Drucker-Prager column on the slip floor, and von Mises,
+a J-fluid box, a Drucker-Prager column on the slip floor, von Mises,
 non-associated Cam-clay and linear cubes loaded by shear, converging and
-uniform initial velocity fields, 128 substeps of dt = 2^-14.  The reference exports unordered positions, so particles are
+uniform initial velocity fields, a fluid box against slip walls and a fixed box,
+and the column and the fluid box with the material constants of the
+reference's sand_armadillo and fluid_dam_break scenes, 128 substeps of
+dt = 2^-14.  The reference exports unordered positions, so particles are
 matched by nearest neighbour (spacing dx/2 = 7.8e-3 is far above the errors).
 
 Tolerance on positions after N substeps: 1e-6 + N * 2^-24.  The reference
