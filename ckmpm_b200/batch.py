@@ -5,7 +5,10 @@ No counterpart in the reference, whose MPMEngine is a per-GridConfig singleton
 SceneBatch holds up to 65536 scenes that share dx, the domain extent, gravity
 and the boundary rule, each with one model of its own material; every substep
 of every scene runs in one persistent fused launch plus the rebinning, replayed
-from CUDA graphs.  Each scene's result equals that of the same scene run alone.
+from CUDA graphs.  A scene's result does not depend, by a single bit, on the
+other scenes of the batch or on the launch shape; against the same scene run
+alone (a kernel compiled per material) it agrees to the last bits of x, v and
+F, as the two compilations may fuse a multiply-add differently.
 
 Across GPUs the scenes shard with no data exchange: shard_scenes() assigns
 scenes to ranks by a greedy longest-first bin-pack on their particle counts.

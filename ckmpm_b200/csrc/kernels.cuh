@@ -687,7 +687,10 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
     uint32_t n = cur.count[item];
     int kind = KIND;
     float mp0 = md.mat.p[0], mp1 = md.mat.p[1], mp2 = md.mat.p[2];
-    float vol_over_mass = md.vol / md.mass, unit = sc.grid_unit;
+    // Rounded division: the same bits as the host's V / m that a batched
+    // scene carries in its SceneMat (the build's fast division may differ by
+    // an ulp), so both forms start from the same constants.
+    float vol_over_mass = __fdiv_rn(md.vol, md.mass), unit = sc.grid_unit;
     double ratio = md.flush_ratio;
     if (KIND == kMixed) {
       const SceneMat& sm = md.smat[key.w];

@@ -253,8 +253,11 @@ ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, const ckmpm_ma
  * that share dx, the domain extent, gravity and the boundary rule of `desc`;
  * each scene has one model with its own material, particle mass and volume.
  * Every substep of every scene runs in the same launches (one persistent fused
- * kernel and the rebinning, captured in CUDA graphs), and each scene's results
- * equal those of the same scene run alone through ckmpm_create.  After
+ * kernel and the rebinning, captured in CUDA graphs).  A scene's results do not
+ * depend on the other scenes of the batch or on the launch shape, bit for bit;
+ * against the same scene run alone through ckmpm_create (whose kernel is
+ * compiled per material) they agree to the last bits of x, v and F, as the two
+ * compilations may fuse a multiply-add differently.  After
  * ckmpm_add_batch, the scene calls (ckmpm_setup, ckmpm_step*, ckmpm_status_check,
  * ckmpm_get_count, ckmpm_get_state, ckmpm_get_counters, ckmpm_destroy, ...)
  * take the batch handle with model 0; ckmpm_get_state returns all live

@@ -222,6 +222,34 @@ def test_particles_leaving_domain_are_counted(engine_lib, oracle_mod):
     assert s.counters()["lost"] == 1
 
 
+def test_full_block_next_to_lone_particles(engine_lib, oracle_mod):
+    """Ragged extremes of the per-block work: one block holding the maximum of
+    4096 particles (64 per cell over its 64 cells, the reference's bucket
+    capacity) and three blocks holding one particle each.  Ten substeps match
+    the FP64 oracle, and no capacity or consistency flag is raised."""
+    from ckmpm_b200.engine import compute_lame_parameters
+    dx, b = 1 / 64, 7
+    # Block b along an axis takes int(x / dx + 0.25) in [4b + 2, 4b + 5], so
+    # x / dx in [4b + 1.75, 4b + 5.75): a 16^3 lattice over [4b + 1.85, 4b + 5.65].
+    g = (4 * b + 1.85 + (np.arange(16) + 0.5) / 16 * 3.8) * dx
+    full = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    lone = np.array([[0.2, 0.2, 0.2], [0.8, 0.3, 0.7], [0.3, 0.75, 0.25]])
+    x = np.concatenate([full, lone]).astype(np.float32)
+    v = np.random.default_rng(3).uniform(-0.2, 0.2, x.shape).astype(np.float32)
+    lam, mu = compute_lame_parameters(5e4, 0.3)
+    vol = dx ** 3 / 64
+    m = MPMModel(1000.0 * vol, vol, x, v, MPMMaterial.fixed_corotated(lam, mu))
+    cfg = MPMConfig(dx=dx, domain_blocks=(16, 16, 16), gravity=-9.8)
+    s = run_engine(cfg, [m], 0, 1e-4)
+    keys, counts = s.blocks()
+    assert sorted(counts.tolist()) == [1, 1, 1, 4096]
+    assert [b, b, b] in keys.tolist()
+    s.step(10, 1e-4)
+    o = run_oracle(oracle_mod, cfg, [m], 10, 1e-4)
+    assert s.count(0) == len(x)
+    compare(s, o)
+
+
 def test_capacity_overflow_is_reported(engine_lib):
     cfg, models = scenes.jelly_cube()
     cfg.max_particles_per_block = 64  # a full block holds 512 particles at 8 ppc
