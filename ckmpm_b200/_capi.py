@@ -49,7 +49,7 @@ EXPORTED = (
     "ckmpm_set_tuning", "ckmpm_get_tuning", "ckmpm_autotune", "ckmpm_checkpoint_bytes", "ckmpm_checkpoint_save",
     "ckmpm_checkpoint_restore", "ckmpm_diff_create", "ckmpm_diff_forward", "ckmpm_diff_backward", "ckmpm_diff_timing",
     "ckmpm_diff_last_error", "ckmpm_diff_destroy", "ckmpm_set_rigid", "ckmpm_set_rigid_velocity", "ckmpm_get_time",
-    "ckmpm_set_boundary_field",
+    "ckmpm_set_boundary_field", "ckmpm_export_positions_async", "ckmpm_export_wait",
 )
 
 MAX_BATCH_SCENES = 65536
@@ -123,6 +123,8 @@ def lib() -> C.CDLL:
         L.ckmpm_set_boundary_field.argtypes = [P, C.POINTER(C.c_uint8), C.POINTER(C.c_float)]
         L.ckmpm_get_count.argtypes = [P, C.c_int32, u32p]
         L.ckmpm_get_state.argtypes = [P, C.c_int32, f32p, f32p, f32p, f32p, u32p, C.c_uint32, u32p]
+        L.ckmpm_export_positions_async.argtypes = [P, C.c_int32, f32p, C.c_uint32]
+        L.ckmpm_export_wait.argtypes = [P, u32p]
         L.ckmpm_get_blocks.argtypes = [P, C.c_int32, C.c_int32, i32p, u32p, C.c_uint32, u32p]
         L.ckmpm_get_counters.argtypes = [P, C.POINTER(C.c_uint64)]
         L.ckmpm_get_dt.argtypes = [P, f32p]

@@ -72,6 +72,7 @@ class SceneBatch(Scene):
             raise ValueError(f"at most {capi.MAX_BATCH_SCENES} scenes per batch")
         self.config = config
         self._h = C.c_void_p()
+        self._exports_in_flight: list[np.ndarray] = []
         L = capi.lib()
         desc = config.to_c()
         capi.check(L.ckmpm_create_batch(C.byref(desc), len(scenes), C.byref(self._h)), "ckmpm_create_batch", None)

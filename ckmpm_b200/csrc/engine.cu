@@ -46,6 +46,10 @@ struct ModelHost {
   uint32_t* opos = nullptr;
   void* oscan = nullptr;
   size_t oscan_bytes = 0;
+  // Asynchronous export: recorded on the copy stream after this model's
+  // staging buffer has been copied out.
+  cudaEvent_t ev_copied = nullptr;
+  bool copy_pending = false;
   // Batch: per-scene materials and input offsets (host copies and device arrays).
   std::vector<SceneMat> smat;
   std::vector<uint32_t> sstart;
@@ -76,6 +80,12 @@ struct ckmpm_scene {
   cudaGraphExec_t graph_chunk = nullptr;
   cudaGraphExec_t graph_one = nullptr;
   uint64_t host_step = 0;
+  // Asynchronous position export: copy stream, its events, the live count
+  // (pinned host scalar) and whether a copy may still be in flight.
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_probe = nullptr, ev_copy = nullptr;
+  uint32_t* export_count = nullptr;
+  bool export_pending = false;
   uint32_t rigid_count = 0;       // leading rigid particles of every von Mises model
   float rigid_v[3] = {0.f, 0.f, 0.f};
 };
@@ -828,6 +838,59 @@ ckmpm_status ckmpm_get_count(ckmpm_scene* s, int32_t model, uint32_t* n_live) {
   return CKMPM_OK;
 }
 
+// Export buffers of one model, allocated on first use.
+static cudaError_t ensure_export_buffers(ckmpm_scene* s, ModelHost& m) {
+  if (m.ox) return cudaSuccess;
+  const size_t cap_p = m.dev.cap_particles;
+  cudaError_t e;
+  if ((e = dalloc(s, &m.ox, 3 * cap_p)) != cudaSuccess) return e;
+  if ((e = dalloc(s, &m.ov, 3 * cap_p)) != cudaSuccess) return e;
+  if ((e = dalloc(s, &m.oF, 9 * cap_p)) != cudaSuccess) return e;
+  if ((e = dalloc(s, &m.oaux, cap_p)) != cudaSuccess) return e;
+  if ((e = dalloc(s, &m.oid, cap_p)) != cudaSuccess) return e;
+  if (m.dev.track_ids) {
+    if ((e = dalloc(s, &m.oflag, cap_p)) != cudaSuccess) return e;
+    if ((e = dalloc(s, &m.opos, cap_p)) != cudaSuccess) return e;
+    if ((e = cub::DeviceScan::ExclusiveSum(nullptr, m.oscan_bytes, m.oflag, m.opos, static_cast<int>(cap_p),
+                                           s->stream)) != cudaSuccess)
+      return e;
+    unsigned char* t = nullptr;
+    if ((e = dalloc(s, &t, m.oscan_bytes)) != cudaSuccess) return e;
+    m.oscan = t;
+  }
+  return cudaSuccess;
+}
+
+// Enqueues the gather of the requested per-particle arrays into the model's
+// export buffers (input order when ids are tracked).  n_upper bounds the live
+// count; n_dev, when given, is the device copy of it.
+static cudaError_t enqueue_export(ckmpm_scene* s, ModelHost& m, bool x, bool v, bool F, bool aux, bool id,
+                                  uint32_t n_upper, const uint32_t* n_dev) {
+  const size_t cap_p = m.dev.cap_particles;
+  const dim3 pg(s->sm_count * 4), pb(kProbeThreads);
+  const uint32_t* dest = nullptr;
+  cudaError_t e;
+  if (m.copy_pending && (e = cudaStreamWaitEvent(s->stream, m.ev_copied, 0)) != cudaSuccess) return e;
+  if (m.dev.track_ids) {
+    // ids in block order, then the position of each live id in input order
+    probe_kernel<kProbeThreads><<<pg, pb, kSmemVTile, s->stream>>>(s->sc, m.dev, s->grid, s->scal, nullptr, nullptr,
+                                                                 nullptr, nullptr, m.oid, nullptr);
+    if ((e = cudaMemsetAsync(m.oflag, 0, sizeof(uint32_t) * cap_p, s->stream)) != cudaSuccess) return e;
+    if (n_upper)
+      mark_ids_kernel<<<(n_upper + 255) / 256, 256, 0, s->stream>>>(n_upper, m.oid, m.oflag,
+                                                                    static_cast<uint32_t>(cap_p), n_dev);
+    size_t tb = m.oscan_bytes;
+    if ((e = cub::DeviceScan::ExclusiveSum(m.oscan, tb, m.oflag, m.opos, static_cast<int>(cap_p), s->stream)) !=
+        cudaSuccess)
+      return e;
+    dest = m.opos;
+  }
+  probe_kernel<kProbeThreads><<<pg, pb, kSmemVTile, s->stream>>>(s->sc, m.dev, s->grid, s->scal, x ? m.ox : nullptr,
+                                                               v ? m.ov : nullptr, F ? m.oF : nullptr,
+                                                               aux ? m.oaux : nullptr, id ? m.oid : nullptr, dest);
+  return cudaGetLastError();
+}
+
 ckmpm_status ckmpm_get_state(ckmpm_scene* s, int32_t model, float* x, float* v, float* F, float* aux, uint32_t* id,
                              uint32_t cap, uint32_t* n_out) {
   if (!s) return fail(s, CKMPM_ERR_INVALID, "null scene");
@@ -841,46 +904,60 @@ ckmpm_status ckmpm_get_state(ckmpm_scene* s, int32_t model, float* x, float* v, 
   if (n_out) *n_out = n;
   if (cap < n) return fail(s, CKMPM_ERR_NOT_FOUND, "output capacity too small");
   if (n == 0) return CKMPM_OK;
-  const size_t cap_p = m.dev.cap_particles;
-  const bool sorted = m.dev.track_ids != 0;
-  if (!m.ox) {
-    CK_CUDA(s, dalloc(s, &m.ox, 3 * cap_p));
-    CK_CUDA(s, dalloc(s, &m.ov, 3 * cap_p));
-    CK_CUDA(s, dalloc(s, &m.oF, 9 * cap_p));
-    CK_CUDA(s, dalloc(s, &m.oaux, cap_p));
-    CK_CUDA(s, dalloc(s, &m.oid, cap_p));
-    if (sorted) {
-      CK_CUDA(s, dalloc(s, &m.oflag, cap_p));
-      CK_CUDA(s, dalloc(s, &m.opos, cap_p));
-      CK_CUDA(s, cub::DeviceScan::ExclusiveSum(nullptr, m.oscan_bytes, m.oflag, m.opos, static_cast<int>(cap_p),
-                                               s->stream));
-      unsigned char* t = nullptr;
-      CK_CUDA(s, dalloc(s, &t, m.oscan_bytes));
-      m.oscan = t;
-    }
-  }
-  const dim3 pg(s->sm_count * 4), pb(kProbeThreads);
-  const uint32_t* dest = nullptr;
-  if (sorted) {
-    // ids in block order, then the position of each live id in input order
-    probe_kernel<kProbeThreads><<<pg, pb, kSmemVTile, s->stream>>>(s->sc, m.dev, s->grid, s->scal, nullptr, nullptr,
-                                                                 nullptr, nullptr, m.oid, nullptr);
-    CK_CUDA(s, cudaMemsetAsync(m.oflag, 0, sizeof(uint32_t) * cap_p, s->stream));
-    mark_ids_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(n, m.oid, m.oflag, static_cast<uint32_t>(cap_p));
-    size_t tb = m.oscan_bytes;
-    CK_CUDA(s, cub::DeviceScan::ExclusiveSum(m.oscan, tb, m.oflag, m.opos, static_cast<int>(cap_p), s->stream));
-    dest = m.opos;
-  }
-  probe_kernel<kProbeThreads><<<pg, pb, kSmemVTile, s->stream>>>(s->sc, m.dev, s->grid, s->scal, x ? m.ox : nullptr,
-                                                               v ? m.ov : nullptr, F ? m.oF : nullptr,
-                                                               aux ? m.oaux : nullptr, id ? m.oid : nullptr, dest);
-  CK_CUDA(s, cudaGetLastError());
+  CK_CUDA(s, ensure_export_buffers(s, m));
+  CK_CUDA(s, enqueue_export(s, m, x, v, F, aux, id, n, nullptr));
   if (x) CK_CUDA(s, cudaMemcpyAsync(x, m.ox, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
   if (v) CK_CUDA(s, cudaMemcpyAsync(v, m.ov, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->stream));
   if (F) CK_CUDA(s, cudaMemcpyAsync(F, m.oF, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost, s->stream));
   if (aux) CK_CUDA(s, cudaMemcpyAsync(aux, m.oaux, sizeof(float) * n, cudaMemcpyDeviceToHost, s->stream));
   if (id) CK_CUDA(s, cudaMemcpyAsync(id, m.oid, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s->stream));
   CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_export_positions_async(ckmpm_scene* s, int32_t model, float* x, uint32_t cap) {
+  if (!s || !x) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  if (!s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  if (model < 0 || model >= static_cast<int32_t>(s->models.size())) return fail(s, CKMPM_ERR_NOT_FOUND, "no such model");
+  ModelHost& m = s->models[model];
+  // Live particles never exceed those binned at setup, nor the id range.
+  const uint32_t n_upper = m.n_valid;
+  if (cap < n_upper) return fail(s, CKMPM_ERR_NOT_FOUND, "output capacity too small");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  if (!s->copy_stream) {
+    CK_CUDA(s, cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+    CK_CUDA(s, cudaEventCreateWithFlags(&s->ev_probe, cudaEventDisableTiming));
+    CK_CUDA(s, cudaEventCreateWithFlags(&s->ev_copy, cudaEventDisableTiming));
+    CK_CUDA(s, cudaMallocHost(&s->export_count, sizeof(uint32_t)));
+    *s->export_count = 0;
+  }
+  CK_CUDA(s, ensure_export_buffers(s, m));
+  if (!m.ev_copied) CK_CUDA(s, cudaEventCreateWithFlags(&m.ev_copied, cudaEventDisableTiming));
+  const uint32_t* n_dev = m.dev.bl[s->host_step & 1].nparticles;
+  CK_CUDA(s, enqueue_export(s, m, true, false, false, false, false, n_upper, n_dev));
+  CK_CUDA(s, cudaEventRecord(s->ev_probe, s->stream));
+  CK_CUDA(s, cudaStreamWaitEvent(s->copy_stream, s->ev_probe, 0));
+  CK_CUDA(s, cudaMemcpyAsync(s->export_count, n_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->copy_stream));
+  if (n_upper)
+    CK_CUDA(s, cudaMemcpyAsync(x, m.ox, sizeof(float) * 3 * n_upper, cudaMemcpyDeviceToHost, s->copy_stream));
+  CK_CUDA(s, cudaEventRecord(m.ev_copied, s->copy_stream));
+  CK_CUDA(s, cudaEventRecord(s->ev_copy, s->copy_stream));
+  m.copy_pending = true;
+  s->export_pending = true;
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_export_wait(ckmpm_scene* s, uint32_t* n_out) {
+  if (!s) return fail(s, CKMPM_ERR_INVALID, "null scene");
+  if (!s->export_pending) {
+    if (n_out) *n_out = s->export_count ? *s->export_count : 0u;
+    return CKMPM_OK;
+  }
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  CK_CUDA(s, cudaEventSynchronize(s->ev_copy));  // the copy stream runs in order: every export is done
+  s->export_pending = false;
+  for (auto& m : s->models) m.copy_pending = false;
+  if (n_out) *n_out = *s->export_count;
   return CKMPM_OK;
 }
 
@@ -1130,6 +1207,15 @@ ckmpm_status ckmpm_destroy(ckmpm_scene* s) {
   if (!s) return CKMPM_OK;
   cudaSetDevice(s->desc.device);
   if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->copy_stream) {
+    cudaStreamSynchronize(s->copy_stream);
+    cudaStreamDestroy(s->copy_stream);
+    cudaEventDestroy(s->ev_probe);
+    cudaEventDestroy(s->ev_copy);
+    cudaFreeHost(s->export_count);
+    for (auto& m : s->models)
+      if (m.ev_copied) cudaEventDestroy(m.ev_copied);
+  }
   free_graphs(s);
   for (auto& p : s->allocs) cudaFree(p.first);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);

@@ -1378,10 +1378,13 @@ __global__ void __launch_bounds__(NT) probe_kernel(SceneDev sc, ModelDev md, Gri
 // Input-order export: flag[id] = 1 for every live particle (ids from the
 // block-order probe); an exclusive scan of the flags gives each live id its
 // position among the live particles in input order.
+// Marks the live ids (the first n of ids, or the first *n_dev when given: an
+// export enqueued without reading the live count back).
 __global__ void mark_ids_kernel(uint32_t n, const uint32_t* __restrict__ ids, uint32_t* __restrict__ flag,
-                               uint32_t cap) {
+                               uint32_t cap, const uint32_t* __restrict__ n_dev) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && ids[i] < cap) flag[ids[i]] = 1u;
+  const uint32_t live = n_dev ? min(n, *n_dev) : n;
+  if (i < live && ids[i] < cap) flag[ids[i]] = 1u;
 }
 
 // ------------------------------------------------------------------ debug hook

@@ -271,6 +271,7 @@ class Scene:
         desc = config.to_c()
         capi.check(L.ckmpm_create(C.byref(desc), C.byref(self._h)), "ckmpm_create", None)
         self.models: list[MPMModel] = []
+        self._exports_in_flight: list[np.ndarray] = []  # host buffers of unfinished exports
         if config.exist_rigid_particle:
             self.set_rigid(config.rigid_particle_count, config.GetRigidParticleVelocity(0))
         if config.boundary == "field" and config.boundary_field is not None:
@@ -358,6 +359,26 @@ class Scene:
     def count(self, model: int = 0) -> int:
         n = C.c_uint32()
         capi.check(capi.lib().ckmpm_get_count(self._h, model, C.byref(n)), "ckmpm_get_count", self._h)
+        return n.value
+
+    def export_positions_async(self, model: int, x: np.ndarray) -> None:
+        """Enqueue a positions export of `model` into x (float32, C-contiguous, at
+        least the model's particle count rows of 3), as state(model).x would hold
+        it; returns at once.  With x in pinned memory (torch's pin_memory) the
+        copy overlaps the substeps enqueued after this call.  x is filled when
+        export_wait() returns, which gives the number of valid leading rows; read
+        nothing from x before that."""
+        if x.dtype != np.float32 or not x.flags.c_contiguous or x.ndim != 2 or x.shape[1] != 3:
+            raise ValueError("x must be a C-contiguous float32 array of shape (n, 3)")
+        capi.check(capi.lib().ckmpm_export_positions_async(self._h, model, capi.fptr(x), x.shape[0]),
+                   "ckmpm_export_positions_async", self._h)
+        self._exports_in_flight.append(x)
+
+    def export_wait(self) -> int:
+        """Wait for the exports enqueued so far; returns the live count of the last one."""
+        n = C.c_uint32()
+        capi.check(capi.lib().ckmpm_export_wait(self._h, C.byref(n)), "ckmpm_export_wait", self._h)
+        self._exports_in_flight.clear()
         return n.value
 
     def state(self, model: int = 0) -> ParticleState:

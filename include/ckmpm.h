@@ -188,6 +188,21 @@ ckmpm_status ckmpm_get_count(ckmpm_scene* s, int32_t model, uint32_t* n_live);
 ckmpm_status ckmpm_get_state(ckmpm_scene* s, int32_t model, float* x, float* v, float* F, float* aux,
                              uint32_t* id, uint32_t cap, uint32_t* n_out);
 
+/* Positions export that overlaps the substeps enqueued after it, in place of
+ * the reference's per-frame ExportParticleToModel + background exporter
+ * thread (include/mpm_engine.cuh:386-454, include/mpm_io.h:93-166).  Enqueues
+ * on the scene's stream the gather of model's positions as ckmpm_get_state
+ * writes x (input order with CKMPM_FLAG_TRACK_IDS, else block order) into a
+ * device staging buffer, then copies it into x on a second stream; returns
+ * without waiting.  x is a host buffer (pinned, for the copy to overlap) of
+ * cap >= the model's particle count floats x 3; it must not be read before
+ * ckmpm_export_wait, which waits for the last export and gives its live
+ * count (the valid leading entries of x).  A later export or ckmpm_get_state
+ * waits for the previous copy on the device before it reuses the staging
+ * buffer. */
+ckmpm_status ckmpm_export_positions_async(ckmpm_scene* s, int32_t model, float* x, uint32_t cap);
+ckmpm_status ckmpm_export_wait(ckmpm_scene* s, uint32_t* n_out);
+
 /* Canonical block sets (what MPMPartition holds after a substep,
  * include/mpm_partition.cuh:37-174 and include/mpm_engine.cuh:659-865):
  * which = 0: blocks holding particles of `model` (all models if model < 0),

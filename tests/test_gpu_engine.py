@@ -250,6 +250,40 @@ def test_full_block_next_to_lone_particles(engine_lib, oracle_mod):
     compare(s, o)
 
 
+def test_async_position_export(engine_lib):
+    """ckmpm_export_positions_async: each model's buffer receives the positions
+    as of the export, not those of substeps enqueued after it, bit for bit
+    what state() returns; export_wait gives the live count; ckmpm_get_state
+    after an export waits for its copy; a short buffer is refused."""
+    import torch
+    cfg, m1 = scenes.jelly_cube(lo=(0.3, 0.3, 0.3), hi=(0.42, 0.42, 0.42), v0=(1.0, 0.0, 0.0))
+    _, m2 = scenes.fluid_box(lo=(0.44, 0.3, 0.3), hi=(0.55, 0.4, 0.42), v0=(-1.0, 0.0, 0.0))
+    models = [m1[0], m2[0]]
+    s = run_engine(cfg, models, 6, 1e-4)
+    ref = [s.state(i).x for i in range(2)]
+    bufs = [torch.zeros((len(m.particle_position), 3), dtype=torch.float32).pin_memory().numpy() for m in models]
+    for i in range(2):
+        s.export_positions_async(i, bufs[i])
+    s.step_async(25, 1e-4)
+    n = s.export_wait()
+    assert n == len(ref[1])
+    for i in range(2):
+        assert np.array_equal(bufs[i][:len(ref[i])], ref[i]), i
+    later = s.state(0).x
+    assert not np.array_equal(later, ref[0])
+    s.export_positions_async(0, bufs[0])
+    again = s.state(0).x  # reuses the staging buffer after the copy
+    assert s.export_wait() == len(again)
+    assert np.array_equal(bufs[0][:len(again)], again) and np.array_equal(again, later)
+    pageable = np.zeros_like(bufs[1])
+    s.export_positions_async(1, pageable)
+    s.export_wait()
+    assert np.array_equal(pageable[:len(ref[1])], s.state(1).x)
+    with pytest.raises(capi.CkmpmError):
+        s.export_positions_async(0, np.zeros((3, 3), np.float32))
+    s.close()
+
+
 def test_capacity_overflow_is_reported(engine_lib):
     cfg, models = scenes.jelly_cube()
     cfg.max_particles_per_block = 64  # a full block holds 512 particles at 8 ppc
