@@ -32,7 +32,10 @@ struct ModelHost {
   float mass = 0.f, vol = 0.f;
   uint32_t n = 0;       // particles passed in
   uint32_t n_valid = 0; // particles binned at setup
-  std::vector<float> x, v;
+  // Input positions and velocities on the device, copied there by
+  // ckmpm_add_model / ckmpm_add_batch and released by ckmpm_setup.
+  float* x_dev = nullptr;
+  float* v_dev = nullptr;
   uint32_t nv = 0;
   ModelDev dev{};
   uint32_t ntiles = 0;
@@ -408,6 +411,26 @@ cudaError_t checkpoint_copy(ckmpm_scene* s, unsigned char* buf, bool save) {
 
 }  // namespace
 
+// Copies a model's input positions and velocities to the device (DMA when the
+// caller's buffers are pinned) and waits, so the caller may reuse its buffers
+// on return and ckmpm_setup reads the inputs from device memory.
+static cudaError_t stage_inputs(ckmpm_scene* s, ModelHost& m, const float* x, const float* v) {
+  cudaError_t e = cudaSetDevice(s->desc.device);
+  if (e == cudaSuccess) e = cudaMalloc(&m.x_dev, sizeof(float) * 3 * static_cast<size_t>(m.n));
+  if (e == cudaSuccess) e = cudaMalloc(&m.v_dev, sizeof(float) * 3 * static_cast<size_t>(m.nv));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m.x_dev, x, sizeof(float) * 3 * static_cast<size_t>(m.n), cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m.v_dev, v, sizeof(float) * 3 * static_cast<size_t>(m.nv), cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) {
+    cudaFree(m.x_dev);
+    cudaFree(m.v_dev);
+    m.x_dev = m.v_dev = nullptr;
+  }
+  return e;
+}
+
 extern "C" {
 
 const char* ckmpm_version(void) { return kVersion; }
@@ -455,8 +478,7 @@ ckmpm_status ckmpm_add_batch(ckmpm_scene* s, uint32_t nscenes, const ckmpm_batch
   m.nv = m.n;
   m.mass = lightest;  // only the adaptive-dt mass floor reads it for a batch
   m.vol = 1.f;
-  m.x.assign(x, x + 3 * static_cast<size_t>(total));
-  m.v.assign(v, v + 3 * static_cast<size_t>(total));
+  CK_CUDA(s, stage_inputs(s, m, x, v));
   s->models.push_back(std::move(m));
   return CKMPM_OK;
 }
@@ -521,8 +543,7 @@ ckmpm_status ckmpm_add_model(ckmpm_scene* s, const ckmpm_material* material, uin
   m.vol = volume;
   m.n = n;
   m.nv = nv;
-  m.x.assign(x, x + 3 * static_cast<size_t>(n));
-  m.v.assign(v, v + 3 * static_cast<size_t>(nv));
+  CK_CUDA(s, stage_inputs(s, m, x, v));
   s->models.push_back(std::move(m));
   if (model_index) *model_index = static_cast<int32_t>(s->models.size()) - 1;
   return CKMPM_OK;
@@ -608,16 +629,12 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     }
 
     // Upload, bin, radix-sort by colour-major block index, compact.
-    float *dx_in = nullptr, *dv_in = nullptr;
+    float *dx_in = m.x_dev, *dv_in = m.v_dev;
     uint32_t *k_in = nullptr, *k_out = nullptr, *v_in = nullptr, *v_out = nullptr;
-    CK_CUDA(s, cudaMalloc(&dx_in, sizeof(float) * 3 * n));
-    CK_CUDA(s, cudaMalloc(&dv_in, sizeof(float) * 3 * m.nv));
     CK_CUDA(s, cudaMalloc(&k_in, sizeof(uint32_t) * n));
     CK_CUDA(s, cudaMalloc(&k_out, sizeof(uint32_t) * n));
     CK_CUDA(s, cudaMalloc(&v_in, sizeof(uint32_t) * n));
     CK_CUDA(s, cudaMalloc(&v_out, sizeof(uint32_t) * n));
-    CK_CUDA(s, cudaMemcpyAsync(dx_in, m.x.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->stream));
-    CK_CUDA(s, cudaMemcpyAsync(dv_in, m.v.data(), sizeof(float) * 3 * m.nv, cudaMemcpyHostToDevice, s->stream));
     setup_bin_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(s->sc, n, dx_in, d.sstart, k_in, v_in, d.dense_total);
     size_t temp_bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, k_in, k_out, v_in, v_out, static_cast<int>(n), 0, 32,
@@ -655,6 +672,7 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     CK_CUDA(s, cudaStreamSynchronize(s->stream));
     cudaFree(dx_in);
     cudaFree(dv_in);
+    m.x_dev = m.v_dev = nullptr;
     cudaFree(k_in);
     cudaFree(k_out);
     cudaFree(v_in);
@@ -1215,6 +1233,10 @@ ckmpm_status ckmpm_destroy(ckmpm_scene* s) {
     cudaFreeHost(s->export_count);
     for (auto& m : s->models)
       if (m.ev_copied) cudaEventDestroy(m.ev_copied);
+  }
+  for (auto& m : s->models) {  // inputs of a scene that never ran ckmpm_setup
+    if (m.x_dev) cudaFree(m.x_dev);
+    if (m.v_dev) cudaFree(m.v_dev);
   }
   free_graphs(s);
   for (auto& p : s->allocs) cudaFree(p.first);

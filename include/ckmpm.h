@@ -111,7 +111,8 @@ ckmpm_status ckmpm_create(const ckmpm_scene_desc* desc, ckmpm_scene** out);
 /* Replaces MPMModel(mass, volume, x, v, material) (include/mpm_model.h:19-33)
  * plus the per-model part of MPMEngine::InitializeParticle
  * (include/mpm_engine.cuh:92-168).  x: n float3 positions, v: nv float3
- * velocities with nv == 1 (shared) or nv == n.  Host pointers. */
+ * velocities with nv == 1 (shared) or nv == n.  Host pointers; they are
+ * copied to the device before the call returns (by DMA when pinned). */
 ckmpm_status ckmpm_add_model(ckmpm_scene* s, const ckmpm_material* material, uint32_t n, const float* x,
                              const float* v, uint32_t nv, float mass, float volume, int32_t* model_index);
 
