@@ -856,25 +856,27 @@ ckmpm_status ckmpm_get_count(ckmpm_scene* s, int32_t model, uint32_t* n_live) {
   return CKMPM_OK;
 }
 
-// Export buffers of one model, allocated on first use.
+// Export buffers of one model, allocated on first use (each one that is still
+// missing, so a call after a failed allocation completes the set).
 static cudaError_t ensure_export_buffers(ckmpm_scene* s, ModelHost& m) {
-  if (m.ox) return cudaSuccess;
   const size_t cap_p = m.dev.cap_particles;
-  cudaError_t e;
-  if ((e = dalloc(s, &m.ox, 3 * cap_p)) != cudaSuccess) return e;
-  if ((e = dalloc(s, &m.ov, 3 * cap_p)) != cudaSuccess) return e;
-  if ((e = dalloc(s, &m.oF, 9 * cap_p)) != cudaSuccess) return e;
-  if ((e = dalloc(s, &m.oaux, cap_p)) != cudaSuccess) return e;
-  if ((e = dalloc(s, &m.oid, cap_p)) != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
+  if (!m.ox && (e = dalloc(s, &m.ox, 3 * cap_p)) != cudaSuccess) return e;
+  if (!m.ov && (e = dalloc(s, &m.ov, 3 * cap_p)) != cudaSuccess) return e;
+  if (!m.oF && (e = dalloc(s, &m.oF, 9 * cap_p)) != cudaSuccess) return e;
+  if (!m.oaux && (e = dalloc(s, &m.oaux, cap_p)) != cudaSuccess) return e;
+  if (!m.oid && (e = dalloc(s, &m.oid, cap_p)) != cudaSuccess) return e;
   if (m.dev.track_ids) {
-    if ((e = dalloc(s, &m.oflag, cap_p)) != cudaSuccess) return e;
-    if ((e = dalloc(s, &m.opos, cap_p)) != cudaSuccess) return e;
-    if ((e = cub::DeviceScan::ExclusiveSum(nullptr, m.oscan_bytes, m.oflag, m.opos, static_cast<int>(cap_p),
-                                           s->stream)) != cudaSuccess)
-      return e;
-    unsigned char* t = nullptr;
-    if ((e = dalloc(s, &t, m.oscan_bytes)) != cudaSuccess) return e;
-    m.oscan = t;
+    if (!m.oflag && (e = dalloc(s, &m.oflag, cap_p)) != cudaSuccess) return e;
+    if (!m.opos && (e = dalloc(s, &m.opos, cap_p)) != cudaSuccess) return e;
+    if (!m.oscan) {
+      if ((e = cub::DeviceScan::ExclusiveSum(nullptr, m.oscan_bytes, m.oflag, m.opos, static_cast<int>(cap_p),
+                                             s->stream)) != cudaSuccess)
+        return e;
+      unsigned char* t = nullptr;
+      if ((e = dalloc(s, &t, m.oscan_bytes)) != cudaSuccess) return e;
+      m.oscan = t;
+    }
   }
   return cudaSuccess;
 }
