@@ -67,13 +67,14 @@ CKMPM_DEV void matmul3(const float* a, const float* b, float* r) {
 // (include/mpm_math.cuh:1-18).  Implemented here from the published outline:
 //   1. symmetric eigenproblem of A^T A by cyclic Jacobi (fixed sweep count,
 //      exact rotation angles from the 2x2 Schur form).  Three sweeps reach
-//      FP32 rounding: in an FP32 emulation of these steps over 3000 random
+//      FP32 rounding: in an FP32 emulation of these steps over 4000 random
 //      F = R1 diag(s) R2 per family, with s in [0.1, 3] and
 //      e^[-2, 2], and I + N(0, 0.5) shears, the singular values agree with an
 //      FP64 SVD to 4e-7 relative (max) with three sweeps and with four; the
-//      off-diagonal residual of (A V)^T (A V) is 1.5e-7 at the 99th percentile
-//      either way and 1.8e-6 at worst with three (2.7e-7 with four);
-//      the fourth sweep costs ~2 % of the substep;
+//      off-diagonal residual of (A V)^T (A V) is ~1.6e-7 at the 99th percentile
+//      either way, and up to 6e-6 for about 1 matrix in 1000 with three
+//      (2.7e-7 at worst with four); the fourth sweep costs ~2 % of the substep
+//      (tests/test_svd_sweeps.py restates these steps and checks the bounds);
 //   2. B = A V, columns sorted by decreasing norm (sign flips keep det V = 1);
 //   3. Givens QR of B gives U and the diagonal S.
 
