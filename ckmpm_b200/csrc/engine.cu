@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -32,14 +33,14 @@ struct ModelHost {
   float mass = 0.f, vol = 0.f;
   uint32_t n = 0;       // particles passed in
   uint32_t n_valid = 0; // particles binned at setup
-  // Input positions and velocities on the device, copied there by
-  // ckmpm_add_model / ckmpm_add_batch and released by ckmpm_setup.
-  float* x_dev = nullptr;
-  float* v_dev = nullptr;
   uint32_t nv = 0;
   ModelDev dev{};
   uint32_t ntiles = 0;
-  // Export buffers (device), allocated on the first ckmpm_get_state.
+  // The model's I/O arena: one device allocation made by ckmpm_add_model /
+  // ckmpm_add_batch and kept until ckmpm_destroy.  Until setup it holds the
+  // inputs (x in ox, v in ov) and, during setup, the binning sort's keys and
+  // values (in oF) and its scratch; afterwards the export buffers.
+  unsigned char* io = nullptr;
   float* ox = nullptr;
   float* ov = nullptr;
   float* oF = nullptr;
@@ -49,6 +50,8 @@ struct ModelHost {
   uint32_t* opos = nullptr;
   void* oscan = nullptr;
   size_t oscan_bytes = 0;
+  void* sort_temp = nullptr;
+  size_t sort_temp_bytes = 0;
   // Asynchronous export: recorded on the copy stream after this model's
   // staging buffer has been copied out.
   cudaEvent_t ev_copied = nullptr;
@@ -107,6 +110,21 @@ ckmpm_status fail(ckmpm_scene* s, ckmpm_status code, const std::string& msg) {
     if (e_ != cudaSuccess)                                                                            \
       return fail((s), CKMPM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));           \
   } while (0)
+
+// Consecutive sub-allocations of one device allocation, each on a 256-byte
+// boundary.  With a null base it only measures: run a layout once to size the
+// allocation, then again on the allocation to place the pointers.
+struct Carve {
+  unsigned char* base = nullptr;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t count) {
+    off = (off + 255) & ~static_cast<size_t>(255);
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += std::max<size_t>(count, 1) * sizeof(T);
+    return p;
+  }
+};
 
 template <typename T>
 cudaError_t dalloc(ckmpm_scene* s, T** p, size_t count) {
@@ -324,6 +342,13 @@ ckmpm_status create_impl(const ckmpm_scene_desc* desc, uint32_t nstack, ckmpm_sc
   if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(s, CKMPM_ERR_CUDA, "cudaStreamCreate failed"));
   s->stream = s->own_stream;
+  // Asynchronous position export: its copy stream, events and pinned live count.
+  if (cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_probe, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_copy, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost(&s->export_count, sizeof(uint32_t)) != cudaSuccess)
+    return bail(fail(s, CKMPM_ERR_CUDA, "export stream, events or pinned count could not be created"));
+  *s->export_count = 0;
 
   SceneDev& sc = s->sc;
   sc.dx = desc->dx;
@@ -411,22 +436,97 @@ cudaError_t checkpoint_copy(ckmpm_scene* s, unsigned char* buf, bool save) {
 
 }  // namespace
 
-// Copies a model's input positions and velocities to the device (DMA when the
-// caller's buffers are pinned) and waits, so the caller may reuse its buffers
-// on return and ckmpm_setup reads the inputs from device memory.
+// Places the I/O arena of a model (see ModelHost::io): export buffers for
+// n particles, with the setup sort's four key/value arrays inside oF, the
+// sort's and the export scan's scratch after them.
+static void io_layout(ModelHost& m, bool track, Carve& c) {
+  const size_t n = m.n;
+  m.ox = c.take<float>(3 * n);
+  m.ov = c.take<float>(3 * n);
+  m.oF = c.take<float>(9 * n);
+  m.oaux = c.take<float>(n);
+  m.oid = c.take<uint32_t>(n);
+  m.oflag = track ? c.take<uint32_t>(n) : nullptr;
+  m.opos = track ? c.take<uint32_t>(n) : nullptr;
+  m.oscan = track ? c.take<unsigned char>(m.oscan_bytes) : nullptr;
+  m.sort_temp = c.take<unsigned char>(m.sort_temp_bytes);
+}
+
+// Places a model's simulation state: the double-buffered particle arrays and
+// block lists, the binning totals, compaction partials, the work ticket, the
+// sorted initial velocities and a batch's per-scene tables.
+static void state_layout(ModelHost& m, uint32_t nbd, bool track, Carve& c) {
+  ModelDev& d = m.dev;
+  const size_t n = m.n;
+  const bool batch = m.mat.kind == kMixedKind;
+  const bool hasF = batch || material_has_F(m.mat.kind);
+  const bool hasAux = batch || material_has_aux(m.mat.kind);
+  const bool hasQ = batch ? std::count(m.skind.begin(), m.skind.end(), CKMPM_LINEAR) > 0 : m.mat.kind == CKMPM_LINEAR;
+  for (int b = 0; b < 2; ++b) {
+    StateDev& st = d.st[b];
+    for (int a = 0; a < 3; ++a) st.x[a] = c.take<float>(n);
+    for (int k = 0; k < 9; ++k) st.F[k] = hasF ? c.take<float>(n) : nullptr;
+    st.aux = hasAux ? c.take<float>(n) : nullptr;
+    for (int k = 0; k < 9; ++k) st.Q[k] = hasQ ? c.take<float>(n) : nullptr;
+    st.id = track ? c.take<uint32_t>(n) : nullptr;
+    BlockListDev& bl = d.bl[b];
+    bl.keys = c.take<int4>(d.cap_slots);
+    bl.start = c.take<uint32_t>(d.cap_slots);
+    bl.count = c.take<uint32_t>(d.cap_slots);
+    bl.table = c.take<int32_t>(nbd);
+    bl.prefix28 = c.take<uint32_t>(static_cast<size_t>(d.cap_slots) * 28);
+    bl.idx = c.take<uint16_t>(n);
+    bl.nblocks = c.take<uint32_t>(1);
+    bl.nparticles = c.take<uint32_t>(1);
+  }
+  d.dense_total = c.take<uint32_t>(nbd);
+  d.tile_sums = c.take<uint32_t>(2 * static_cast<size_t>(m.ntiles));
+  d.ticket = c.take<uint32_t>(1);
+  d.vel_in = c.take<float>(3 * n);
+  d.smat = batch ? c.take<SceneMat>(m.smat.size()) : nullptr;
+  d.sstart = batch ? c.take<uint32_t>(m.sstart.size()) : nullptr;
+}
+
+// The setup sort's keys and values: four arrays of n u32 inside oF (9 n floats).
+static uint32_t* sort_array(const ModelHost& m, int k) {
+  return reinterpret_cast<uint32_t*>(m.oF) + static_cast<size_t>(k) * m.n;
+}
+
+// Makes the model's I/O arena and copies its input positions and velocities
+// into it (DMA when the caller's buffers are pinned), then waits, so the
+// caller may reuse its buffers on return and ckmpm_setup reads the inputs
+// from device memory.
 static cudaError_t stage_inputs(ckmpm_scene* s, ModelHost& m, const float* x, const float* v) {
   cudaError_t e = cudaSetDevice(s->desc.device);
-  if (e == cudaSuccess) e = cudaMalloc(&m.x_dev, sizeof(float) * 3 * static_cast<size_t>(m.n));
-  if (e == cudaSuccess) e = cudaMalloc(&m.v_dev, sizeof(float) * 3 * static_cast<size_t>(m.nv));
+  if (e != cudaSuccess) return e;
+  const bool track = m.mat.kind == kMixedKind || (s->desc.flags & CKMPM_FLAG_TRACK_IDS) != 0;
+  const int n = static_cast<int>(m.n);
+  cub::DoubleBuffer<uint32_t> keys(nullptr, nullptr), vals(nullptr, nullptr);
+  e = cub::DeviceRadixSort::SortPairs(nullptr, m.sort_temp_bytes, keys, vals, n, 0, 32, s->stream);
+  if (e == cudaSuccess && track)
+    e = cub::DeviceScan::ExclusiveSum(nullptr, m.oscan_bytes, static_cast<uint32_t*>(nullptr),
+                                      static_cast<uint32_t*>(nullptr), n, s->stream);
+  if (e != cudaSuccess) return e;
+  Carve size;
+  io_layout(m, track, size);
+  e = cudaMalloc(&m.io, size.off);
+  if (e != cudaSuccess) {
+    m.io = nullptr;
+    return e;
+  }
+  Carve place{m.io, 0};
+  io_layout(m, track, place);
+  if (!m.ev_copied) e = cudaEventCreateWithFlags(&m.ev_copied, cudaEventDisableTiming);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(m.x_dev, x, sizeof(float) * 3 * static_cast<size_t>(m.n), cudaMemcpyHostToDevice, s->stream);
+    e = cudaMemcpyAsync(m.ox, x, sizeof(float) * 3 * static_cast<size_t>(m.n), cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(m.v_dev, v, sizeof(float) * 3 * static_cast<size_t>(m.nv), cudaMemcpyHostToDevice, s->stream);
+    e = cudaMemcpyAsync(m.ov, v, sizeof(float) * 3 * static_cast<size_t>(m.nv), cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) {
-    cudaFree(m.x_dev);
-    cudaFree(m.v_dev);
-    m.x_dev = m.v_dev = nullptr;
+    cudaFree(m.io);
+    m.io = nullptr;
+    if (m.ev_copied) cudaEventDestroy(m.ev_copied);
+    m.ev_copied = nullptr;
   }
   return e;
 }
@@ -555,7 +655,6 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
   if (s->models.empty()) return fail(s, CKMPM_ERR_INVALID, "no models");
   CK_CUDA(s, cudaSetDevice(s->desc.device));
   const uint32_t nbd = s->sc.nblocks_domain;
-  uint32_t lost_at_setup = 0;
   // The grid's fixed-point unit: 2^-36 of the heaviest model's particle mass;
   // lighter models' sums are rescaled when they are added.  A batch uses each
   // scene's own mass (one model per scene).
@@ -578,83 +677,41 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     d.mass = m.mass;
     d.vol = m.vol;
     m.ntiles = (nbd + kCompactTile - 1) / kCompactTile;
-    const bool hasF = batch || material_has_F(m.mat.kind);
-    const bool hasAux = batch || material_has_aux(m.mat.kind);
-    const bool hasQ = batch ? std::count(m.skind.begin(), m.skind.end(), CKMPM_LINEAR) > 0 : m.mat.kind == CKMPM_LINEAR;
+    // All of the model's state in one allocation (one entry of s->allocs, so
+    // checkpoints copy it whole).
+    Carve size;
+    state_layout(m, nbd, track, size);
+    unsigned char* arena = nullptr;
+    CK_CUDA(s, dalloc(s, &arena, size.off));
+    Carve place{arena, 0};
+    state_layout(m, nbd, track, place);
     for (int b = 0; b < 2; ++b) {
-      StateDev& st = d.st[b];
-      for (int a = 0; a < 3; ++a) CK_CUDA(s, dalloc(s, &st.x[a], n));
-      for (int k = 0; k < 9; ++k) {
-        st.F[k] = nullptr;
-        if (hasF) CK_CUDA(s, dalloc(s, &st.F[k], n));
-      }
-      st.aux = nullptr;
-      if (hasAux) CK_CUDA(s, dalloc(s, &st.aux, n));
-      for (int k = 0; k < 9; ++k) {
-        st.Q[k] = nullptr;
-        if (hasQ) CK_CUDA(s, dalloc(s, &st.Q[k], n));
-      }
-      st.id = nullptr;
-      if (track) CK_CUDA(s, dalloc(s, &st.id, n));
-      BlockListDev& bl = d.bl[b];
-      CK_CUDA(s, dalloc(s, &bl.keys, d.cap_slots));
-      CK_CUDA(s, dalloc(s, &bl.start, d.cap_slots));
-      CK_CUDA(s, dalloc(s, &bl.count, d.cap_slots));
-      CK_CUDA(s, dalloc(s, &bl.table, nbd));
-      CK_CUDA(s, dalloc(s, &bl.prefix28, static_cast<size_t>(d.cap_slots) * 28));
-      CK_CUDA(s, dalloc(s, &bl.idx, n));
-      CK_CUDA(s, dalloc(s, &bl.nblocks, 1));
-      CK_CUDA(s, dalloc(s, &bl.nparticles, 1));
-      CK_CUDA(s, cudaMemsetAsync(bl.nblocks, 0, sizeof(uint32_t), s->stream));
-      CK_CUDA(s, cudaMemsetAsync(bl.nparticles, 0, sizeof(uint32_t), s->stream));
+      CK_CUDA(s, cudaMemsetAsync(d.bl[b].nblocks, 0, sizeof(uint32_t), s->stream));
+      CK_CUDA(s, cudaMemsetAsync(d.bl[b].nparticles, 0, sizeof(uint32_t), s->stream));
     }
-    CK_CUDA(s, dalloc(s, &d.dense_total, nbd));
     CK_CUDA(s, cudaMemsetAsync(d.dense_total, 0, sizeof(uint32_t) * nbd, s->stream));
-    CK_CUDA(s, dalloc(s, &d.tile_sums, 2 * static_cast<size_t>(m.ntiles)));
-    CK_CUDA(s, dalloc(s, &d.ticket, 1));
     CK_CUDA(s, cudaMemsetAsync(d.ticket, 0, sizeof(uint32_t), s->stream));
-    CK_CUDA(s, dalloc(s, &d.vel_in, 3 * static_cast<size_t>(n)));
-    d.smat = nullptr;
-    d.sstart = nullptr;
     if (batch) {
-      SceneMat* sm = nullptr;
-      uint32_t* ss = nullptr;
-      CK_CUDA(s, dalloc(s, &sm, m.smat.size()));
-      CK_CUDA(s, dalloc(s, &ss, m.sstart.size()));
-      CK_CUDA(s, cudaMemcpyAsync(sm, m.smat.data(), sizeof(SceneMat) * m.smat.size(), cudaMemcpyHostToDevice, s->stream));
-      CK_CUDA(s, cudaMemcpyAsync(ss, m.sstart.data(), sizeof(uint32_t) * m.sstart.size(), cudaMemcpyHostToDevice,
-                                 s->stream));
-      d.smat = sm;
-      d.sstart = ss;
+      CK_CUDA(s, cudaMemcpyAsync(const_cast<SceneMat*>(d.smat), m.smat.data(), sizeof(SceneMat) * m.smat.size(),
+                                 cudaMemcpyHostToDevice, s->stream));
+      CK_CUDA(s, cudaMemcpyAsync(const_cast<uint32_t*>(d.sstart), m.sstart.data(), sizeof(uint32_t) * m.sstart.size(),
+                                 cudaMemcpyHostToDevice, s->stream));
     }
 
-    // Upload, bin, radix-sort by colour-major block index, compact.
-    float *dx_in = m.x_dev, *dv_in = m.v_dev;
-    uint32_t *k_in = nullptr, *k_out = nullptr, *v_in = nullptr, *v_out = nullptr;
-    CK_CUDA(s, cudaMalloc(&k_in, sizeof(uint32_t) * n));
-    CK_CUDA(s, cudaMalloc(&k_out, sizeof(uint32_t) * n));
-    CK_CUDA(s, cudaMalloc(&v_in, sizeof(uint32_t) * n));
-    CK_CUDA(s, cudaMalloc(&v_out, sizeof(uint32_t) * n));
-    setup_bin_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(s->sc, n, dx_in, d.sstart, k_in, v_in, d.dense_total);
-    size_t temp_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, k_in, k_out, v_in, v_out, static_cast<int>(n), 0, 32,
-                                    s->stream);
-    void* temp = nullptr;
-    CK_CUDA(s, cudaMalloc(&temp, std::max<size_t>(temp_bytes, 1)));
-    CK_CUDA(s, cub::DeviceRadixSort::SortPairs(temp, temp_bytes, k_in, k_out, v_in, v_out, static_cast<int>(n), 0, 32,
+    // Bin, radix-sort by colour-major block index, compact; the inputs and the
+    // sort's arrays live in the model's I/O arena.  Nothing here waits for the
+    // device: kernels that depend on the binned count read it on the device.
+    cub::DoubleBuffer<uint32_t> keys(sort_array(m, 0), sort_array(m, 1)), vals(sort_array(m, 2), sort_array(m, 3));
+    setup_bin_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(s->sc, n, m.ox, d.sstart, keys.Current(), vals.Current(),
+                                                             d.dense_total);
+    size_t temp_bytes = m.sort_temp_bytes;
+    CK_CUDA(s, cub::DeviceRadixSort::SortPairs(m.sort_temp, temp_bytes, keys, vals, static_cast<int>(n), 0, 32,
                                                s->stream));
     CK_CUDA(s, launch_compact(s, m, d.bl[0]));
-    uint32_t counts[2] = {0, 0};
-    CK_CUDA(s, cudaMemcpyAsync(&counts[0], d.bl[0].nblocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
-    CK_CUDA(s, cudaMemcpyAsync(&counts[1], d.bl[0].nparticles, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
-    CK_CUDA(s, cudaStreamSynchronize(s->stream));
-    m.n_valid = counts[1];
-    lost_at_setup += n - m.n_valid;
     const float aux0 = initial_aux(m.mat);
-    if (m.n_valid > 0)
-      setup_gather_kernel<<<(m.n_valid + 255) / 256, 256, 0, s->stream>>>(
-          d, s->nstack, m.n_valid, v_out, dx_in, dv_in, m.nv, aux0,
-          (s->sc.rigid && m.mat.kind == CKMPM_VON_MISES) ? s->rigid_count : 0u);
+    setup_gather_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(
+        d, s->nstack, n, vals.Current(), m.ox, m.ov, m.nv, aux0,
+        (s->sc.rigid && m.mat.kind == CKMPM_VON_MISES) ? s->rigid_count : 0u, d.bl[0].nparticles);
     // Identity previous-step structures in list 1.
     CK_CUDA(s, cudaMemcpyAsync(d.bl[1].table, d.bl[0].table, sizeof(int32_t) * nbd, cudaMemcpyDeviceToDevice,
                                s->stream));
@@ -667,17 +724,10 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
     CK_CUDA(s, cudaMemcpyAsync(d.bl[1].nblocks, d.bl[0].nblocks, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s->stream));
     CK_CUDA(s, cudaMemcpyAsync(d.bl[1].nparticles, d.bl[0].nparticles, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                                s->stream));
-    if (counts[0] > 0) setup_identity_kernel<<<counts[0], 256, 0, s->stream>>>(d.bl[0], d.bl[1]);
+    setup_identity_kernel<<<s->sm_count * 4, 256, 0, s->stream>>>(d.bl[0], d.bl[1]);
+    // Particles outside the domain are dropped at binning and counted.
+    count_lost_kernel<<<1, 32, 0, s->stream>>>(s->scal, n, d.bl[0].nparticles);
     CK_CUDA(s, cudaGetLastError());
-    CK_CUDA(s, cudaStreamSynchronize(s->stream));
-    cudaFree(dx_in);
-    cudaFree(dv_in);
-    m.x_dev = m.v_dev = nullptr;
-    cudaFree(k_in);
-    cudaFree(k_out);
-    cudaFree(v_in);
-    cudaFree(v_out);
-    cudaFree(temp);
   }
   // Initial grid: every model deposits mass and momentum into grid[0], epoch 0;
   // then the blocks substep 0 deposits into are zeroed in grid[1] (epoch 1).
@@ -692,14 +742,20 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
   CK_CUDA(s, launch_zero(s, 0, 1, 1));
   // The scalars were zeroed at creation; setup's kernels may have raised status
   // bits in them, which ckmpm_setup then reports.
-  finish_setup_kernel<<<1, 32, 0, s->stream>>>(s->scal, lost_at_setup, s->rigid_v[0], s->rigid_v[1], s->rigid_v[2]);
+  finish_setup_kernel<<<1, 32, 0, s->stream>>>(s->scal, 0u, s->rigid_v[0], s->rigid_v[1], s->rigid_v[2]);
   CK_CUDA(s, cudaGetLastError());
+  // The one wait of setup: the status word and each model's binned count.
+  std::vector<uint32_t> binned(s->models.size(), 0u);
+  for (size_t i = 0; i < s->models.size(); ++i)
+    CK_CUDA(s, cudaMemcpyAsync(&binned[i], s->models[i].dev.bl[0].nparticles, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                               s->stream));
+  Scalars r{};
+  CK_CUDA(s, cudaMemcpyAsync(&r, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
   CK_CUDA(s, cudaStreamSynchronize(s->stream));
+  for (size_t i = 0; i < s->models.size(); ++i) s->models[i].n_valid = binned[i];
   s->setup_done = true;
   s->host_step = 0;
   s->n_state_allocs = s->allocs.size();
-  Scalars r{};
-  CK_CUDA(s, cudaMemcpy(&r, s->scal, sizeof(Scalars), cudaMemcpyDeviceToHost));
   return status_from(s, r);
 }
 
@@ -856,29 +912,11 @@ ckmpm_status ckmpm_get_count(ckmpm_scene* s, int32_t model, uint32_t* n_live) {
   return CKMPM_OK;
 }
 
-// Export buffers of one model, allocated on first use (each one that is still
-// missing, so a call after a failed allocation completes the set).
-static cudaError_t ensure_export_buffers(ckmpm_scene* s, ModelHost& m) {
-  const size_t cap_p = m.dev.cap_particles;
-  cudaError_t e = cudaSuccess;
-  if (!m.ox && (e = dalloc(s, &m.ox, 3 * cap_p)) != cudaSuccess) return e;
-  if (!m.ov && (e = dalloc(s, &m.ov, 3 * cap_p)) != cudaSuccess) return e;
-  if (!m.oF && (e = dalloc(s, &m.oF, 9 * cap_p)) != cudaSuccess) return e;
-  if (!m.oaux && (e = dalloc(s, &m.oaux, cap_p)) != cudaSuccess) return e;
-  if (!m.oid && (e = dalloc(s, &m.oid, cap_p)) != cudaSuccess) return e;
-  if (m.dev.track_ids) {
-    if (!m.oflag && (e = dalloc(s, &m.oflag, cap_p)) != cudaSuccess) return e;
-    if (!m.opos && (e = dalloc(s, &m.opos, cap_p)) != cudaSuccess) return e;
-    if (!m.oscan) {
-      if ((e = cub::DeviceScan::ExclusiveSum(nullptr, m.oscan_bytes, m.oflag, m.opos, static_cast<int>(cap_p),
-                                             s->stream)) != cudaSuccess)
-        return e;
-      unsigned char* t = nullptr;
-      if ((e = dalloc(s, &t, m.oscan_bytes)) != cudaSuccess) return e;
-      m.oscan = t;
-    }
-  }
-  return cudaSuccess;
+// Export buffers of one model: part of its I/O arena (ckmpm_add_model).
+static cudaError_t ensure_export_buffers(ckmpm_scene*, ModelHost& m) {
+  return (m.ox && m.ov && m.oF && m.oaux && m.oid && (!m.dev.track_ids || (m.oflag && m.opos && m.oscan)))
+             ? cudaSuccess
+             : cudaErrorInvalidValue;
 }
 
 // Enqueues the gather of the requested per-particle arrays into the model's
@@ -944,15 +982,7 @@ ckmpm_status ckmpm_export_positions_async(ckmpm_scene* s, int32_t model, float* 
   const uint32_t n_upper = m.n_valid;
   if (cap < n_upper) return fail(s, CKMPM_ERR_NOT_FOUND, "output capacity too small");
   CK_CUDA(s, cudaSetDevice(s->desc.device));
-  if (!s->copy_stream) {
-    CK_CUDA(s, cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
-    CK_CUDA(s, cudaEventCreateWithFlags(&s->ev_probe, cudaEventDisableTiming));
-    CK_CUDA(s, cudaEventCreateWithFlags(&s->ev_copy, cudaEventDisableTiming));
-    CK_CUDA(s, cudaMallocHost(&s->export_count, sizeof(uint32_t)));
-    *s->export_count = 0;
-  }
   CK_CUDA(s, ensure_export_buffers(s, m));
-  if (!m.ev_copied) CK_CUDA(s, cudaEventCreateWithFlags(&m.ev_copied, cudaEventDisableTiming));
   const uint32_t* n_dev = m.dev.bl[s->host_step & 1].nparticles;
   CK_CUDA(s, enqueue_export(s, m, true, false, false, false, false, n_upper, n_dev));
   CK_CUDA(s, cudaEventRecord(s->ev_probe, s->stream));
@@ -1009,6 +1039,33 @@ ckmpm_status ckmpm_get_blocks_in(ckmpm_scene* s, uint32_t scene, int32_t model, 
     }
     for (uint32_t i = 0; i < nb; ++i)
       if (static_cast<uint32_t>(hk[i].w) == scene) set[std::make_tuple(hk[i].x, hk[i].y, hk[i].z)] += hc[i];
+    if (step == 0 && nb) {
+      // Right after setup the reference's partition also holds the blocks of
+      // each particle's cell on the +dx/4 grid, (int(x/dx - 1/4) - 2) / 4
+      // (ActivateBlocksWithParticles inserts both staggered grids' blocks,
+      // include/mpm_algorithm.cuh:713-736); they hold no particles.  The
+      // first rebinning keeps only blocks with particles, as here.
+      std::vector<uint32_t> hs(nb);
+      CK_CUDA(s, cudaMemcpy(hs.data(), cur.start, sizeof(uint32_t) * nb, cudaMemcpyDeviceToHost));
+      const StateDev& st = s->models[mi].dev.st[0];
+      const uint32_t np = s->models[mi].n_valid;
+      std::vector<float> hx[3];
+      for (int a = 0; a < 3; ++a) {
+        hx[a].resize(np);
+        if (np) CK_CUDA(s, cudaMemcpy(hx[a].data(), st.x[a], sizeof(float) * np, cudaMemcpyDeviceToHost));
+      }
+      const float inv_dx = s->sc.inv_dx;
+      for (uint32_t i = 0; i < nb; ++i) {
+        if (static_cast<uint32_t>(hk[i].w) != scene) continue;
+        for (uint32_t p = hs[i]; p < hs[i] + hc[i] && p < np; ++p) {
+          int b[3];
+          for (int a = 0; a < 3; ++a) b[a] = (static_cast<int>(std::fma(hx[a][p], inv_dx, -0.25f)) - 2) / 4;
+          if (b[0] >= 0 && b[1] >= 0 && b[2] >= 0 && b[0] < s->sc.dims[0] && b[1] < s->sc.dims[1] &&
+              b[2] < s->sc.dims[2])
+            set.emplace(std::make_tuple(b[0], b[1], b[2]), 0u);
+        }
+      }
+    }
   }
   if (which >= 1) {
     const int lo = which == 1 ? 0 : -1;
@@ -1232,13 +1289,11 @@ ckmpm_status ckmpm_destroy(ckmpm_scene* s) {
     cudaStreamDestroy(s->copy_stream);
     cudaEventDestroy(s->ev_probe);
     cudaEventDestroy(s->ev_copy);
-    cudaFreeHost(s->export_count);
-    for (auto& m : s->models)
-      if (m.ev_copied) cudaEventDestroy(m.ev_copied);
   }
-  for (auto& m : s->models) {  // inputs of a scene that never ran ckmpm_setup
-    if (m.x_dev) cudaFree(m.x_dev);
-    if (m.v_dev) cudaFree(m.v_dev);
+  if (s->export_count) cudaFreeHost(s->export_count);
+  for (auto& m : s->models) {
+    if (m.io) cudaFree(m.io);
+    if (m.ev_copied) cudaEventDestroy(m.ev_copied);
   }
   free_graphs(s);
   for (auto& p : s->allocs) cudaFree(p.first);

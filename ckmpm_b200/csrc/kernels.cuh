@@ -1262,11 +1262,13 @@ __global__ void setup_bin_kernel(SceneDev sc, uint32_t n, const float* __restric
 // J0 or the rigid flag (0 for the first rigid_count input particles, else
 // aux0 = 1), id = input index, velocities gathered for the rasterisation
 // (include/mpm_algorithm.cuh:974-1081).
+// n bounds the binned count; n_dev, when given, is the binned count on the
+// device (setup launches before it is known on the host).
 __global__ void setup_gather_kernel(ModelDev md, uint32_t nstack, uint32_t n, const uint32_t* __restrict__ perm,
                                     const float* __restrict__ x, const float* __restrict__ v, uint32_t nv, float aux0,
-                                    uint32_t rigid_count) {
+                                    uint32_t rigid_count, const uint32_t* __restrict__ n_dev = nullptr) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || (n_dev && i >= *n_dev)) return;
   const uint32_t s = perm[i];
   StateDev st = md.st[0];
   st.x[0][i] = x[3 * s];
@@ -1291,12 +1293,20 @@ __global__ void setup_gather_kernel(ModelDev md, uint32_t nstack, uint32_t n, co
 // Identity "previous step" for the first substep: every particle stays in
 // its block (direction 13), index list = in-block position
 // (include/mpm_algorithm.cuh:950-964 InitializeAdvectionBucket).
+// One CTA per block of the list, grid-strided (the block count is read on the
+// device).
 __global__ void setup_identity_kernel(BlockListDev cur, BlockListDev prev) {
-  const uint32_t slot = blockIdx.x;
-  if (slot >= *cur.nblocks) return;
-  const uint32_t n = cur.count[slot], start = cur.start[slot];
-  if (threadIdx.x < 28) prev.prefix28[slot * 28 + threadIdx.x] = threadIdx.x <= 13 ? 0u : n;
-  for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) prev.idx[start + q] = static_cast<uint16_t>(q);
+  const uint32_t nb = *cur.nblocks;
+  for (uint32_t slot = blockIdx.x; slot < nb; slot += gridDim.x) {
+    const uint32_t n = cur.count[slot], start = cur.start[slot];
+    if (threadIdx.x < 28) prev.prefix28[slot * 28 + threadIdx.x] = threadIdx.x <= 13 ? 0u : n;
+    for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) prev.idx[start + q] = static_cast<uint16_t>(q);
+  }
+}
+
+// Setup: the particles of a model that binning dropped (outside the domain).
+__global__ void count_lost_kernel(Scalars* scal, uint32_t n, const uint32_t* __restrict__ binned) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) scal->lost += n - *binned;
 }
 
 // ------------------------------------------------------------------ probe / export

@@ -22,8 +22,10 @@
 //  * Constitutive: fixed-corotated (mpm_algorithm.cuh:193-254, mpm_material.cuh:320-357),
 //    Drucker-Prager StVK-Hencky with sin(phi)=0.5 (mpm_algorithm.cuh:261-327,
 //    mpm_material.cuh:362-464), J-fluid (mpm_algorithm.cuh:528-569, mpm_material.cuh:468-477).
-//  * P2G: A = C m - dt_next V (D_new/2)^-1 tau; m_i += w m; mv_i += w (m v + A (x_i - x_p))
-//    (mpm_algorithm.cuh:1687-1792).
+//  * P2G: A = C m - dt_next V M tau with M = (1/2 (D_old + D_new))^-1, D_old the G2P D of the
+//    old position (the reference never resets D between its G2P and P2G loops and inverts
+//    half the sum, mpm_algorithm.cuh:1524,1604,1729-1736); m_i += w m;
+//    mv_i += w (m v + A (x_i - x_p)) (mpm_algorithm.cuh:1687-1792).
 //  * A particle whose new cell leaves the (1..6) window of its block is skipped in P2G
 //    (mpm_algorithm.cuh:1670-1683); block of a particle = (int(x/dx + 1/4) - 2) / 4
 //    (mpm_algorithm.cuh:595-600, mpm_particle.cuh:337-340).
@@ -938,9 +940,25 @@ int oracle_get_blocks(void* h, int model, int which, int32_t* keys, uint32_t* co
     }
   }
   std::unordered_map<int64_t, uint32_t> set = pb;
+  if (s->steps == 0) {
+    // Right after setup the partition also holds the block of each particle's
+    // cell on the +dx/4 grid (ActivateBlocksWithParticles activates both
+    // staggered grids' blocks, mpm_algorithm.cuh:713-736), with no particles.
+    for (int mi = 0; mi < static_cast<int>(s->models.size()); ++mi) {
+      if (model >= 0 && mi != model) continue;
+      const Model& m = s->models[mi];
+      for (int p = 0; p < m.n; ++p) {
+        if (!m.alive[p]) continue;
+        int K[3];
+        for (int a = 0; a < 3; ++a) K[a] = trunc_div4(static_cast<int>(m.x[3 * p + a] * invdx - 0.25) - 2);
+        if (in_domain(*s, K[0], K[1], K[2])) set.emplace(flat_key(*s, K[0], K[1], K[2]), 0u);
+      }
+    }
+  }
   if (which >= 1) {
     const int lo = which == 1 ? 0 : -1;
-    for (auto& kv : pb) {
+    const std::unordered_map<int64_t, uint32_t> na = set;
+    for (auto& kv : na) {
       const int64_t k = kv.first;
       const int bz = static_cast<int>(k % s->d.dims[2]);
       const int by = static_cast<int>((k / s->d.dims[2]) % s->d.dims[1]);

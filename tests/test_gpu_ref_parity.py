@@ -1,0 +1,202 @@
+"""The CUDA engine against the reference CUDA build run live on the same seeded inputs, at the
+benchmark scenes the reference harness covers: the jelly cube (16,795 particles, fixed-corotated,
+sticky walls, dt = 1e-4, 1000 substeps) and the sand column (1,686,824 particles, Drucker-Prager
+on a slip floor, dt = 5e-5, 500 substeps).
+
+The reference runs through its own MPMEngine (Initialize -> InitializeParticle -> InitialSetup ->
+Simulate, oracle/_ref built from its headers by oracle/Makefile); its state after K substeps is
+read from its partition and particle buckets, with particle ids carried along its own advection
+records (oracle/ref_harness.cu, mode 2).
+
+Integer contract (binning and the block table), checked exactly:
+  * the reference's block of every particle equals the binning formula of its position
+    ((int(x/dx + 1/4) - 2) / 4, include/mpm_particle.cuh:337-340), and so does the engine's;
+  * its NA keys are the blocks holding particles (at setup also the blocks of the +dx/4 grid
+    cells, ActivateBlocksWithParticles, include/mpm_algorithm.cuh:713-736), NN and NE their
+    {0,1}^3 and {-1,0,1}^3 neighbours clipped to the domain (:658-695);
+  * the engine's NA / NN / NE key sets, per-block counts and per-block id sets equal the
+    reference's at setup and after 1 and 10 substeps; later, wherever a particle's block
+    differs the two positions straddle a block face within the float tolerance.
+Float contract: the reference's P2G sums with float atomics, so two runs of it differ; x, v, F
+(and logJp for the sand) of the engine must lie within a few times that run-to-run spread of
+the reference, with a floor (the tolerances are stated at FLOAT_TOL).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from ckmpm_b200 import Scene, scenes
+
+pytestmark = pytest.mark.gpu
+
+# (workload, reference harness family, substeps at which both sides are compared)
+CASES = {
+    "jelly_cube": ("jelly", [0, 1, 10, 100, 1000]),
+    "sand_column": ("sand", [0, 1, 10, 100, 500]),
+}
+EARLY = (0, 1, 10)  # substep counts at which every integer output must agree exactly
+
+# Engine-vs-reference error allowed at each compared substep count, per quantity:
+# max |engine - reference| <= max(SPREAD_FACTOR * (max |reference run 2 - reference run 1|), floor).
+# Floors: x absolute (positions in a unit domain), v relative to the largest |v| of the scene,
+# F absolute (|F| ~ 1), logJp absolute.
+SPREAD_FACTOR = 4.0
+FLOAT_TOL = {"x": 1e-5, "v": 1e-4, "F": 1e-4, "aux": 1e-4}
+X_TOL_BLOCK = 1e-5  # position difference allowed for a particle binned into another block
+
+
+def _ref():
+    from oracle import ref_runner
+    return ref_runner
+
+
+def block_of(x: np.ndarray, inv_dx: float, shift: float = 0.25) -> np.ndarray:
+    """(int(x * inv_dx + shift) - 2) / 4 per axis with C truncation, in float32 as the reference
+    computes it (inv_dx is a power of two, so the product is exact and fused or not, the sum
+    rounds once)."""
+    c = (x.astype(np.float32) * np.float32(inv_dx) + np.float32(shift)).astype(np.int64)
+    q = c - 2
+    return np.where(q < 0, -((-q) // 4), q // 4).astype(np.int32)
+
+
+def expand(keys: np.ndarray, lo: int, dims) -> np.ndarray:
+    """keys plus their {lo..1}^3 neighbours inside the domain, sorted and unique."""
+    off = np.array([(i, j, k) for i in range(lo, 2) for j in range(lo, 2) for k in range(lo, 2)], np.int32)
+    allk = (keys[:, None, :] + off[None, :, :]).reshape(-1, 3)
+    ok = np.all((allk >= 0) & (allk < np.asarray(dims, np.int32)), axis=1)
+    return np.unique(np.concatenate([keys, allk[ok]]), axis=0)
+
+
+def sorted_keys(k: np.ndarray) -> np.ndarray:
+    return np.unique(np.asarray(k, np.int32).reshape(-1, 3), axis=0)
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def run(request, engine_lib):
+    ref = _ref()
+    name = request.param
+    family, ks = CASES[name]
+    if not ref.available(family):
+        pytest.skip(f"oracle/_ref/ref_{family} is not built (make -C oracle ref)")
+    cfg, models = scenes.WORKLOADS[name](track_ids=True)
+    dt = cfg.dt
+    a = ref.dump(family, models, dt, ks)
+    b = ref.dump(family, models, dt, ks)
+    s = Scene(cfg)
+    s.add_model(models[0])
+    s.setup()
+    ours = {}
+    done = 0
+    for k in ks:
+        if k > done:
+            s.step(k - done, dt)
+            done = k
+        st = s.state(0)
+        ours[k] = {"state": st, "blocks": [s.blocks(0, w) for w in (0, 1, 2)]}
+    s.close()
+    return {"name": name, "cfg": cfg, "ks": ks, "a": a, "b": b, "ours": ours}
+
+
+def test_reference_binning_is_the_formula(run):
+    """The reference's own block of each particle, and its NA / NN / NE construction, are the rule
+    the engine implements: checked on the reference's dumps at every compared substep."""
+    cfg = run["cfg"]
+    dims = cfg.domain_blocks
+    for k in run["ks"]:
+        d = run["a"][k]
+        m = d["models"][0]
+        assert np.array_equal(m["block"], block_of(m["x"], 1.0 / cfg.dx)), k
+        pb = sorted_keys(m["block"])
+        na = sorted_keys(d["keys"][:d["na"]])
+        if k == 0:  # InitialSetup activates the blocks of both staggered grids' cells
+            pb = np.unique(np.concatenate([pb, block_of(m["x"], 1.0 / cfg.dx, -0.25)]), axis=0)
+        assert np.array_equal(na, pb), k
+        assert np.array_equal(sorted_keys(d["keys"][:d["nn"]]), expand(na, 0, dims)), k
+        assert np.array_equal(sorted_keys(d["keys"][:d["ne"]]), expand(na, -1, dims)), k
+        # per-block counts are the particles binned into each block
+        keys = d["keys"][:d["na"]]
+        u, c = np.unique(m["block"], axis=0, return_counts=True)
+        cnt = dict(zip(map(tuple, u), c))
+        assert all(int(d["counts"][0][i]) == cnt.get(tuple(keys[i]), 0) for i in range(d["na"])), k
+
+
+def _compare_integers(cfg, d, o, k):
+    """Engine vs reference at one substep count: (number of particles whose block differs,
+    whether the key sets and counts are identical)."""
+    m = d["models"][0]
+    st = o["state"]
+    assert np.array_equal(st.id, m["id"]), "the two sides hold different particles"
+    bo = block_of(st.x, 1.0 / cfg.dx)
+    # the engine is self-consistent: its NA keys and counts are the blocks of its particles
+    kg, cg = o["blocks"][0]
+    u, c = np.unique(bo, axis=0, return_counts=True)
+    if k == 0:
+        extra = block_of(st.x, 1.0 / cfg.dx, -0.25)
+        allk = np.unique(np.concatenate([u, extra]), axis=0)
+        cc = dict(zip(map(tuple, u), c))
+        assert np.array_equal(kg, allk)
+        assert np.array_equal(cg, np.array([cc.get(tuple(t), 0) for t in allk], np.uint32))
+    else:
+        assert np.array_equal(kg, u) and np.array_equal(cg, c.astype(np.uint32))
+    differ = np.any(bo != m["block"], axis=1)
+    same_sets = True
+    ref_sets = [sorted_keys(d["keys"][:d[w]]) for w in ("na", "nn", "ne")]
+    for w in range(3):
+        same_sets &= np.array_equal(o["blocks"][w][0], ref_sets[w])
+    keys = d["keys"][:d["na"]]
+    order = np.lexsort(keys.T[::-1])
+    same_sets &= np.array_equal(o["blocks"][0][1], d["counts"][0][order])
+    return int(differ.sum()), bool(same_sets), differ
+
+
+def test_block_sets_match_reference(run):
+    cfg = run["cfg"]
+    rows = []
+    for k in run["ks"]:
+        d, o = run["a"][k], run["ours"][k]
+        ndiff, same, differ = _compare_integers(cfg, d, o, k)
+        dx = (float(np.abs(o["state"].x[differ].astype(np.float64) - d["models"][0]["x"][differ]).max())
+              if ndiff else 0.0)
+        rows.append((k, ndiff, same, dx))
+        ref_diff = int(np.any(run["b"][k]["models"][0]["block"] != d["models"][0]["block"], axis=1).sum())
+        print(f"{run['name']} K={k}: NA {d['na']} NN {d['nn']} NE {d['ne']}; identical sets and counts: {same}; "
+              f"particles in another block: {ndiff} (largest position difference among them {dx:.2e}); "
+              f"between two reference runs: {ref_diff}")
+    for k, ndiff, same, dx in rows:
+        if k in EARLY:
+            assert ndiff == 0 and same, (k, ndiff)
+        # every disagreement is a float position difference across a block face
+        assert ndiff > 0 or same, f"K={k}: every particle is in the same block but the key sets differ"
+        assert dx <= X_TOL_BLOCK, (k, dx)
+
+
+def _errors(p, q, scale_v):
+    d = {"x": np.abs(p["x"].astype(np.float64) - q["x"]).max(axis=1),
+         "v": np.abs(p["v"].astype(np.float64) - q["v"]).max(axis=1) / scale_v,
+         "F": np.abs(p["F"].astype(np.float64) - q["F"]).reshape(len(q["F"]), -1).max(axis=1),
+         "aux": np.abs(p["aux"].astype(np.float64) - q["aux"])}
+    return {k: (float(v.max()), float(np.quantile(v, 0.999))) for k, v in d.items()}
+
+
+def test_state_within_reference_spread(run):
+    name = run["name"]
+    rows = []
+    for k in run["ks"]:
+        ma, mb = run["a"][k]["models"][0], run["b"][k]["models"][0]
+        st = run["ours"][k]["state"]
+        assert np.array_equal(ma["id"], mb["id"]) and np.array_equal(ma["id"], st.id)
+        scale_v = max(float(np.abs(ma["v"]).max()), 1e-6)
+        ours = {"x": st.x, "v": st.v, "F": st.F.reshape(-1, 3, 3), "aux": st.aux}
+        if name == "jelly_cube":
+            ours["aux"] = np.zeros_like(st.aux)  # fixed-corotated keeps no scalar
+        spread = _errors(mb, ma, scale_v)
+        err = _errors(ours, ma, scale_v)
+        rows.append((k, err, spread))
+        print(f"{name} K={k}: |v|max {scale_v:.3e}; engine vs reference (max / 99.9 %) "
+              + " ".join(f"{q} {err[q][0]:.2e}/{err[q][1]:.2e}" for q in err) + "; reference run to run "
+              + " ".join(f"{q} {spread[q][0]:.2e}/{spread[q][1]:.2e}" for q in spread))
+    for k, err, spread in rows:
+        for q in err:
+            bound = max(SPREAD_FACTOR * spread[q][0], FLOAT_TOL[q])
+            assert err[q][0] <= bound, (name, k, q, err[q], bound)
