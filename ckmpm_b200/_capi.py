@@ -14,6 +14,7 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libckmpm_b200.so"
 
 CKMPM_OK = 0
+CKMPM_ERR_INVALID = 1
 STATUS_NAMES = {
     0: "CKMPM_OK",
     1: "CKMPM_ERR_INVALID",

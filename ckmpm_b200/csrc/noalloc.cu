@@ -1,18 +1,24 @@
 // ckmpm_simulate_noalloc: the one entry point of this library that allocates
 // no memory at all.
 //
-// Some callers cannot call cudaMalloc: code that runs while another framework
-// is capturing a CUDA graph on the stream (an allocation there is illegal or
-// breaks the capture), plugins hosted by runtimes that own the whole device
-// memory budget through their own pool, and real-time loops that cannot
-// afford the device-wide synchronisation a cudaMalloc / cudaFree may cause.
-// For them this entry point runs a complete small simulation -- setup and
-// nsteps substeps of one model -- with every piece of scratch memory (grid,
-// block tables, index lists, sort buffers, work counters, flags) taken from
-// one file-scope __device__ array of fixed size.  The caller passes its inputs
-// and outputs as device pointers.  The same kernels as the allocating path run
-// in the same order, so the outputs match ckmpm_create / ckmpm_add_model /
-// ckmpm_setup / ckmpm_step / ckmpm_get_state on the same inputs.
+// Some callers cannot call cudaMalloc: plugins hosted by runtimes that own the
+// whole device memory budget through their own pool (an allocation behind the
+// pool's back can fail or push the host over its limit), and loops that
+// cannot afford the device-wide synchronisation a cudaMalloc / cudaFree may
+// cause.  For them this entry point runs a complete small simulation -- setup
+// and nsteps substeps of one model -- with every piece of scratch memory
+// (grid, block tables, index lists, sort buffers, work counters, flags) taken
+// from one file-scope __device__ array of fixed size.  The caller passes its
+// inputs and outputs as device pointers.  The same kernels as the allocating
+// path run in the same order, so the outputs match ckmpm_create /
+// ckmpm_add_model / ckmpm_setup / ckmpm_step / ckmpm_get_state on the same
+// inputs.
+//
+// The call waits for its own work: it reads the binned and live particle
+// counts back to the host and synchronises the caller's stream three times.
+// So it cannot be recorded into a CUDA graph: on a stream that is capturing it
+// returns CKMPM_ERR_INVALID before enqueuing anything, and the capture stays
+// valid.
 //
 // Limits: one model of at most kNoAllocMaxParticles particles in a domain of
 // at most kNoAllocMaxDomainBlocks 4^3-cell blocks; the array takes
@@ -56,11 +62,13 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 unsigned char* g_na_base[kNoAllocMaxDevices] = {};
 int g_na_ctas[kNoAllocMaxDevices] = {};
+std::mutex g_na_mutex;  // host threads making a first call at the same time
 
 // Per-device set-up, done by the first call on each device with that device
 // current: the device address of the scratch array and the persistent grid size.
 cudaError_t na_base(int device, unsigned char** base, int* ctas) {
   if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_na_mutex);
   if (!g_na_base[device]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -172,11 +180,19 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
     int d;
     ~Restore() { cudaSetDevice(d); }
   } restore{prev_device};
+  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+  // The call synchronises its stream and reads counts back to the host, which a
+  // stream capture cannot record: refuse before enqueuing anything.
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &capture) != cudaSuccess)
+    return na_fail(message, CKMPM_ERR_CUDA, "cudaStreamIsCapturing failed");
+  if (capture != cudaStreamCaptureStatusNone)
+    return na_fail(message, CKMPM_ERR_INVALID,
+                   "the stream is capturing a CUDA graph; this call synchronises its stream and cannot be captured");
   unsigned char* base = nullptr;
   int ctas = 0;
   if (na_base(desc->device, &base, &ctas) != cudaSuccess)
     return na_fail(message, CKMPM_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
-  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
   const uint32_t nbd = static_cast<uint32_t>(nbd64);
 
   // Scene constants, as ckmpm_create computes them.

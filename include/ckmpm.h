@@ -244,14 +244,16 @@ ckmpm_status ckmpm_debug_constitutive(const ckmpm_material* material, uint32_t n
  * model -- setup and nsteps substeps, the same kernels in the same order as
  * ckmpm_create / ckmpm_add_model / ckmpm_setup / ckmpm_step / ckmpm_get_state
  * -- without allocating any memory, for callers that cannot call cudaMalloc:
- * code running while another framework captures a CUDA graph on the stream,
- * plugins whose host runtime owns the device memory budget, and real-time
- * loops that cannot take the device-wide synchronisation of an allocation.
- * All scratch lives in one fixed __device__ array of 53.1 MB that every GPU
- * loading this library keeps until exit; limits: n <= 65536 particles and at
- * most 4096 blocks in the domain (e.g. 16^3), else CKMPM_ERR_CAPACITY.  The
- * first call on a device looks up the array's device address, so make that
- * first call before any stream capture.  x, v (nv = 1 or n float3) and the
+ * plugins whose host runtime owns the device memory budget through its own
+ * pool, and loops that cannot take the device-wide synchronisation of an
+ * allocation.  All scratch lives in one fixed __device__ array of 53.1 MB,
+ * part of this library's device code, that every GPU loading this library
+ * keeps until exit; limits: n <= 65536 particles and at most 4096 blocks in
+ * the domain (e.g. 16^3), else CKMPM_ERR_CAPACITY.  The first call on a device
+ * looks up the array's device address (thread-safe).  The call waits for its
+ * own work (it synchronises cuda_stream and reads counts back to the host), so
+ * it cannot be captured into a CUDA graph: on a capturing stream it returns
+ * CKMPM_ERR_INVALID without enqueuing anything.  x, v (nv = 1 or n float3) and the
  * outputs x_out, v_out (3n), F_out (9n), aux_out (n) are DEVICE pointers in
  * input order (outputs may be NULL; particles lost at the domain edge read
  * NaN).  Materials: every kind but the linear model (which keeps a stored
