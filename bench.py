@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--profile-steps", type=int, default=200)
     ap.add_argument("--e2e-frame", type=int, default=100, help="substeps between position exports in the e2e run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-subrecords", action="store_true",
+                    help="headline line only (no bounded records of the jelly cube, batched and differentiable forms)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sand_column")
     ap.add_argument("--ncu-case", action="store_true",
@@ -496,14 +498,17 @@ def run_batched(args, rank, world, local_rank):
 
     looped = None
     if world == 1:
-        # The plain path over the same scenes, one after another on one stream.
-        loop_steps = min(args.steps, 64)
+        # The plain path over the same scenes, one after another on one stream,
+        # each at the launch shape the autotuner picks for it, over as many
+        # substeps as the batch was timed over.
+        loop_steps = args.steps
         plain = []
         for m in sub:
             s = Scene(cfg)
             s.set_stream(stream.cuda_stream)
             s.add_model(m)
             s.setup()
+            s.autotune(16, dt)
             s.step(8, dt)
             plain.append(s)
         torch.cuda.synchronize()
@@ -521,17 +526,16 @@ def run_batched(args, rank, world, local_rank):
         lv = n_plain * loop_steps / (lms / 1e3)
         looped = {"value": lv, "unit": METRIC, "steps": loop_steps, "ms_per_step": lms / loop_steps,
                   "speedup_of_batched": value / lv,
-                  "how": "each scene through ckmpm_create/ckmpm_step_async (graphs of 8 substeps), scenes in turn "
-                         "on one stream, device time of the whole loop"}
+                  "how": "each scene through ckmpm_create / ckmpm_autotune / ckmpm_step_async (CUDA graphs at its "
+                         "autotuned launch shape), scenes in turn on one stream, device time of the whole loop over "
+                         "the batch's substep count"}
 
     # End to end through the public API with host buffers (the export buffer is
     # pinned host memory, allocated before the timed region).
     xb_t = torch.zeros((sum(len(m.particle_position) for m in sub), 3), dtype=torch.float32).pin_memory()
     xb = xb_t.numpy()
     torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    t_e2e = time.perf_counter()
     b2 = SceneBatch(cfg, sub)
     b2.set_stream(stream.cuda_stream)
     b2.setup()
@@ -544,15 +548,15 @@ def run_batched(args, rank, world, local_rank):
         exports += 1
         done += k
     b2.export_wait()
-    e1.record(stream)
-    e1.synchronize()
-    e2e_ms, _ = reduce_over_ranks(e0.elapsed_time(e1), 0.0)
+    torch.cuda.synchronize()
+    e2e_ms, _ = reduce_over_ranks((time.perf_counter() - t_e2e) * 1e3, 0.0)
     b2.close()
     n_in = sum(len(m.particle_position) for m in sub)
     e2e = {"value": total_live * args.steps / (e2e_ms / 1e3), "unit": METRIC,
            "h2d_bytes_per_step": n_in * 24 / args.steps,
            "d2h_bytes_per_step": exports * (n_in * 12 + 4 + 64) / args.steps,
-           "includes": "batch construction and setup (upload of x, v; binning; initial grid); frames of "
+           "includes": "host clock from before ckmpm_create_batch to the last export landing: batch construction "
+                       "and setup (upload of x, v; binning; initial grid); frames of "
                        f"{args.e2e_frame} substeps, each followed by the status read and a position export in "
                        "input order (gathered on the compute stream, copied to pinned host memory on a second "
                        "stream while the next frame runs; the last one waited for)"}
@@ -656,13 +660,11 @@ def run_ours(args, rank, world, local_rank):
     models_h = [dataclasses.replace(m, particle_position=pin(m.particle_position),
                                     particle_velocity=pin(m.particle_velocity)) for m in models]
     xbufs = [pin(np.zeros((len(m.particle_position), 3), np.float32)) for m in models]
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter()
     s2 = Scene(cfg)
     s2.set_stream(stream.cuda_stream)
     s2.set_tuning(tuning["threads"], tuning["ctas_per_sm"], tuning["graph_chunk"])
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
     for m in models_h:
         s2.add_model(m)
     s2.setup()
@@ -676,9 +678,8 @@ def run_ours(args, rank, world, local_rank):
         exports += 1
         done += k
     s2.export_wait()
-    e1.record(stream)
-    e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t_e2e) * 1e3
     if world > 1:
         t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -687,7 +688,8 @@ def run_ours(args, rank, world, local_rank):
     e2e = {"value": world * n_live * args.steps / (e2e_ms / 1e3), "unit": METRIC,
            "h2d_bytes_per_step": (n_total * 12 + 12) / args.steps,
            "d2h_bytes_per_step": exports * (n_total * 12 + 4 * len(models) + 64) / args.steps,
-           "includes": "setup (upload of x, v from pinned host memory; binning; initial grid); frames of "
+           "includes": "host clock from before ckmpm_create to the last export landing: scene creation, setup "
+                       "(upload of x, v from pinned host memory; binning; initial grid); frames of "
                        f"{args.e2e_frame} substeps, each followed by the status read and a position export "
                        "(gathered on the compute stream, copied to pinned host memory on a second stream while "
                        "the next frame runs; the last one waited for)"}
@@ -720,33 +722,109 @@ def run_reference(args, rank, world):
         # The reference runs one scene per process: loop it over every 8th scene.
         from oracle import ref_runner
         work, secs = 0, 0.0
-        sample = models[::8]
+        sample = models[::getattr(args, "reference_every", 8)]
         for m in sample:
             r = ref_runner.time_reference(family, cfg, [m], args.steps, args.warmup)
             work += r["particles"] * r["substeps"]
             secs += r["seconds"]
-        value = work / secs
+        value = e2e_value = work / secs
         cpu = {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
                "runs_on": "one B200: the reference's implementation of this path is CUDA code",
                "sample": f"reference CUDA build (oracle/_ref/ref_{family}) via MPMEngine::Simulate in profile mode, "
-                         f"one process per scene, every 8th scene ({len(sample)} of {len(models)}), "
+                         f"one process per scene, every {getattr(args, 'reference_every', 8)}th scene "
+                         f"({len(sample)} of {len(models)}), "
                          f"{args.warmup + args.steps} substeps each; host timer around each frame loop, summed"}
     elif family and harness.exists():
         from oracle import ref_runner
-        res = ref_runner.time_reference(family, cfg, models, args.steps, args.warmup)
+        res = ref_runner.time_reference_e2e(family, cfg, models, args.steps, args.warmup)
         value = res["value"]
-        cpu = {"value": value, "unit": METRIC, "cores": 1, "kind": "reference", "sample": res["sample"],
+        e2e_value = res["e2e_value"] or value
+        cpu = {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
+               "sample": f"reference CUDA build (oracle/_ref/ref_{family}) via MPMEngine::Simulate in profile mode: "
+                         f"{res['substeps']} substeps of the {res['particles']}-particle scene, its own host timer "
+                         "around its frame loop",
                "runs_on": "one B200: the reference's implementation of this path is CUDA code"}
     else:
         cpu = cpu_baseline_oracle(cfg, models, args.cpu_seconds)
         cpu["kind"] = "port"
-        value = cpu["value"]
-    return {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        value = e2e_value = cpu["value"]
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded jittered lattice, numpy PCG64 seed 0)",
             "config": {"workload": WORKLOADS[args.workload], "particles": sum(len(m.particle_position) for m in models)},
             "impl": "reference", "cpu_baseline": cpu,
-            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if e2e_value != value:
+        line["e2e"]["includes"] = ("the harness's host clock from before MPMEngine::Initialize to the end of "
+                                   "Simulate's frame loop (Initialize, InitializeParticle with the upload of x and v, "
+                                   "InitialSetup, the frame loop; no export); the CUDA context and every kernel "
+                                   "module are loaded before it starts, as for ours")
+    return line
+
+
+def subrecords(args) -> dict:
+    """Bounded lines for the other benchmark configurations, measured after the headline line at
+    N = 1: the jelly cube (config 1) beside the reference build on the same scene, the 256 batched
+    scenes (config 4) beside the same scenes looped through the plain path at their autotuned
+    shapes and a sample of them through the reference, and the differentiable cube (config 5)
+    beside the plain engine's forward.  Each record carries its own value, e2e and roofline; a
+    failure is recorded in place of the record and does not stop the run."""
+    import copy
+
+    def sub(**kw):
+        a = copy.copy(args)
+        for k, v in kw.items():
+            setattr(a, k, v)
+        return a
+
+    keep = ("value", "unit", "steps", "warmup", "ms_per_step", "e2e", "roofline", "config", "gpu_launches", "clocks")
+    out = {}
+    try:
+        a = sub(workload="jelly_cube", steps=1000, warmup=20, no_cpu_baseline=True)
+        line = run_ours(a, 0, 1, 0)
+        ref = run_reference(a, 0, 1)
+        rec = {k: line[k] for k in keep if k in line}
+        rec["reference"] = {"value": ref["value"], "e2e": ref["e2e"]["value"], "sample": ref["cpu_baseline"]["sample"]}
+        rec["vs_reference"] = {"ratio": line["value"] / ref["value"],
+                               "e2e_ratio": line["e2e"]["value"] / ref["e2e"]["value"]}
+        out["jelly_cube"] = rec
+    except Exception as e:  # recorded, not raised: the headline line stands on its own
+        out["jelly_cube"] = {"error": repr(e)}
+    try:
+        a = sub(workload="batched_256", steps=200, warmup=5, no_cpu_baseline=True, reference_every=16)
+        line = run_batched(a, 0, 1, 0)
+        ref = run_reference(a, 0, 1)
+        rec = {k: line[k] for k in keep if k in line}
+        rec["looped_plain"] = line.get("looped_plain")
+        rec["reference"] = {"value": ref["value"], "sample": ref["cpu_baseline"]["sample"]}
+        rec["vs_reference"] = {"ratio": line["value"] / ref["value"]}
+        out["batched_256"] = rec
+    except Exception as e:
+        out["batched_256"] = {"error": repr(e)}
+    try:
+        a = sub(workload="diff_cube", steps=3, warmup=3, no_cpu_baseline=True)
+        line = run_diff(a, 0, 1, 0)
+        rec = {k: line[k] for k in keep if k in line}
+        for k in ("forward_ms", "adjoint_ms", "train_step_ms", "fwd_adj_over_fwd", "plain_forward_ms",
+                  "fwd_adj_over_plain_forward"):
+            rec[k] = line[k]
+        out["diff_cube"] = rec
+    except Exception as e:
+        out["diff_cube"] = {"error": repr(e)}
+    return out
+
+
+def host_cpu() -> dict:
+    """Host cores and CPU model of the machine the CPU baselines ran on."""
+    model = None
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    return {"nproc": os.cpu_count(), "model": model}
 
 
 def ncu_case_other(args):
@@ -831,6 +909,9 @@ def main():
             else:
                 line["cpu_baseline"] = cpu_baseline_oracle(cfg, models, args.cpu_seconds)
             line["cpu_pic_baseline"] = cpu_baseline_pic(min(args.cpu_seconds, 10.0))
+            line["cpu_pic_baseline"]["host"] = host_cpu()
+        if world == 1 and args.workload == "sand_column" and not args.no_subrecords:
+            line["configs"] = subrecords(args)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch
