@@ -319,6 +319,7 @@ __device__ __forceinline__ AxisStencil axis_stencil(float xs) {
   return s;
 }
 
+
 // First and second weighted moments of one grid along one axis (world units):
 // m1 = sum_d w_d (d - o) dx, m2 = sum_d w_d (d - o)^2 dx^2.  With a tensor
 // product kernel whose 1-D weights sum to one, D = sum_nodes w r r^T has
@@ -1307,6 +1308,50 @@ __global__ void setup_identity_kernel(BlockListDev cur, BlockListDev prev) {
 // Setup: the particles of a model that binning dropped (outside the domain).
 __global__ void count_lost_kernel(Scalars* scal, uint32_t n, const uint32_t* __restrict__ binned) {
   if (threadIdx.x == 0 && blockIdx.x == 0) scal->lost += n - *binned;
+}
+
+// ------------------------------------------------------------------ decomposed scene
+// One scene split over ranks by particle ownership (no counterpart in the
+// reference, which runs on one GPU): every rank keeps the whole dense grid,
+// deposits only its own particles, and before the next substep the ranks sum
+// the blocks that more than one of them deposited into.  The sums are exact
+// 64-bit integers, so every rank then reads the grid a single GPU would hold.
+
+// mask[b] = 1 when block b of the grid the next substep reads holds this
+// rank's deposits (its stamp is the read epoch), else 0.
+__global__ void dd_mark_kernel(const int32_t* __restrict__ stamp, int32_t epoch, uint32_t nbd, int32_t* mask) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nbd; b += gridDim.x * blockDim.x)
+    mask[b] = stamp[b] == epoch ? 1 : 0;
+}
+
+// Copies the listed blocks (512 sums each) into buf; a block without this
+// rank's deposits contributes zeros.  One warp per block.
+__global__ void dd_pack_kernel(const long long* __restrict__ g, const int32_t* __restrict__ stamp, int32_t epoch,
+                               const int32_t* __restrict__ list, uint32_t n, uint32_t nbd,
+                               longlong2* __restrict__ buf) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < n; t += nwarps) {
+    const int32_t b = list[t];
+    const bool own = b >= 0 && static_cast<uint32_t>(b) < nbd && stamp[b] == epoch;
+    const longlong2* src = reinterpret_cast<const longlong2*>(g + static_cast<int64_t>(own ? b : 0) * 512);
+    for (int i = lane; i < 256; i += 32) buf[static_cast<size_t>(t) * 256 + i] = own ? src[i] : make_longlong2(0, 0);
+  }
+}
+
+// Writes the summed blocks back and stamps them with the read epoch.
+__global__ void dd_unpack_kernel(long long* __restrict__ g, int32_t* __restrict__ stamp, int32_t epoch,
+                                 const int32_t* __restrict__ list, uint32_t n, uint32_t nbd,
+                                 const longlong2* __restrict__ buf) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < n; t += nwarps) {
+    const int32_t b = list[t];
+    if (b < 0 || static_cast<uint32_t>(b) >= nbd) continue;
+    longlong2* dst = reinterpret_cast<longlong2*>(g + static_cast<int64_t>(b) * 512);
+    for (int i = lane; i < 256; i += 32) dst[i] = buf[static_cast<size_t>(t) * 256 + i];
+    if (lane == 0) stamp[b] = epoch;
+  }
 }
 
 // ------------------------------------------------------------------ probe / export

@@ -122,6 +122,35 @@ def test_constitutive_matches_oracle(engine_lib, oracle_mod):
                 assert np.abs(S[i] - So).max() <= 3e-6 * max(1.0, So[0])
 
 
+def test_near_identity_deformation_stays_unrotated(engine_lib):
+    """A deformation gradient within rounding of the identity (a free-falling or rigidly moving
+    body: F = I + dt C with dt C ~ 1e-11) leaves the SVD's pairs unrotated, as the reference's SVD
+    does: V is exactly the identity, fixed-corotated stress is exactly zero, and the Drucker-Prager
+    tension branch's re-projected F = U V^T stays within 1e-10 of the identity instead of picking
+    up the ~1e-7 rounding of 45-degree rotations every substep."""
+    rng = np.random.default_rng(9)
+    n = 256
+    F0 = (np.eye(3) + rng.normal(scale=1e-11, size=(n, 3, 3))).astype(np.float32)
+    Cm = np.zeros((n, 3, 3), np.float32)
+    lam, mu = 1.0e5, 1.35e5
+    for kind in (capi.FIXED_COROTATED, capi.DRUCKER_PRAGER):
+        cm = capi.Material()
+        cm.kind = kind
+        cm.p[0], cm.p[1] = lam, mu
+        F, aux, tau = F0.copy(), np.zeros(n, np.float32), np.zeros((n, 3, 3), np.float32)
+        U, S, V = np.zeros_like(F), np.zeros((n, 3), np.float32), np.zeros_like(F)
+        capi.check(engine_lib.ckmpm_debug_constitutive(cm, n, capi.fptr(Cm), 1e-4, capi.fptr(F), capi.fptr(aux),
+                                                       capi.fptr(tau), capi.fptr(U), capi.fptr(S), capi.fptr(V)),
+                   "debug")
+        assert np.array_equal(V, np.broadcast_to(np.eye(3, dtype=np.float32), V.shape)), kind
+        assert np.abs(S - 1.0).max() == 0.0, kind
+        if kind == capi.FIXED_COROTATED:
+            assert not tau.any()
+        else:
+            assert np.abs(F.astype(np.float64) - np.eye(3)).max() <= 1e-10
+            assert np.abs(tau).max() <= 1e-3  # Pa: at most rounding of a zero strain
+
+
 def test_setup_binning_exact(engine_lib, oracle_mod):
     cfg, models = scenes.jelly_cube()
     s = run_engine(cfg, models, 0, 0.0)

@@ -15,11 +15,13 @@ f32 = np.float32
 
 def _rotate(M, V, p, q, r):
     app, aqq, apq = M[p, p], M[q, q], M[p, q]
+    if not abs(apq) >= 2e-10:  # negligible off-diagonal: the pair stays unrotated
+        return
     d = aqq - app
     e = f32(2) * apq
     h = np.sqrt(d * d + e * e)
     den = d + np.copysign(h, d)
-    t = e / den if (abs(e) > 1e-30 and den != 0) else f32(0)
+    t = e / den if den != 0 else f32(0)
     c = f32(1) / np.sqrt(f32(1) + t * t)
     s = t * c
     M[p, p] = app - t * apq
@@ -60,6 +62,7 @@ FAMILIES = {
     "stretch 0.1-3": lambda r: _rotation(r) @ np.diag(r.uniform(0.1, 3.0, 3)) @ _rotation(r),
     "log-uniform e^[-2,2]": lambda r: _rotation(r) @ np.diag(np.exp(r.uniform(-2, 2, 3))) @ _rotation(r),
     "near-isotropic 1+-1e-3": lambda r: _rotation(r) @ np.diag(1 + r.uniform(-1e-3, 1e-3, 3)) @ _rotation(r),
+    "rotation 1+-1e-6": lambda r: _rotation(r) @ np.diag(1 + r.uniform(-1e-6, 1e-6, 3)),
     "two equal values": lambda r: _rotation(r) @ np.diag([1.0, 1.0, r.uniform(0.8, 1.2)]) @ _rotation(r),
     "shear I + N(0, 0.5)": lambda r: np.eye(3) + r.normal(scale=0.5, size=(3, 3)),
 }
@@ -79,3 +82,19 @@ def test_three_jacobi_sweeps_reach_float32_rounding(family):
     assert worst_s < 5e-7, (family, worst_s)
     assert np.quantile(offs, 0.99) < 3e-7, (family, np.quantile(offs, 0.99))
     assert max(offs) < 1e-5, (family, max(offs))
+
+
+def test_near_identity_is_left_unrotated():
+    """A deformation gradient within rounding of the identity (a free-falling or rigidly moving
+    body: I + dt C with dt C ~ 1e-11) gives A^T A with equal diagonal entries in float32 and a
+    negligible off-diagonal; the sweeps leave it unrotated, so V stays exactly the identity."""
+    rng = np.random.default_rng(5)
+    for _ in range(200):
+        A = (np.eye(3) + rng.normal(scale=1e-11, size=(3, 3))).astype(f32)
+        M = (A.T @ A).astype(f32)
+        V = np.eye(3, dtype=f32)
+        for _ in range(3):
+            _rotate(M, V, 0, 1, 2)
+            _rotate(M, V, 0, 2, 1)
+            _rotate(M, V, 1, 2, 0)
+        assert np.array_equal(V, np.eye(3, dtype=f32))
