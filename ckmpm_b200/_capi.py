@@ -51,6 +51,7 @@ EXPORTED = (
     "ckmpm_checkpoint_restore", "ckmpm_diff_create", "ckmpm_diff_forward", "ckmpm_diff_backward", "ckmpm_diff_timing",
     "ckmpm_diff_last_error", "ckmpm_diff_destroy", "ckmpm_set_rigid", "ckmpm_set_rigid_velocity", "ckmpm_get_time",
     "ckmpm_set_boundary_field", "ckmpm_export_positions_async", "ckmpm_export_wait",
+    "ckmpm_dd_blocks", "ckmpm_dd_mark", "ckmpm_dd_pack", "ckmpm_dd_unpack",
 )
 
 MAX_BATCH_SCENES = 65536
@@ -136,6 +137,10 @@ def lib() -> C.CDLL:
                                              C.c_float, C.c_float, C.c_uint32, C.c_float, P, P, P, P, P,
                                              C.POINTER(C.c_uint32), C.POINTER(C.c_char_p)]
         L.ckmpm_create_batch.argtypes = [C.POINTER(SceneDesc), C.c_uint32, C.POINTER(P)]
+        L.ckmpm_dd_blocks.argtypes = [P, u32p]
+        L.ckmpm_dd_mark.argtypes = [P, P]
+        L.ckmpm_dd_pack.argtypes = [P, P, C.c_uint32, P]
+        L.ckmpm_dd_unpack.argtypes = [P, P, C.c_uint32, P]
         L.ckmpm_add_batch.argtypes = [P, C.c_uint32, C.POINTER(BatchScene), f32p, f32p]
         L.ckmpm_get_blocks_in.argtypes = [P, C.c_uint32, C.c_int32, C.c_int32, i32p, u32p, C.c_uint32, u32p]
         L.ckmpm_set_tuning.argtypes = [P, C.POINTER(Tuning)]

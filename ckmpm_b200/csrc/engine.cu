@@ -1188,6 +1188,73 @@ ckmpm_status ckmpm_get_time(ckmpm_scene* s, double* out2) {
   return CKMPM_OK;
 }
 
+// The grid the next substep reads and its epoch (the substep count).
+static void dd_grid(ckmpm_scene* s, long long** g, int32_t** stamp, int32_t* epoch) {
+  const int parity = static_cast<int>(s->host_step & 1);
+  *g = s->grid.grid[parity];
+  *stamp = s->grid.stamp[parity];
+  *epoch = static_cast<int32_t>(s->host_step);
+}
+
+static ckmpm_status dd_check(ckmpm_scene* s) {
+  if (!s) return fail(s, CKMPM_ERR_INVALID, "null scene");
+  if (!s->setup_done) return fail(s, CKMPM_ERR_INVALID, "ckmpm_setup has not run");
+  if (s->nstack != 1) return fail(s, CKMPM_ERR_INVALID, "a batch is not decomposed");
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_dd_blocks(ckmpm_scene* s, uint32_t* n_blocks) {
+  if (!s || !n_blocks) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  *n_blocks = s->sc.nblocks_domain;
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_dd_mark(ckmpm_scene* s, int32_t* mask) {
+  ckmpm_status st = dd_check(s);
+  if (st != CKMPM_OK) return st;
+  if (!mask) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  long long* g;
+  int32_t* stamp;
+  int32_t epoch;
+  dd_grid(s, &g, &stamp, &epoch);
+  dd_mark_kernel<<<s->sm_count * 4, 256, 0, s->stream>>>(stamp, epoch, s->sc.nblocks_domain, mask);
+  CK_CUDA(s, cudaGetLastError());
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_dd_pack(ckmpm_scene* s, const int32_t* blocks, uint32_t n, long long* buf) {
+  ckmpm_status st = dd_check(s);
+  if (st != CKMPM_OK) return st;
+  if (n == 0) return CKMPM_OK;
+  if (!blocks || !buf) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  long long* g;
+  int32_t* stamp;
+  int32_t epoch;
+  dd_grid(s, &g, &stamp, &epoch);
+  dd_pack_kernel<<<s->sm_count * 4, 256, 0, s->stream>>>(g, stamp, epoch, blocks, n, s->sc.nblocks_domain,
+                                                         reinterpret_cast<longlong2*>(buf));
+  CK_CUDA(s, cudaGetLastError());
+  return CKMPM_OK;
+}
+
+ckmpm_status ckmpm_dd_unpack(ckmpm_scene* s, const int32_t* blocks, uint32_t n, const long long* buf) {
+  ckmpm_status st = dd_check(s);
+  if (st != CKMPM_OK) return st;
+  if (n == 0) return CKMPM_OK;
+  if (!blocks || !buf) return fail(s, CKMPM_ERR_INVALID, "null argument");
+  CK_CUDA(s, cudaSetDevice(s->desc.device));
+  long long* g;
+  int32_t* stamp;
+  int32_t epoch;
+  dd_grid(s, &g, &stamp, &epoch);
+  dd_unpack_kernel<<<s->sm_count * 4, 256, 0, s->stream>>>(g, stamp, epoch, blocks, n, s->sc.nblocks_domain,
+                                                           reinterpret_cast<const longlong2*>(buf));
+  CK_CUDA(s, cudaGetLastError());
+  return CKMPM_OK;
+}
+
 ckmpm_status ckmpm_get_dt(ckmpm_scene* s, float* out2) {
   if (!s || !out2) return fail(s, CKMPM_ERR_INVALID, "null argument");
   Scalars h{};

@@ -231,6 +231,26 @@ ckmpm_status ckmpm_get_time(ckmpm_scene* s, double* out2);
  * of the rebinning launches, [2]: number of fused launches. */
 ckmpm_status ckmpm_step_profiled(ckmpm_scene* s, uint32_t nsteps, float dt, double* ms_out3);
 
+/* One scene decomposed over ranks (no counterpart in the reference, which runs
+ * on one GPU, src/cuda_util.cu:5-17).  Each rank creates the whole scene with
+ * only the particles it owns; every rank then holds the whole dense grid and
+ * deposits only its own particles.  After ckmpm_setup and after every single
+ * substep (ckmpm_step_async with nsteps = 1), before the next one, the ranks
+ * exchange the grid the next substep reads: ckmpm_dd_mark sets mask[b] = 1
+ * (device int32, ckmpm_dd_blocks entries) for every domain block holding this
+ * rank's deposits; the caller sums the masks over ranks and lists, in
+ * increasing block order, the blocks with a sum of 2 or more (only those are
+ * read by more than one rank); ckmpm_dd_pack copies the listed blocks (512
+ * int64 sums, 4 KB each; zeros where this rank has no deposits) into buf; the
+ * caller sums buf over ranks (an int64 all-reduce); ckmpm_dd_unpack writes the
+ * sums back.  The sums are exact integers, so every rank's particles then
+ * evolve bit for bit as in the undecomposed scene.  All on the scene's stream;
+ * device pointers. */
+ckmpm_status ckmpm_dd_blocks(ckmpm_scene* s, uint32_t* n_blocks);
+ckmpm_status ckmpm_dd_mark(ckmpm_scene* s, int32_t* mask);
+ckmpm_status ckmpm_dd_pack(ckmpm_scene* s, const int32_t* blocks, uint32_t n, long long* buf);
+ckmpm_status ckmpm_dd_unpack(ckmpm_scene* s, const int32_t* blocks, uint32_t n, const long long* buf);
+
 /* Device-math test hook: applies one constitutive update to n particles on
  * the GPU exactly as the substep does (dW = I + dt C; F <- dW F; SVD; return
  * map; stress).  F (9n), aux (n) are updated in place; tau (9n) receives the
