@@ -88,3 +88,49 @@ def test_sharded_batch_over_gloo_world_size_2():
 
 def test_reduce_over_ranks_without_a_process_group():
     assert reduce_over_ranks(3.0, 7.0, device="cpu") == (3.0, 7.0)
+
+
+def _oracle_scene_state(cfg, model, nsteps):
+    from oracle import oracle as O
+    o = O.OracleScene(cfg, [model])
+    o.setup()
+    o.step(nsteps, cfg.dt)
+    st = o.state(0)
+    o.close()
+    return st["x"].copy(), st["F"].copy()
+
+
+def _shard_rank_main(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        cfg, models = scenes.batched_scenes(n_scenes=8, seed=5, n_min=300, n_max=1200)
+        mine = shard_scenes([len(m.particle_position) for m in models], world)[rank]
+        res = {i: _oracle_scene_state(cfg, models[i], 6) for i in mine}
+        gathered = [None] * world
+        dist.all_gather_object(gathered, res)
+        if rank == 0:
+            union = {}
+            for g in gathered:
+                union.update(g)
+            out["union"] = union
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_scenes_through_the_oracle_equal_the_unsharded_run():
+    """Each of two gloo ranks runs its shard of a small batch through the FP64 oracle; the union
+    of their results, gathered over the process group, is the unsharded run scene for scene."""
+    from oracle import oracle as O
+    O.build()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_shard_rank_main, args=(2, _free_port(), out), nprocs=2, join=True)
+        union = dict(out)["union"]
+    cfg, models = scenes.batched_scenes(n_scenes=8, seed=5, n_min=300, n_max=1200)
+    assert sorted(union) == list(range(8))
+    for i, m in enumerate(models):
+        x, F = _oracle_scene_state(cfg, m, 6)
+        assert np.array_equal(union[i][0], x) and np.array_equal(union[i][1], F), i
