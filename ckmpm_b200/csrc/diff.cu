@@ -11,7 +11,12 @@
 //    the dense passes run over that box only, and every box is zeroed after use;
 //  * particles SoA (x[3][n], F[9][n]); checkpoints every K substeps hold x, F
 //    and the node velocities of that substep; the backward recomputes one
-//    segment at a time into a tape of K substeps, then runs the adjoint.
+//    segment at a time into a tape of K substeps, then runs the adjoint;
+//  * vbar: the node-velocity adjoint the particle adjoints scatter, as exact
+//    int64 fixed-point sums like the forward's, so gradients are bitwise
+//    reproducible too.  Its unit is set on the device at the start of each
+//    backward from the largest incoming adjoint (the backward is linear in its
+//    seed): 2^-40 of that largest component.
 #include <climits>
 
 #include "diff_math.cuh"
@@ -27,6 +32,8 @@ constexpr int kThreads = 128;
 constexpr float kScale = 68719476736.0f;  // 2^36
 constexpr float kMaxValue = 131072.0f;    // 2^17
 constexpr uint32_t kErrOutside = 1u, kErrRange = 2u;
+constexpr float kAdjUnits = 1099511627776.0f;  // 2^40 fixed-point units per largest seed component
+constexpr float kAdjMaxUnits = 4.6e18f;        // |contribution| bound in units (< 2^62)
 
 struct Box {
   int lo[3], hi[3];
@@ -37,6 +44,7 @@ struct Dev {
   uint32_t n;
   float dx, inv_dx, mass, vol_over_mass, unit;  // unit = mass * 2^-36
   uint32_t* status;
+  float* adj_scale;  // [0]: fixed-point units per adjoint unit, [1]: its inverse; [2]: max |seed| (bits)
 };
 
 __device__ __forceinline__ void box_reset(int* b) {
@@ -215,11 +223,31 @@ __global__ void __launch_bounds__(kThreads) particle_kernel(Dev d, const float* 
 
 // Adjoint of one substep for every particle.  xb / Fb hold the adjoints of the
 // substep's outputs on entry and of its inputs on exit.
+// The fixed-point unit of the velocity adjoint: the largest |component| of the
+// incoming adjoints (x and F at the end of the rollout), then 2^40 units per it.
+__global__ void adj_seed_max_kernel(uint32_t n, const float* __restrict__ xb, const float* __restrict__ Fb,
+                                    float* adj_scale) {
+  float m = 0.f;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 12 * n; i += gridDim.x * blockDim.x)
+    m = fmaxf(m, fabsf(i < 3 * n ? xb[i] : Fb[i - 3 * n]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  // non-negative floats order like their bit patterns
+  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(reinterpret_cast<unsigned*>(adj_scale + 2), __float_as_uint(m));
+}
+
+__global__ void adj_scale_kernel(float* adj_scale) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    const float m = adj_scale[2];
+    adj_scale[0] = m > 0.f ? __fdiv_rn(kAdjUnits, m) : 1.f;
+    adj_scale[1] = m > 0.f ? __fdiv_rn(m, kAdjUnits) : 1.f;
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, 3) particle_adjoint_kernel(
     Dev d, const float* __restrict__ x, const float* __restrict__ F, const float* __restrict__ lam,
     const float* __restrict__ mu, const float4* __restrict__ vel, float dt, float ndt, const float4* __restrict__ gadj,
     float* __restrict__ xb, float* __restrict__ Fb, float* __restrict__ mub, float* __restrict__ lamb,
-    float* __restrict__ vbar) {
+    unsigned long long* __restrict__ vbar) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= d.n) return;
   Particle<float> pp;
@@ -240,12 +268,19 @@ __global__ void __launch_bounds__(kThreads, 3) particle_adjoint_kernel(
     out[2] = q.z;
     out[3] = q.w;
   };
+  const float units = d.adj_scale[0];
   auto vs = [&](int g, int cx, int cy, int cz, const float* vb) {
     if (!diff::node_in_grid(G, cx, cy, cz)) return;
-    float* q = vbar + 3 * diff::node_index(G, g, cx, cy, cz);
-    atomicAdd(q, vb[0]);
-    atomicAdd(q + 1, vb[1]);
-    atomicAdd(q + 2, vb[2]);
+    unsigned long long* q = vbar + 3 * diff::node_index(G, g, cx, cy, cz);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float u = vb[c] * units;
+      if (!(fabsf(u) < kAdjMaxUnits)) {
+        atomicOr(d.status, kErrRange);
+        continue;
+      }
+      atomicAdd(q + c, static_cast<unsigned long long>(__float2ll_rn(u)));
+    }
   };
   float xnb[3], Fnb[9], xo[3], Fo[9];
   for (int a = 0; a < 3; ++a) xnb[a] = xb[a * d.n + p];
@@ -261,7 +296,7 @@ __global__ void __launch_bounds__(kThreads, 3) particle_adjoint_kernel(
 
 // Grid-update adjoint over box b: node velocity adjoint -> (mbar, mvbar); zeroes vbar.
 __global__ void grid_adjoint_kernel(Dev d, const int* __restrict__ b, const float4* __restrict__ vel, float dt,
-                                    float* __restrict__ vbar, float4* __restrict__ gadj) {
+                                    unsigned long long* __restrict__ vbar, float4* __restrict__ gadj) {
   if (b[0] > b[3]) return;
   const int ex = b[3] - b[0] + 1, ey = b[4] - b[1] + 1, ez = b[5] - b[2] + 1;
   const int64_t total = 2ll * ex * ey * ez;
@@ -272,9 +307,12 @@ __global__ void grid_adjoint_kernel(Dev d, const int* __restrict__ b, const floa
     const int g = static_cast<int>(t / (static_cast<int64_t>(ez) * ey * ex));
     const int cx = b[0] + x, cy = b[1] + y, cz = b[2] + z;
     const int64_t id = diff::node_index(d.G, g, cx, cy, cz);
-    float* vb = vbar + 3 * id;
-    const float vbv[3] = {vb[0], vb[1], vb[2]};
-    vb[0] = vb[1] = vb[2] = 0.f;
+    unsigned long long* vb = vbar + 3 * id;
+    const float inv_units = d.adj_scale[1];
+    const float vbv[3] = {__ll2float_rn(static_cast<long long>(vb[0])) * inv_units,
+                          __ll2float_rn(static_cast<long long>(vb[1])) * inv_units,
+                          __ll2float_rn(static_cast<long long>(vb[2])) * inv_units};
+    vb[0] = vb[1] = vb[2] = 0ull;
     const float4 q = vel[id];
     const float v[3] = {q.x, q.y, q.z};
     float out[4];
@@ -353,7 +391,8 @@ struct ckmpm_diff {
   float4* vel = nullptr;              // scratch node velocities (forward pass)
   unsigned long long* gsum[2] = {nullptr, nullptr};
   int* box = nullptr;                 // (nsteps + 1) x 6
-  float *xb = nullptr, *Fb = nullptr, *mub = nullptr, *lamb = nullptr, *vbar = nullptr;
+  float *xb = nullptr, *Fb = nullptr, *mub = nullptr, *lamb = nullptr;
+  unsigned long long* vbar = nullptr;
   float4* gadj = nullptr;
   cudaGraphExec_t gfwd = nullptr, gbwd = nullptr;
   uint64_t generation = 0;
@@ -468,12 +507,14 @@ ckmpm_status ckmpm_diff_create(const ckmpm_scene_desc* desc, uint32_t n, float m
             dk_alloc(h, &h->box, 6 * static_cast<size_t>(nsteps + 1)) == cudaSuccess &&
             dk_alloc(h, &h->xb, 3 * n) == cudaSuccess && dk_alloc(h, &h->Fb, 9 * n) == cudaSuccess &&
             dk_alloc(h, &h->mub, n) == cudaSuccess && dk_alloc(h, &h->lamb, n) == cudaSuccess &&
-            dk_alloc(h, &h->vbar, 3 * nn) == cudaSuccess && dk_alloc(h, &h->gadj, nn) == cudaSuccess;
+            dk_alloc(h, &h->vbar, 3 * nn) == cudaSuccess && dk_alloc(h, &h->gadj, nn) == cudaSuccess &&
+            dk_alloc(h, &h->d.adj_scale, 4) == cudaSuccess;
   if (!ok) return bail(dfail(h, CKMPM_ERR_CUDA, "device allocation failed"));
   // Sums and velocity adjoints start (and are always left) at zero inside every box.
   if (cudaMemsetAsync(h->gsum[0], 0, 32 * nn, h->stream) != cudaSuccess ||
       cudaMemsetAsync(h->gsum[1], 0, 32 * nn, h->stream) != cudaSuccess ||
-      cudaMemsetAsync(h->vbar, 0, 12 * nn, h->stream) != cudaSuccess ||
+      cudaMemsetAsync(h->vbar, 0, 24 * nn, h->stream) != cudaSuccess ||
+      cudaMemsetAsync(h->d.adj_scale, 0, 4 * sizeof(float), h->stream) != cudaSuccess ||
       cudaMemsetAsync(h->vel, 0, 16 * nn, h->stream) != cudaSuccess ||
       cudaStreamSynchronize(h->stream) != cudaSuccess)
     return bail(dfail(h, CKMPM_ERR_CUDA, "initialisation failed"));
@@ -552,7 +593,11 @@ cudaError_t enqueue_backward(ckmpm_diff* h) {
   cudaStream_t st = h->stream;
   aos_to_soa_kernel<<<blocks_for(n), kThreads, 0, st>>>(n, 3, h->gxT, h->xb);
   aos_to_soa_kernel<<<blocks_for(n), kThreads, 0, st>>>(n, 9, h->gFT, h->Fb);
-  cudaError_t e = cudaMemsetAsync(h->mub, 0, sizeof(float) * n, st);
+  cudaError_t e = cudaMemsetAsync(h->d.adj_scale + 2, 0, sizeof(float), st);
+  if (e != cudaSuccess) return e;
+  adj_seed_max_kernel<<<ctas, 256, 0, st>>>(n, h->xb, h->Fb, h->d.adj_scale);
+  adj_scale_kernel<<<1, 32, 0, st>>>(h->d.adj_scale);
+  e = cudaMemsetAsync(h->mub, 0, sizeof(float) * n, st);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(h->lamb, 0, sizeof(float) * n, st);
   if (e != cudaSuccess) return e;

@@ -7,13 +7,15 @@ Tolerances (FP32 engine vs FP64 oracle on the same seeded inputs):
   * after N substeps: positions within 2e-6 (absolute, domain [0,1]),
     deformation gradients within 5e-5, velocities within 1e-4 x max|v| + 1e-6,
     J / logJp within 5e-5;
-  * Drucker-Prager: singular values near 1 carry ~1e-7 absolute noise in FP32,
-    so at the ~1e-5 strains of a column settling under gravity the Hencky
-    strain (log sigma) has ~1% noise, which the zero-pressure branch and the
-    logJp volume correction of the return map (include/mpm_material.cuh:400-445)
-    carry into the stress; the reference's FP32 SVD has the same floor.
-    Velocities are compared as: 99% of particles within 3% of max|v| and all
-    within 5%; x and F at the 99th percentile with the tolerances above;
+  * Drucker-Prager: at the ~1e-5 strains of a column settling under gravity,
+    FP32 rounding of singular values near 1 is a visible part of the Hencky
+    strain, which the zero-pressure branch and the logJp volume correction of
+    the return map (include/mpm_material.cuh:400-445) carry into the stress, so
+    velocities differ by up to ~0.6 % of max|v| between any two implementations
+    (this engine, the FP64 oracle, the reference build: the oracle and the
+    reference differ from each other by as much on the full column).  Compared
+    as: every velocity within 1 % of max|v|, x within the tolerance above, F and
+    logJp within twice theirs;
   * integer outputs (block sets, per-block counts, live counts): exact.
 """
 import numpy as np
@@ -71,10 +73,9 @@ def compare(s, o, model=0, x_tol=X_TOL, f_tol=F_TOL, v_rel=V_REL, aux_tol=AUX_TO
           f"vmax {vmax:.3e}, worst at x={r['x'][alive][w]}) |daux|={ea.max():.3e}")
     vtol = v_rel * vmax + 1e-6
     if branchy:
-        assert np.percentile(ev, 99) <= 0.03 * vmax + 1e-6
-        assert ev.max() <= 0.05 * vmax + 1e-6
-        assert np.percentile(ex, 99) <= x_tol and ex.max() <= 10 * x_tol
-        assert np.percentile(eF, 99) <= f_tol and np.percentile(ea, 99) <= aux_tol
+        assert ev.max() <= 1e-2 * vmax + 1e-6
+        assert ex.max() <= x_tol
+        assert eF.max() <= 2 * f_tol and ea.max() <= 2 * aux_tol
     else:
         assert ex.max() <= x_tol
         assert eF.max() <= f_tol
