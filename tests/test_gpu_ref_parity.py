@@ -16,10 +16,13 @@ Integer contract (binning and the block table), checked exactly:
     {0,1}^3 and {-1,0,1}^3 neighbours clipped to the domain (:658-695);
   * the engine's NA / NN / NE key sets, per-block counts and per-block id sets equal the
     reference's at setup and after 1 and 10 substeps; later, wherever a particle's block
-    differs the two positions straddle a block face within the float tolerance.
+    differs the two positions straddle a block face within the float tolerance on x below.
 Float contract: the reference's P2G sums with float atomics, so two runs of it differ; x, v, F
 (and logJp for the sand) of the engine must lie within a few times that run-to-run spread of
-the reference, with a floor (the tolerances are stated at FLOAT_TOL).
+the reference, with a floor (the tolerances are stated at FLOAT_TOL).  The reference runs three
+times; the engine is compared with the first run and the spread is the largest distance between
+any two of the three, which one pair alone estimates too noisily after hundreds of substeps (at
+500 sand substeps single pairs measured 4.5e-6 to 1.3e-5 in x).
 """
 from __future__ import annotations
 
@@ -38,16 +41,18 @@ CASES = {
 EARLY = (0, 1, 10)  # substep counts at which every integer output must agree exactly
 
 # Engine-vs-reference error allowed at each compared substep count, per quantity:
-# max |engine - reference| <= max(SPREAD_FACTOR * (max |reference run 2 - reference run 1|), floor).
+# max |engine - reference run 1| <= max(SPREAD_FACTOR * (max |reference run i - reference run j|), floor).
 # Floors: x absolute (positions in a unit domain), v relative to the largest |v| of the scene,
 # F absolute (|F| ~ 1), logJp absolute.  The reference's run-to-run spread comes from its float
 # atomics alone; the engine differs from it by rounding everywhere (another SVD, a closed-form D,
-# exact integer grid sums), so its distance is a few times that spread: at most 5.0x measured
-# (the sand column's velocities after 100 substeps), and the FP64 oracle sits as far from the
-# reference as the engine does.
+# exact integer grid sums), so its distance is a few times that spread wherever it is above the
+# floor (at most 4.4x measured: the sand column's velocities after 100 substeps; after 500 sand
+# substeps 1.1-1.4x), and the FP64 oracle sits as far from the reference as the engine does.
 SPREAD_FACTOR = 8.0
 FLOAT_TOL = {"x": 1e-5, "v": 1e-4, "F": 1e-4, "aux": 1e-4}
-X_TOL_BLOCK = 1e-5  # position difference allowed for a particle binned into another block
+# Position difference allowed for a particle that the engine bins into another block than the
+# reference: the bound of the state test for x, max(SPREAD_FACTOR * reference spread, X_TOL_BLOCK).
+X_TOL_BLOCK = 1e-5
 
 
 def _ref():
@@ -85,8 +90,7 @@ def run(request, engine_lib):
         pytest.skip(f"oracle/_ref/ref_{family} is not built (make -C oracle ref)")
     cfg, models = scenes.WORKLOADS[name](track_ids=True)
     dt = cfg.dt
-    a = ref.dump(family, models, dt, ks)
-    b = ref.dump(family, models, dt, ks)
+    refs = [ref.dump(family, models, dt, ks) for _ in range(3)]
     s = Scene(cfg)
     s.add_model(models[0])
     s.setup()
@@ -99,7 +103,13 @@ def run(request, engine_lib):
         st = s.state(0)
         ours[k] = {"state": st, "blocks": [s.blocks(0, w) for w in (0, 1, 2)]}
     s.close()
-    return {"name": name, "cfg": cfg, "ks": ks, "a": a, "b": b, "ours": ours}
+    return {"name": name, "cfg": cfg, "ks": ks, "a": refs[0], "refs": refs, "ours": ours}
+
+
+def _pairs(run, k):
+    """(model-0 dump i, model-0 dump j) for every pair of reference runs at substep count k."""
+    ms = [r[k]["models"][0] for r in run["refs"]]
+    return [(ms[i], ms[j]) for i in range(len(ms)) for j in range(i + 1, len(ms))]
 
 
 def test_reference_binning_is_the_formula(run):
@@ -162,17 +172,20 @@ def test_block_sets_match_reference(run):
         ndiff, same, differ = _compare_integers(cfg, d, o, k)
         dx = (float(np.abs(o["state"].x[differ].astype(np.float64) - d["models"][0]["x"][differ]).max())
               if ndiff else 0.0)
-        rows.append((k, ndiff, same, dx))
-        ref_diff = int(np.any(run["b"][k]["models"][0]["block"] != d["models"][0]["block"], axis=1).sum())
+        pairs = _pairs(run, k)
+        ref_diff = max(int(np.any(p["block"] != q["block"], axis=1).sum()) for p, q in pairs)
+        x_spread = max(float(np.abs(p["x"].astype(np.float64) - q["x"]).max()) for p, q in pairs)
+        rows.append((k, ndiff, same, dx, max(SPREAD_FACTOR * x_spread, X_TOL_BLOCK)))
         print(f"{run['name']} K={k}: NA {d['na']} NN {d['nn']} NE {d['ne']}; identical sets and counts: {same}; "
               f"particles in another block: {ndiff} (largest position difference among them {dx:.2e}); "
-              f"between two reference runs: {ref_diff}")
-    for k, ndiff, same, dx in rows:
+              f"between reference runs (largest of the three pairs): {ref_diff} "
+              f"(position difference {x_spread:.2e})")
+    for k, ndiff, same, dx, x_bound in rows:
         if k in EARLY:
             assert ndiff == 0 and same, (k, ndiff)
         # every disagreement is a float position difference across a block face
         assert ndiff > 0 or same, f"K={k}: every particle is in the same block but the key sets differ"
-        assert dx <= X_TOL_BLOCK, (k, dx)
+        assert dx <= x_bound, (k, dx, x_bound)
 
 
 def _errors(p, q, scale_v):
@@ -187,18 +200,20 @@ def test_state_within_reference_spread(run):
     name = run["name"]
     rows = []
     for k in run["ks"]:
-        ma, mb = run["a"][k]["models"][0], run["b"][k]["models"][0]
+        ma = run["a"][k]["models"][0]
         st = run["ours"][k]["state"]
-        assert np.array_equal(ma["id"], mb["id"]) and np.array_equal(ma["id"], st.id)
+        assert all(np.array_equal(ma["id"], r[k]["models"][0]["id"]) for r in run["refs"])
+        assert np.array_equal(ma["id"], st.id)
         scale_v = max(float(np.abs(ma["v"]).max()), 1e-6)
         ours = {"x": st.x, "v": st.v, "F": st.F.reshape(-1, 3, 3), "aux": st.aux}
         if name == "jelly_cube":
             ours["aux"] = np.zeros_like(st.aux)  # fixed-corotated keeps no scalar
-        spread = _errors(mb, ma, scale_v)
+        pair_errors = [_errors(p, q, scale_v) for p, q in _pairs(run, k)]
+        spread = {q: tuple(max(e[q][i] for e in pair_errors) for i in range(2)) for q in pair_errors[0]}
         err = _errors(ours, ma, scale_v)
         rows.append((k, err, spread))
         print(f"{name} K={k}: |v|max {scale_v:.3e}; engine vs reference (max / 99.9 %) "
-              + " ".join(f"{q} {err[q][0]:.2e}/{err[q][1]:.2e}" for q in err) + "; reference run to run "
+              + " ".join(f"{q} {err[q][0]:.2e}/{err[q][1]:.2e}" for q in err) + "; reference run to run (largest pair) "
               + " ".join(f"{q} {spread[q][0]:.2e}/{spread[q][1]:.2e}" for q in spread))
     for k, err, spread in rows:
         for q in err:
