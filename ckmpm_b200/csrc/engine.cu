@@ -1162,7 +1162,13 @@ ckmpm_status ckmpm_autotune(ckmpm_scene* s, uint32_t probe_steps, float dt, ckmp
   if (n_results) *n_results = static_cast<uint32_t>(cands.size());
   if (results)
     for (uint32_t i = 0; i < std::min<uint32_t>(cap, static_cast<uint32_t>(cands.size())); ++i) results[i] = cands[i];
-  return apply_tuning(s, *pick);
+  const ckmpm_status at = apply_tuning(s, *pick);
+  if (at != CKMPM_OK) return at;
+  // Applying the pick dropped the graphs of the last probed shape: capture the
+  // chosen shape's chunk graph now (capture runs nothing), so that the first
+  // ckmpm_step_async after tuning does not pay for it.
+  CK_CUDA(s, build_graph(s, static_cast<int>(s->tune.graph_chunk), 0, &s->graph_chunk));
+  return CKMPM_OK;
 }
 
 ckmpm_status ckmpm_get_counters(ckmpm_scene* s, uint64_t* out5) {

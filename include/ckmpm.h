@@ -340,8 +340,8 @@ ckmpm_status ckmpm_get_tuning(ckmpm_scene* s, ckmpm_tuning* t, uint32_t* max_cta
  * scene or batch at dt for every candidate launch shape (threads x CTAs per SM
  * x graph chunk), restoring the saved state before each candidate and at the
  * end, so the simulation is left exactly as it was; applies and returns the
- * fastest.  results (cap entries, may be NULL) receives every candidate with
- * its probe_ms. */
+ * fastest, with its chunk graph already captured.  results (cap entries, may
+ * be NULL) receives every candidate with its probe_ms. */
 ckmpm_status ckmpm_autotune(ckmpm_scene* s, uint32_t probe_steps, float dt, ckmpm_tuning* results, uint32_t cap,
                             uint32_t* n_results, ckmpm_tuning* best);
 
