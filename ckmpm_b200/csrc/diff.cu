@@ -10,8 +10,12 @@
 //  * bbox[s]: node-coordinate box of what substep s reads (min x,y,z, max x,y,z);
 //    the dense passes run over that box only, and every box is zeroed after use;
 //  * particles SoA (x[3][n], F[9][n]); checkpoints every K substeps hold x, F
-//    and the node velocities of that substep; the backward recomputes one
-//    segment at a time into a tape of K substeps, then runs the adjoint;
+//    and the node velocities of that substep (the forward writes those states
+//    straight into their checkpoint slots); the backward recomputes one segment
+//    at a time into a tape of the segment's other K - 1 substeps, then runs the
+//    adjoint.  With K = 1 every substep is a checkpoint and the backward is the
+//    adjoint alone (about 2.2 GB for 50k particles, 200 substeps and a 64^3
+//    grid: HBM, not recomputation, holds the rollout);
 //  * vbar: the node-velocity adjoint the particle adjoints scatter, as exact
 //    int64 fixed-point sums like the forward's, so gradients are bitwise
 //    reproducible too.  Its unit is set on the device at the start of each
@@ -386,7 +390,7 @@ struct ckmpm_diff {
   float* xs[2] = {nullptr, nullptr};  // forward ping-pong (SoA x: 3n, F: 9n in one array of 12n)
   float* ck = nullptr;                // checkpoints: nseg x 12n
   float4* ckvel = nullptr;            // nseg x nn
-  float* tape = nullptr;              // (every + 1) x 12n
+  float* tape = nullptr;              // max(every - 1, 1) x 12n: substeps s0 + 1 .. s1 - 1 of a segment
   float4* tapevel = nullptr;          // every x nn
   float4* vel = nullptr;              // scratch node velocities (forward pass)
   unsigned long long* gsum[2] = {nullptr, nullptr};
@@ -500,7 +504,7 @@ ckmpm_status ckmpm_diff_create(const ckmpm_scene_desc* desc, uint32_t n, float m
             dk_alloc(h, &h->xs[1], 12 * n) == cudaSuccess &&
             dk_alloc(h, &h->ck, static_cast<size_t>(h->nseg) * 12 * n) == cudaSuccess &&
             dk_alloc(h, &h->ckvel, static_cast<size_t>(h->nseg) * nn) == cudaSuccess &&
-            dk_alloc(h, &h->tape, static_cast<size_t>(h->every + 1) * 12 * n) == cudaSuccess &&
+            dk_alloc(h, &h->tape, static_cast<size_t>(std::max<uint32_t>(h->every, 2) - 1) * 12 * n) == cudaSuccess &&
             dk_alloc(h, &h->tapevel, static_cast<size_t>(h->every) * nn) == cudaSuccess &&
             dk_alloc(h, &h->vel, nn) == cudaSuccess && dk_alloc(h, &h->gsum[0], 4 * nn) == cudaSuccess &&
             dk_alloc(h, &h->gsum[1], 4 * nn) == cudaSuccess &&
@@ -554,9 +558,15 @@ cudaError_t enqueue_rollout(ckmpm_diff* h) {
   cudaStream_t st = h->stream;
   cudaError_t e = cudaMemsetAsync(d.status, 0, sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
-  init_kernel<<<blocks_for(n), kThreads, 0, st>>>(d, h->x0, h->logE, h->nu, h->xs[0], h->xs[0] + 3 * n, h->lam, h->mu);
+  // State of substep s: its checkpoint slot when it has one, else a ping-pong buffer.
+  auto state = [&](uint32_t s) -> float* {
+    return (s < h->nsteps && s % h->every == 0) ? h->ck + static_cast<size_t>(s / h->every) * 12 * n
+                                                 : h->xs[s & 1];
+  };
+  init_kernel<<<blocks_for(n), kThreads, 0, st>>>(d, h->x0, h->logE, h->nu, state(0), state(0) + 3 * n, h->lam,
+                                                  h->mu);
   box_init_kernel<<<(h->nsteps + 1 + 127) / 128, 128, 0, st>>>(h->box, h->nsteps + 1);
-  raster_kernel<<<blocks_for(n), kThreads, 0, st>>>(d, h->xs[0], h->v0, h->gsum[0], h->box);
+  raster_kernel<<<blocks_for(n), kThreads, 0, st>>>(d, state(0), h->v0, h->gsum[0], h->box);
   for (uint32_t s = 0; s < h->nsteps; ++s) {
     const float cdt = s == 0 ? 0.f : h->dt, ndt = h->dt;
     const bool ck = (s % h->every) == 0;
@@ -564,20 +574,15 @@ cudaError_t enqueue_rollout(ckmpm_diff* h) {
     float4* vs = ck ? h->ckvel + static_cast<size_t>(k) * nn : h->vel;
     // grid update of substep s (reads gsum[s & 1] in box s; resets box s + 1)
     grid_kernel<<<ctas, 256, 0, st>>>(d, h->gsum[s & 1], h->box + 6 * s, cdt, vs);
-    float* in = h->xs[s & 1];
-    float* outp = h->xs[(s + 1) & 1];
-    if (ck) {
-      e = cudaMemcpyAsync(h->ck + static_cast<size_t>(k) * 12 * n, in, sizeof(float) * 12 * n,
-                          cudaMemcpyDeviceToDevice, st);
-      if (e != cudaSuccess) return e;
-    }
+    float* in = state(s);
+    float* outp = state(s + 1);
     particle_kernel<<<blocks_for(n), kThreads, 0, st>>>(d, in, in + 3 * n, h->lam, h->mu, vs, cdt, ndt,
                                                         h->gsum[(s + 1) & 1], h->box + 6 * (s + 1), outp,
                                                         outp + 3 * n);
   }
   // Leave the last deposit's sums at zero (they are never read).
   grid_kernel<<<ctas, 256, 0, st>>>(d, h->gsum[h->nsteps & 1], h->box + 6 * h->nsteps, h->dt, h->vel);
-  const float* fin = h->xs[h->nsteps & 1];
+  const float* fin = state(h->nsteps);
   soa_to_aos_kernel<<<blocks_for(n), kThreads, 0, st>>>(n, 3, fin, h->xT);
   soa_to_aos_kernel<<<blocks_for(n), kThreads, 0, st>>>(n, 9, fin + 3 * n, h->FT);
   return cudaGetLastError();
@@ -605,20 +610,21 @@ cudaError_t enqueue_backward(ckmpm_diff* h) {
   for (int k = static_cast<int>(h->nseg) - 1; k >= 0; --k) {
     const uint32_t s0 = static_cast<uint32_t>(k) * h->every;
     const uint32_t s1 = std::min(h->nsteps, s0 + h->every);
-    // recompute: tape slot j = state of substep s0 + j; tapevel slot j = its node velocities
-    e = cudaMemcpyAsync(h->tape, h->ck + static_cast<size_t>(k) * 12 * n, sizeof(float) * 12 * n,
-                        cudaMemcpyDeviceToDevice, st);
-    if (e != cudaSuccess) return e;
+    // recompute: the segment's first state is its checkpoint, state s0 + j (j >= 1)
+    // tape slot j - 1; tapevel slot j holds the node velocities of substep s0 + j
+    auto statep = [&](uint32_t s) -> float* {
+      return s == s0 ? h->ck + static_cast<size_t>(k) * 12 * n : h->tape + static_cast<size_t>(s - s0 - 1) * 12 * n;
+    };
     auto velp = [&](uint32_t s) -> float4* {
       return s == s0 ? h->ckvel + static_cast<size_t>(k) * nn : h->tapevel + static_cast<size_t>(s - s0) * nn;
     };
     for (uint32_t s = s0; s < s1; ++s) {
       const float cdt = s == 0 ? 0.f : h->dt, ndt = h->dt;
-      float* in = h->tape + static_cast<size_t>(s - s0) * 12 * n;
+      float* in = statep(s);
       if (s > s0)
         grid_kernel<<<ctas, 256, 0, st>>>(d, h->gsum[s & 1], h->box + 6 * s, cdt, velp(s));
       if (s + 1 < s1) {
-        float* outp = h->tape + static_cast<size_t>(s - s0 + 1) * 12 * n;
+        float* outp = statep(s + 1);
         particle_kernel<<<blocks_for(n), kThreads, 0, st>>>(d, in, in + 3 * n, h->lam, h->mu, velp(s), cdt, ndt,
                                                             h->gsum[(s + 1) & 1], h->box + 6 * (s + 1), outp,
                                                             outp + 3 * n);
@@ -627,7 +633,7 @@ cudaError_t enqueue_backward(ckmpm_diff* h) {
     // reverse through the segment
     for (int s = static_cast<int>(s1) - 1; s >= static_cast<int>(s0); --s) {
       const float cdt = s == 0 ? 0.f : h->dt, ndt = h->dt;
-      const float* in = h->tape + static_cast<size_t>(s - s0) * 12 * n;
+      const float* in = statep(static_cast<uint32_t>(s));
       particle_adjoint_kernel<<<blocks_for(n), kThreads, 0, st>>>(d, in, in + 3 * n, h->lam, h->mu, velp(s), cdt, ndt,
                                                                   first ? nullptr : h->gadj, h->xb, h->Fb, h->mub,
                                                                   h->lamb, h->vbar);

@@ -5,11 +5,13 @@ No counterpart in the reference.  The CUDA library runs the forward on a dense
 grid of the scene's domain with exact fixed-point deposits and keeps a
 checkpoint every `checkpoint_every` substeps; backward recomputes one segment
 at a time from its checkpoint and runs the adjoint of P2G, the grid update,
-G2P and the SVD-based stress (ckmpm_b200/csrc/diff_math.cuh).  Inputs and
+G2P and the SVD-based stress (ckmpm_b200/csrc/diff_math.cuh).  By default the
+interval is the smallest whose checkpoints and tape fit in half of the free
+device memory: 1 (the whole rollout kept, nothing recomputed) whenever it fits.  Inputs and
 outputs are CUDA float32 tensors; the work is ordered on torch's current
 stream.
 
-    sim = DiffRollout(cfg, n, mass, volume, nu=0.3, nsteps=200, dt=1e-4, checkpoint_every=20)
+    sim = DiffRollout(cfg, n, mass, volume, nu=0.3, nsteps=200, dt=1e-4)
     xT, FT = rollout(sim, x0, v0, logE)        # x0, v0: [n, 3]; logE: [n]
     loss = ((xT.mean(0) - target) ** 2).sum()
     loss.backward()                            # gradients for x0, v0, logE
@@ -56,12 +58,40 @@ def _ptr(t: torch.Tensor | None):
     return C.c_void_p(t.data_ptr())
 
 
+def rollout_bytes(config: MPMConfig, n: int, nsteps: int, every: int) -> int:
+    """Device bytes of the checkpoints and the recomputation tape of a rollout of n
+    particles over nsteps substeps with a checkpoint every `every` substeps: each
+    checkpoint holds x and F (48 B per particle) and the node velocities (16 B per
+    node of both staggered grids of the domain); the tape holds every - 1 states
+    and every node-velocity slots."""
+    nodes = 2
+    for b in config.domain_blocks:
+        nodes *= 4 * int(b)
+    state, vel = 48 * n, 16 * nodes
+    nseg = -(-nsteps // every)
+    return nseg * (state + vel) + max(every - 1, 1) * state + every * vel
+
+
+def auto_checkpoint_interval(config: MPMConfig, n: int, nsteps: int, budget_bytes: int) -> int:
+    """The smallest checkpoint interval whose checkpoints and tape fit in budget_bytes;
+    when none does, the interval that needs the least memory."""
+    for every in range(1, nsteps + 1):
+        if rollout_bytes(config, n, nsteps, every) <= budget_bytes:
+            return every
+    return min(range(1, nsteps + 1), key=lambda k: (rollout_bytes(config, n, nsteps, k), k))
+
+
 class DiffRollout:
-    """A differentiable rollout of n fixed-corotated particles (ckmpm_diff_* handle)."""
+    """A differentiable rollout of n fixed-corotated particles (ckmpm_diff_* handle).
+    checkpoint_every None picks the interval by memory (auto_checkpoint_interval
+    over half of the device's free memory)."""
 
     def __init__(self, config: MPMConfig, n: int, mass: float, volume: float, nu: float = 0.3, nsteps: int = 200,
-                 dt: float = 1e-4, checkpoint_every: int = 20):
+                 dt: float = 1e-4, checkpoint_every: int | None = None):
         self.config, self.n, self.nsteps, self.dt = config, n, nsteps, dt
+        if checkpoint_every is None:
+            free, _ = torch.cuda.mem_get_info(config.device)
+            checkpoint_every = auto_checkpoint_interval(config, n, nsteps, free // 2)
         self.checkpoint_every = checkpoint_every
         self._h = C.c_void_p()
         desc = config.to_c()

@@ -68,3 +68,22 @@ def test_adjoint_matches_central_differences(harness, nsteps):
         ad = float((grad * d).sum())
         print(f"{nsteps} substeps, {name}: fd {fd:.10e} adjoint {ad:.10e}")
         assert abs(fd - ad) <= 1e-6 * abs(fd) + 1e-9, (name, fd, ad)
+
+
+def test_checkpoint_interval_by_memory():
+    """The rollout keeps every substep when its checkpoints fit the budget and
+    picks the smallest interval that fits otherwise (host logic, no GPU)."""
+    from ckmpm_b200.diff import auto_checkpoint_interval, rollout_bytes
+    from ckmpm_b200.engine import MPMConfig
+    cfg = MPMConfig(dx=1 / 64, domain_blocks=(16, 16, 16))
+    n, nsteps = 50_626, 200
+    full = rollout_bytes(cfg, n, nsteps, 1)
+    # 200 checkpoints of x, F (48 B per particle) and 2 x 64^3 node velocities (16 B)
+    assert full == 200 * (48 * n + 16 * 2 * 64 ** 3) + 48 * n + 16 * 2 * 64 ** 3
+    assert auto_checkpoint_interval(cfg, n, nsteps, full) == 1
+    k = auto_checkpoint_interval(cfg, n, nsteps, full // 4)
+    assert k > 1 and rollout_bytes(cfg, n, nsteps, k) <= full // 4 < rollout_bytes(cfg, n, nsteps, k - 1)
+    # nothing fits: the interval of least memory (the checkpoints fall with it, the tape grows)
+    least = auto_checkpoint_interval(cfg, n, nsteps, 0)
+    assert all(rollout_bytes(cfg, n, nsteps, least) <= rollout_bytes(cfg, n, nsteps, e) for e in range(1, nsteps + 1))
+    assert 1 < least < nsteps

@@ -7,10 +7,12 @@
     of the oracle (per-particle Lame parameters, double inputs): within 1e-3
     relative, for directions in v0, log E and x0 and a linear functional of
     (xT, FT) that depends on all of them;
-  * checkpointing: every-10, every-7 and one-segment runs give the same xT and
-    the same gradients, bit for bit (the forward's node sums and the adjoint's
+  * checkpointing: every-10, every-7, every-1 (the whole tape kept, no
+    recomputation) and one-segment runs give the same xT and the same
+    gradients, bit for bit (the forward's node sums and the adjoint's
     node-velocity sums are both exact integers), and so does a repeated run;
-  * at the config-5 scale (50.6k particles, 200 substeps, checkpoint every 20):
+  * at the config-5 scale (50.6k particles, 200 substeps, a checkpoint at every
+    substep):
     per-particle d loss / d log E and d loss / d v0 on a seeded sample of
     particles against FP64 central differences of the oracle.
 """
@@ -143,7 +145,7 @@ def test_checkpointing_gives_the_same_rollout_and_gradients(engine_lib):
     import torch
     from ckmpm_b200.diff import rollout
     out = []
-    for every in (10, 40, 7):
+    for every in (10, 40, 7, 1):
         d = small_case(every=every)
         sim = make_sim(d)
         x0, v0, lE = (t.requires_grad_() for t in tensors(d))
@@ -196,7 +198,7 @@ def _oracle_loss(args):
 
 
 def test_config5_per_particle_gradients_against_fp64_differences(engine_lib, oracle_mod):
-    """The config-5 rollout (50.6k particles, 200 substeps, checkpoint every 20): d loss / d log E_p
+    """The config-5 rollout (50.6k particles, 200 substeps, every substep kept): d loss / d log E_p
     and d loss / d v0_p (along a random unit direction) for 6 seeded particles p, against FP64
     central differences of the oracle's rollout with per-particle Lame parameters (24 rollouts of
     50.6k particles x 200 substeps, run in a spawn pool on the host cores).  The config-5 loss
