@@ -1,6 +1,5 @@
 // Host side of the B200 CK-MPM engine: scene/model lifetime, device memory,
 // setup, CUDA-graph substep replay and the C ABI declared in include/ckmpm.h.
-#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -48,10 +47,7 @@ struct ModelHost {
   uint32_t* oid = nullptr;
   uint32_t* oflag = nullptr;  // input-order export: live flags by id, then their exclusive scan
   uint32_t* opos = nullptr;
-  void* oscan = nullptr;
-  size_t oscan_bytes = 0;
-  void* sort_temp = nullptr;
-  size_t sort_temp_bytes = 0;
+  uint32_t* oscan = nullptr;  // the export scan's tile sums (scan_tiles(n) words)
   // Asynchronous export: recorded on the copy stream after this model's
   // staging buffer has been copied out.
   cudaEvent_t ev_copied = nullptr;
@@ -448,8 +444,7 @@ static void io_layout(ModelHost& m, bool track, Carve& c) {
   m.oid = c.take<uint32_t>(n);
   m.oflag = track ? c.take<uint32_t>(n) : nullptr;
   m.opos = track ? c.take<uint32_t>(n) : nullptr;
-  m.oscan = track ? c.take<unsigned char>(m.oscan_bytes) : nullptr;
-  m.sort_temp = c.take<unsigned char>(m.sort_temp_bytes);
+  m.oscan = track ? c.take<uint32_t>(scan_tiles(static_cast<uint32_t>(n))) : nullptr;
 }
 
 // Places a model's simulation state: the double-buffered particle arrays and
@@ -487,7 +482,8 @@ static void state_layout(ModelHost& m, uint32_t nbd, bool track, Carve& c) {
   d.sstart = batch ? c.take<uint32_t>(m.sstart.size()) : nullptr;
 }
 
-// The setup sort's keys and values: four arrays of n u32 inside oF (9 n floats).
+// Setup's work arrays, three of n u32 inside oF (9 n floats): 0 the particles'
+// flat block indices, 1 the per-slot placement cursors, 2 the particle order.
 static uint32_t* sort_array(const ModelHost& m, int k) {
   return reinterpret_cast<uint32_t*>(m.oF) + static_cast<size_t>(k) * m.n;
 }
@@ -500,13 +496,6 @@ static cudaError_t stage_inputs(ckmpm_scene* s, ModelHost& m, const float* x, co
   cudaError_t e = cudaSetDevice(s->desc.device);
   if (e != cudaSuccess) return e;
   const bool track = m.mat.kind == kMixedKind || (s->desc.flags & CKMPM_FLAG_TRACK_IDS) != 0;
-  const int n = static_cast<int>(m.n);
-  cub::DoubleBuffer<uint32_t> keys(nullptr, nullptr), vals(nullptr, nullptr);
-  e = cub::DeviceRadixSort::SortPairs(nullptr, m.sort_temp_bytes, keys, vals, n, 0, 32, s->stream);
-  if (e == cudaSuccess && track)
-    e = cub::DeviceScan::ExclusiveSum(nullptr, m.oscan_bytes, static_cast<uint32_t*>(nullptr),
-                                      static_cast<uint32_t*>(nullptr), n, s->stream);
-  if (e != cudaSuccess) return e;
   Carve size;
   io_layout(m, track, size);
   e = cudaMalloc(&m.io, size.off);
@@ -698,19 +687,22 @@ ckmpm_status ckmpm_setup(ckmpm_scene* s) {
                                  cudaMemcpyHostToDevice, s->stream));
     }
 
-    // Bin, radix-sort by colour-major block index, compact; the inputs and the
-    // sort's arrays live in the model's I/O arena.  Nothing here waits for the
-    // device: kernels that depend on the binned count read it on the device.
-    cub::DoubleBuffer<uint32_t> keys(sort_array(m, 0), sort_array(m, 1)), vals(sort_array(m, 2), sort_array(m, 3));
-    setup_bin_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(s->sc, n, m.ox, d.sstart, keys.Current(), vals.Current(),
-                                                             d.dense_total);
-    size_t temp_bytes = m.sort_temp_bytes;
-    CK_CUDA(s, cub::DeviceRadixSort::SortPairs(m.sort_temp, temp_bytes, keys, vals, static_cast<int>(n), 0, 32,
-                                               s->stream));
+    // Bin, compact into the colour-major block list, place every particle in
+    // its block's range and order each range by input index (the order a
+    // stable sort by block gives); the inputs and these arrays live in the
+    // model's I/O arena.  Nothing here waits for the device: kernels that
+    // depend on the binned count read it on the device.
+    uint32_t* flat = sort_array(m, 0);
+    uint32_t* cursor = sort_array(m, 1);
+    uint32_t* perm = sort_array(m, 2);
+    setup_bin_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(s->sc, n, m.ox, d.sstart, flat, d.dense_total);
     CK_CUDA(s, launch_compact(s, m, d.bl[0]));
+    CK_CUDA(s, cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * d.cap_slots, s->stream));
+    setup_place_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(n, flat, d.bl[0], cursor, perm);
+    setup_order_kernel<256><<<s->sm_count * 4, 256, 0, s->stream>>>(d.bl[0], perm, s->scal);
     const float aux0 = initial_aux(m.mat);
     setup_gather_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(
-        d, s->nstack, n, vals.Current(), m.ox, m.ov, m.nv, aux0,
+        d, s->nstack, n, perm, m.ox, m.ov, m.nv, aux0,
         (s->sc.rigid && m.mat.kind == CKMPM_VON_MISES) ? s->rigid_count : 0u, d.bl[0].nparticles);
     // Identity previous-step structures in list 1.
     CK_CUDA(s, cudaMemcpyAsync(d.bl[1].table, d.bl[0].table, sizeof(int32_t) * nbd, cudaMemcpyDeviceToDevice,
@@ -937,10 +929,10 @@ static cudaError_t enqueue_export(ckmpm_scene* s, ModelHost& m, bool x, bool v, 
     if (n_upper)
       mark_ids_kernel<<<(n_upper + 255) / 256, 256, 0, s->stream>>>(n_upper, m.oid, m.oflag,
                                                                     static_cast<uint32_t>(cap_p), n_dev);
-    size_t tb = m.oscan_bytes;
-    if ((e = cub::DeviceScan::ExclusiveSum(m.oscan, tb, m.oflag, m.opos, static_cast<int>(cap_p), s->stream)) !=
-        cudaSuccess)
-      return e;
+    const uint32_t ntiles = scan_tiles(static_cast<uint32_t>(cap_p));
+    scan_reduce_kernel<<<ntiles, kScanThreads, 0, s->stream>>>(m.oflag, static_cast<uint32_t>(cap_p), m.oscan);
+    scan_sums_kernel<<<1, kScanThreads, 0, s->stream>>>(m.oscan, ntiles);
+    scan_apply_kernel<<<ntiles, kScanThreads, 0, s->stream>>>(m.oflag, static_cast<uint32_t>(cap_p), m.oscan, m.opos);
     dest = m.opos;
   }
   probe_kernel<kProbeThreads><<<pg, pb, kSmemVTile, s->stream>>>(s->sc, m.dev, s->grid, s->scal, x ? m.ox : nullptr,

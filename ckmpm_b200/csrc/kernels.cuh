@@ -1161,6 +1161,62 @@ __global__ void __launch_bounds__(kCompactThreads)
   }
 }
 
+// Exclusive prefix sum of n 32-bit values in three launches: per-tile sums,
+// one CTA scanning the tile sums in place, then each tile scanned from its
+// offset.  The export in input order uses it to place each live id.
+constexpr int kScanThreads = kCompactThreads;
+constexpr int kScanPerThread = 8;
+constexpr uint32_t kScanTile = kScanThreads * kScanPerThread;
+
+__host__ __device__ constexpr uint32_t scan_tiles(uint32_t n) { return (n + kScanTile - 1) / kScanTile; }
+
+__global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(const uint32_t* __restrict__ in, uint32_t n,
+                                                                    uint32_t* __restrict__ sums) {
+  __shared__ uint32_t scratch[128];
+  const uint32_t t0 = blockIdx.x * kScanTile + threadIdx.x * kScanPerThread;
+  uint32_t v = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPerThread; ++k)
+    if (t0 + k < n) v += in[t0 + k];
+  v = block_reduce_sum(v, scratch);
+  if (threadIdx.x == 0) sums[blockIdx.x] = v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_sums_kernel(uint32_t* __restrict__ sums, uint32_t ntiles) {
+  __shared__ uint32_t scratch[128];
+  uint32_t carry = 0;
+  for (uint32_t b = 0; b < ntiles; b += kScanThreads) {
+    const uint32_t i = b + threadIdx.x;
+    const uint32_t v = i < ntiles ? sums[i] : 0u;
+    uint32_t e, unused;
+    block_scan2(v, 0u, e, unused, scratch);
+    const uint32_t total = block_reduce_sum(v, scratch);
+    if (i < ntiles) sums[i] = carry + e;
+    carry += total;
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const uint32_t* __restrict__ in, uint32_t n,
+                                                                   const uint32_t* __restrict__ offsets,
+                                                                   uint32_t* __restrict__ out) {
+  __shared__ uint32_t scratch[128];
+  const uint32_t t0 = blockIdx.x * kScanTile + threadIdx.x * kScanPerThread;
+  uint32_t v[kScanPerThread], sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPerThread; ++k) {
+    v[k] = t0 + k < n ? in[t0 + k] : 0u;
+    sum += v[k];
+  }
+  uint32_t e, unused;
+  block_scan2(sum, 0u, e, unused, scratch);
+  uint32_t run = offsets[blockIdx.x] + e;
+#pragma unroll
+  for (int k = 0; k < kScanPerThread; ++k) {
+    if (t0 + k < n) out[t0 + k] = run;
+    run += v[k];
+  }
+}
+
 // Advance the substep counter and roll the dt pair: currentDt = nextDt, then
 // the clock advances by it (include/mpm_engine.cuh:869-871).
 // End of setup: the particles dropped while binning and the rigid velocity.
@@ -1242,29 +1298,89 @@ __global__ void adaptive_dt_kernel(Scalars* scal, float dx, float cfl, float dt_
 }
 
 // ------------------------------------------------------------------ setup
-// Initial binning key of every particle: its colour-major traversal index
-// (0xFFFFFFFF outside the domain), and the per-block count.  Replaces
-// ActivateBlocksWithParticles + BuildParticleCellBucket
+// Initial binning of every particle: its block's flat index in the dense
+// table (0xFFFFFFFF outside the domain or not finite), and the per-block
+// count.  With the compaction, setup_place_kernel and setup_order_kernel it
+// replaces ActivateBlocksWithParticles + BuildParticleCellBucket
 // (include/mpm_algorithm.cuh:586-626,713-736).
 __global__ void setup_bin_kernel(SceneDev sc, uint32_t n, const float* __restrict__ x, const uint32_t* __restrict__ sstart,
-                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t* __restrict__ total) {
+                                 uint32_t* __restrict__ flat, uint32_t* __restrict__ total) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
   const int cx = static_cast<int>(px * sc.inv_dx + 0.25f), cy = static_cast<int>(py * sc.inv_dx + 0.25f),
             cz = static_cast<int>(pz * sc.inv_dx + 0.25f);
   const int bx = trunc_div4(cx - 2), by = trunc_div4(cy - 2), bz = trunc_div4(cz - 2);
-  uint32_t key = 0xFFFFFFFFu;
+  uint32_t f = 0xFFFFFFFFu;
   const bool finite = isfinite(px) && isfinite(py) && isfinite(pz) && px >= 0.f && py >= 0.f && pz >= 0.f;
   if (finite && in_domain(sc, bx, by, bz)) {
     const int w = sstart ? scene_of(sstart, sc.nstack, i) : 0;
-    const int c = colour_of(bx, by, bz);
-    const uint32_t nz = sc.cdims[c][2], ny = sc.cdims[c][1];
-    key = sc.cbase[c] + w * sc.ccount[c] + ((bx >> 1) * ny + (by >> 1)) * nz + (bz >> 1);
-    atomicAdd(total + flat_block(sc, w, bx, by, bz), 1u);
+    f = static_cast<uint32_t>(flat_block(sc, w, bx, by, bz));
+    atomicAdd(total + f, 1u);
   }
-  keys[i] = key;
-  vals[i] = i;
+  flat[i] = f;
+}
+
+// Setup placement: after the compaction has laid out the block list (colour-
+// major, each block's range [start, start + count)), particle i takes the next
+// free position of its block's range.  Inputs usually arrive in spatial order,
+// so the lanes of a warp mostly share a block: one atomic per distinct block of
+// the warp takes the positions of all its lanes.  The order the atomics hand
+// positions out in is not deterministic; setup_order_kernel removes it.
+__global__ void setup_place_kernel(uint32_t n, const uint32_t* __restrict__ flat, BlockListDev list,
+                                   uint32_t* __restrict__ cursor, uint32_t* __restrict__ perm) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  int32_t slot = -1;
+  if (i < n) {
+    const uint32_t f = flat[i];
+    if (f != 0xFFFFFFFFu) slot = list.table[f];
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t group = __match_any_sync(0xffffffffu, slot);
+  const uint32_t leader = __ffs(group) - 1u;
+  uint32_t base = 0;
+  if (slot >= 0 && lane == leader) base = atomicAdd(cursor + slot, static_cast<uint32_t>(__popc(group)));
+  base = __shfl_sync(0xffffffffu, base, static_cast<int>(leader));
+  if (slot >= 0) perm[list.start[slot] + base + __popc(group & ((1u << lane) - 1u))] = i;
+}
+
+// Setup ordering: each block's range sorted by input index (bitonic sort in
+// shared memory, one block at a time per CTA), so the particles of a block sit
+// in input order -- the order a stable sort by block gives, whatever order the
+// placement's atomics ran in.  A block above kMaxParticlesPerBlock particles
+// cannot be held and is reported as a capacity overflow.
+template <int NT>
+__global__ void __launch_bounds__(NT) setup_order_kernel(BlockListDev list, uint32_t* __restrict__ perm, Scalars* scal) {
+  __shared__ uint32_t s[kMaxParticlesPerBlock];
+  const uint32_t nb = *list.nblocks;
+  for (uint32_t slot = blockIdx.x; slot < nb; slot += gridDim.x) {
+    const uint32_t n = list.count[slot], start = list.start[slot];
+    if (n > static_cast<uint32_t>(kMaxParticlesPerBlock)) {
+      if (threadIdx.x == 0) set_status(scal, kStatusCapacity);
+      continue;
+    }
+    uint32_t m = 1;
+    while (m < n) m <<= 1;
+    for (uint32_t i = threadIdx.x; i < m; i += NT) s[i] = i < n ? perm[start + i] : 0xFFFFFFFFu;
+    __syncthreads();
+    for (uint32_t k = 2; k <= m; k <<= 1) {
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        for (uint32_t i = threadIdx.x; i < m; i += NT) {
+          const uint32_t l = i ^ j;
+          if (l > i) {
+            const uint32_t a = s[i], b = s[l];
+            if ((a > b) == ((i & k) == 0)) {
+              s[i] = b;
+              s[l] = a;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (uint32_t i = threadIdx.x; i < n; i += NT) perm[start + i] = s[i];
+    __syncthreads();
+  }
 }
 
 // Sorted initial state: x from the input, F = I, aux = logJp0 (0), alpha0,
@@ -1279,6 +1395,7 @@ __global__ void setup_gather_kernel(ModelDev md, uint32_t nstack, uint32_t n, co
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || (n_dev && i >= *n_dev)) return;
   const uint32_t s = perm[i];
+  if (s >= md.cap_particles) return;  // a position the placement never filled
   StateDev st = md.st[0];
   st.x[0][i] = x[3 * s];
   st.x[1][i] = x[3 * s + 1];

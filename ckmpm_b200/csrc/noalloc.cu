@@ -7,7 +7,7 @@
 // cannot afford the device-wide synchronisation a cudaMalloc / cudaFree may
 // cause.  For them this entry point runs a complete small simulation -- setup
 // and nsteps substeps of one model -- with every piece of scratch memory
-// (grid, block tables, index lists, sort buffers, work counters, flags) taken
+// (grid, block tables, index lists, setup ordering buffers, work counters, flags) taken
 // from one file-scope __device__ array of fixed size.  The caller passes its
 // inputs and outputs as device pointers.  The same kernels as the allocating
 // path run in the same order, so the outputs match ckmpm_create /
@@ -32,7 +32,6 @@ namespace {
 
 constexpr uint32_t kNoAllocMaxParticles = 65536;
 constexpr uint32_t kNoAllocMaxDomainBlocks = 4096;
-constexpr size_t kNoAllocCubTempBytes = size_t(4) << 20;
 constexpr int kNoAllocMaxDevices = 64;
 
 constexpr size_t na_align(size_t b) { return (b + 255) & ~size_t(255); }
@@ -51,7 +50,8 @@ constexpr size_t kNoAllocScratchBytes =
     2 * kNaGrid + 2 * kNaDomainU32 + na_align(sizeof(Scalars)) + 2 * kNaState + 2 * kNaBlockList +
     kNaDomainU32 /*dense totals*/ + na_align(sizeof(uint32_t) * 2 * 64) /*tile sums*/ + na_align(4) /*ticket*/ +
     3 * kNaParticleU32 /*initial velocities*/ +
-    4 * kNaParticleU32 /*sort keys and values*/ + kNoAllocCubTempBytes + 18 * kNaParticleU32 /*export*/;
+    3 * kNaParticleU32 /*setup: flat block indices, placement cursors, particle order*/ +
+    18 * kNaParticleU32 /*export*/;
 
 static_assert(kNoAllocScratchBytes < (size_t(56) << 20), "no-alloc scratch must stay modest");
 
@@ -243,11 +243,9 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   d.tile_sums = cv.take<uint32_t>(2 * 64);
   d.ticket = cv.take<uint32_t>(1);
   d.vel_in = cv.take<float>(3 * size_t(kNoAllocMaxParticles));
-  uint32_t* sort_keys_in = cv.take<uint32_t>(kNoAllocMaxParticles);
-  uint32_t* sort_keys_out = cv.take<uint32_t>(kNoAllocMaxParticles);
-  uint32_t* sort_vals_in = cv.take<uint32_t>(kNoAllocMaxParticles);
-  uint32_t* sort_vals_out = cv.take<uint32_t>(kNoAllocMaxParticles);
-  void* cub_temp = cv.take<unsigned char>(kNoAllocCubTempBytes);
+  uint32_t* flat = cv.take<uint32_t>(kNoAllocMaxParticles);
+  uint32_t* cursor = cv.take<uint32_t>(kNoAllocMaxParticles);
+  uint32_t* perm = cv.take<uint32_t>(kNoAllocMaxParticles);
   float* ex = cv.take<float>(3 * size_t(kNoAllocMaxParticles));
   float* ev = cv.take<float>(3 * size_t(kNoAllocMaxParticles));
   float* eF = cv.take<float>(9 * size_t(kNoAllocMaxParticles));
@@ -267,13 +265,6 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   d.flush_ratio = 1.0;
   const uint32_t ntiles = (nbd + kCompactTile - 1) / kCompactTile;
 
-  size_t temp_bytes = 0;
-  if (cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, sort_keys_in, sort_keys_out, sort_vals_in, sort_vals_out,
-                                      static_cast<int>(n), 0, 32, st) !=
-          cudaSuccess ||
-      temp_bytes > kNoAllocCubTempBytes)
-    return na_fail(message, CKMPM_ERR_CAPACITY, "sort scratch larger than the reserved region");
-
 #define NA_CUDA(call)                                                   \
   do {                                                                  \
     if ((call) != cudaSuccess) return na_fail(message, CKMPM_ERR_CUDA, #call " failed"); \
@@ -289,14 +280,15 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
   NA_CUDA(cudaMemsetAsync(d.dense_total, 0, sizeof(uint32_t) * nbd, st));
   NA_CUDA(cudaMemsetAsync(d.ticket, 0, sizeof(uint32_t), st));
 
-  // Setup: bin, sort by colour-major block index, compact, gather, identity
-  // previous step, initial grid -- the sequence of ckmpm_setup.
-  setup_bin_kernel<<<(n + 255) / 256, 256, 0, st>>>(sc, n, x, nullptr, sort_keys_in, sort_vals_in, d.dense_total);
-  NA_CUDA(cub::DeviceRadixSort::SortPairs(cub_temp, temp_bytes, sort_keys_in, sort_keys_out, sort_vals_in,
-                                          sort_vals_out, static_cast<int>(n), 0, 32, st));
+  // Setup: bin, compact, place and order each block's particles, gather,
+  // identity previous step, initial grid -- the sequence of ckmpm_setup.
+  setup_bin_kernel<<<(n + 255) / 256, 256, 0, st>>>(sc, n, x, nullptr, flat, d.dense_total);
   compact_reduce_kernel<<<ntiles, kCompactThreads, 0, st>>>(sc, d.dense_total, d.tile_sums);
   compact_scatter_kernel<<<ntiles, kCompactThreads, 0, st>>>(sc, d.dense_total, d.tile_sums, d.bl[0], d.cap_slots,
                                                              d.ticket, scal);
+  NA_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * d.cap_slots, st));
+  setup_place_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, flat, d.bl[0], cursor, perm);
+  setup_order_kernel<256><<<ctas, 256, 0, st>>>(d.bl[0], perm, scal);
   uint32_t counts[2] = {0, 0};
   NA_CUDA(cudaMemcpyAsync(&counts[0], d.bl[0].nblocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   NA_CUDA(cudaMemcpyAsync(&counts[1], d.bl[0].nparticles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -306,7 +298,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
                      : material->kind == CKMPM_NACC ? material->p[2]
                      : material->kind == CKMPM_VON_MISES ? 1.f : 0.f;
   if (n_valid > 0)
-    setup_gather_kernel<<<(n_valid + 255) / 256, 256, 0, st>>>(d, 1, n_valid, sort_vals_out, x, v, nv, aux0, 0u);
+    setup_gather_kernel<<<(n_valid + 255) / 256, 256, 0, st>>>(d, 1, n_valid, perm, x, v, nv, aux0, 0u);
   NA_CUDA(cudaMemcpyAsync(d.bl[1].table, d.bl[0].table, sizeof(int32_t) * nbd, cudaMemcpyDeviceToDevice, st));
   NA_CUDA(cudaMemcpyAsync(d.bl[1].start, d.bl[0].start, sizeof(uint32_t) * d.cap_slots, cudaMemcpyDeviceToDevice, st));
   NA_CUDA(cudaMemcpyAsync(d.bl[1].count, d.bl[0].count, sizeof(uint32_t) * d.cap_slots, cudaMemcpyDeviceToDevice, st));
