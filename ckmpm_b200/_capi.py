@@ -47,8 +47,8 @@ EXPORTED = (
     "ckmpm_get_state", "ckmpm_get_blocks", "ckmpm_get_counters", "ckmpm_get_dt",
     "ckmpm_step_profiled", "ckmpm_debug_constitutive", "ckmpm_destroy", "ckmpm_last_error",
     "ckmpm_version", "ckmpm_simulate_noalloc", "ckmpm_create_batch", "ckmpm_add_batch", "ckmpm_get_blocks_in",
-    "ckmpm_set_tuning", "ckmpm_get_tuning", "ckmpm_autotune", "ckmpm_checkpoint_bytes", "ckmpm_checkpoint_save",
-    "ckmpm_checkpoint_restore", "ckmpm_diff_create", "ckmpm_diff_forward", "ckmpm_diff_backward", "ckmpm_diff_timing",
+    "ckmpm_set_tuning", "ckmpm_set_reorder_interval", "ckmpm_get_tuning", "ckmpm_autotune", "ckmpm_checkpoint_bytes",
+    "ckmpm_checkpoint_save", "ckmpm_checkpoint_restore", "ckmpm_diff_create", "ckmpm_diff_forward", "ckmpm_diff_backward", "ckmpm_diff_timing",
     "ckmpm_diff_last_error", "ckmpm_diff_destroy", "ckmpm_set_rigid", "ckmpm_set_rigid_velocity", "ckmpm_get_time",
     "ckmpm_set_boundary_field", "ckmpm_export_positions_async", "ckmpm_export_wait",
     "ckmpm_dd_blocks", "ckmpm_dd_mark", "ckmpm_dd_pack", "ckmpm_dd_unpack",
@@ -144,6 +144,7 @@ def lib() -> C.CDLL:
         L.ckmpm_add_batch.argtypes = [P, C.c_uint32, C.POINTER(BatchScene), f32p, f32p]
         L.ckmpm_get_blocks_in.argtypes = [P, C.c_uint32, C.c_int32, C.c_int32, i32p, u32p, C.c_uint32, u32p]
         L.ckmpm_set_tuning.argtypes = [P, C.POINTER(Tuning)]
+        L.ckmpm_set_reorder_interval.argtypes = [P, C.c_uint32]
         L.ckmpm_get_tuning.argtypes = [P, C.POINTER(Tuning), u32p]
         L.ckmpm_autotune.argtypes = [P, C.c_uint32, C.c_float, C.POINTER(Tuning), C.c_uint32, u32p,
                                      C.POINTER(Tuning)]

@@ -1344,14 +1344,89 @@ __global__ void setup_place_kernel(uint32_t n, const uint32_t* __restrict__ flat
   if (slot >= 0) perm[list.start[slot] + base + __popc(group & ((1u << lane) - 1u))] = i;
 }
 
-// Setup ordering: each block's range sorted by input index (bitonic sort in
-// shared memory, one block at a time per CTA), so the particles of a block sit
-// in input order -- the order a stable sort by block gives, whatever order the
-// placement's atomics ran in.  A block above kMaxParticlesPerBlock particles
+// Bitonic sort of m (a power of two, <= kMaxParticlesPerBlock) 32-bit values in
+// shared memory, ascending; every thread of the CTA takes part, one
+// compare-exchange pair per thread and stage (m / 2 pairs).
+template <int NT>
+__device__ __forceinline__ void block_bitonic_sort(uint32_t* v, uint32_t m) {
+  for (uint32_t k = 2; k <= m; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      const uint32_t lj = 31u - __clz(j);
+      for (uint32_t p = threadIdx.x; p < (m >> 1); p += NT) {
+        const uint32_t i = ((p >> lj) << (lj + 1)) | (p & (j - 1u));
+        const uint32_t l = i | j;
+        const uint32_t a = v[i], b = v[l];
+        if ((a > b) == ((i & k) == 0)) {
+          v[i] = b;
+          v[l] = a;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Sort keys of the setup order for n particles whose cells (0..63) are cell[0..n):
+// key[j] = ((r * 64 + cell[j]) << 12) | j, r the number of i < j in the same
+// cell, and key[j] = 0xFFFFFFFF for n <= j < m.  Ranks are taken NT particles
+// at a time in order of j: within a warp from the lanes of the same cell
+// (__match_any_sync), across the warps of a chunk and across chunks from
+// per-cell counters.  wcnt holds NT / 32 x 64 counters, base 64.
+template <int NT>
+__device__ __forceinline__ void cell_order_keys(const uint8_t* cell, uint32_t n, uint32_t m, uint32_t* key,
+                                                uint32_t* wcnt, uint32_t* base) {
+  const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  if (threadIdx.x < 64) base[threadIdx.x] = 0u;
+  for (uint32_t i = n + threadIdx.x; i < m; i += NT) key[i] = 0xFFFFFFFFu;
+  for (uint32_t b0 = 0; b0 < n; b0 += NT) {
+    for (uint32_t i = threadIdx.x; i < (NT / 32) * 64; i += NT) wcnt[i] = 0u;
+    __syncthreads();
+    const uint32_t j = b0 + threadIdx.x;
+    const uint32_t c = j < n ? cell[j] : 64u + lane;  // lanes past the end match nobody
+    const uint32_t mask = __match_any_sync(0xffffffffu, c);
+    const uint32_t below = __popc(mask & ((1u << lane) - 1u));
+    if (j < n && below == 0u) wcnt[w * 64 + c] = __popc(mask);
+    __syncthreads();
+    if (threadIdx.x < 64) {
+      uint32_t run = base[threadIdx.x];
+#pragma unroll
+      for (int q = 0; q < NT / 32; ++q) {
+        const uint32_t t = wcnt[q * 64 + threadIdx.x];
+        wcnt[q * 64 + threadIdx.x] = run;
+        run += t;
+      }
+      base[threadIdx.x] = run;
+    }
+    __syncthreads();
+    if (j < n) key[j] = (((wcnt[w * 64 + c] + below) * 64u + c) << 12) | j;
+  }
+  __syncthreads();
+}
+
+// Setup ordering of each block's range, in two sorts in shared memory:
+//  1. by input index, so nothing depends on the order the placement's atomics
+//     ran in;
+//  2. by (rank of the particle within its cell in that order, cell), with the
+//     block's 64 cells numbered x-major (16 x + 4 y + z): 32 consecutive
+//     particles then lie in the 32 different cells of one half block (2 x 4 x 4
+//     cells), one per cell as far as the counts allow.
+// The fused substep hands a warp 32 consecutive particles of a block, and each
+// of them adds to 16 nodes of the P2G tile with shared atomics; with the tile's
+// 68-word x planes the 32 cells of a half block fall in 32 different banks, while
+// particles stored in input (lattice) order put several lanes of a warp in the
+// same cell and serialise their atomics on the same words.  The substep's
+// rebinning keeps each block's particles in their order, so the layout persists
+// while particles stay in their blocks.  Results do not depend on the order (the
+// grid sums are exact integers).  A block above kMaxParticlesPerBlock particles
 // cannot be held and is reported as a capacity overflow.
 template <int NT>
-__global__ void __launch_bounds__(NT) setup_order_kernel(BlockListDev list, uint32_t* __restrict__ perm, Scalars* scal) {
+__global__ void __launch_bounds__(NT) setup_order_kernel(SceneDev sc, BlockListDev list, const float* __restrict__ x,
+                                                         uint32_t* __restrict__ perm, Scalars* scal) {
   __shared__ uint32_t s[kMaxParticlesPerBlock];
+  __shared__ uint32_t t[kMaxParticlesPerBlock];
+  __shared__ uint8_t cell[kMaxParticlesPerBlock];
+  __shared__ uint32_t wcnt[(NT / 32) * 64];
+  __shared__ uint32_t base[64];
   const uint32_t nb = *list.nblocks;
   for (uint32_t slot = blockIdx.x; slot < nb; slot += gridDim.x) {
     const uint32_t n = list.count[slot], start = list.start[slot];
@@ -1359,26 +1434,98 @@ __global__ void __launch_bounds__(NT) setup_order_kernel(BlockListDev list, uint
       if (threadIdx.x == 0) set_status(scal, kStatusCapacity);
       continue;
     }
+    const int4 key = list.keys[slot];
     uint32_t m = 1;
     while (m < n) m <<= 1;
     for (uint32_t i = threadIdx.x; i < m; i += NT) s[i] = i < n ? perm[start + i] : 0xFFFFFFFFu;
     __syncthreads();
-    for (uint32_t k = 2; k <= m; k <<= 1) {
-      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-        for (uint32_t i = threadIdx.x; i < m; i += NT) {
-          const uint32_t l = i ^ j;
-          if (l > i) {
-            const uint32_t a = s[i], b = s[l];
-            if ((a > b) == ((i & k) == 0)) {
-              s[i] = b;
-              s[l] = a;
-            }
-          }
-        }
-        __syncthreads();
-      }
+    block_bitonic_sort<NT>(s, m);
+    // Cell of each particle within the block (the binning's +dx/4 cell).
+    for (uint32_t i = threadIdx.x; i < n; i += NT) {
+      const uint32_t p = s[i];
+      const int lx = (static_cast<int>(x[3 * p] * sc.inv_dx + 0.25f) - 2 - 4 * key.x) & 3;
+      const int ly = (static_cast<int>(x[3 * p + 1] * sc.inv_dx + 0.25f) - 2 - 4 * key.y) & 3;
+      const int lz = (static_cast<int>(x[3 * p + 2] * sc.inv_dx + 0.25f) - 2 - 4 * key.z) & 3;
+      cell[i] = static_cast<uint8_t>(lx * 16 + ly * 4 + lz);
     }
-    for (uint32_t i = threadIdx.x; i < n; i += NT) perm[start + i] = s[i];
+    __syncthreads();
+    cell_order_keys<NT>(cell, n, m, t, wcnt, base);
+    block_bitonic_sort<NT>(t, m);
+    for (uint32_t i = threadIdx.x; i < n; i += NT) perm[start + i] = s[t[i] & 4095u];
+    __syncthreads();
+  }
+}
+
+// Re-layout of a model's particles between two substeps.  The setup order
+// (setup_order_kernel) puts the 32 particles a warp handles in 32 different
+// cells of a half block; the rebinning keeps each block's particles in their
+// order, but as particles change cells and blocks the layout fades (on the
+// sand column the fused substep's advantage over input order went from 7 % to
+// none between 800 and 1600 substeps).  Every so many substeps the host runs
+// this kernel before the next substep, whose block list is `parity`: each
+// block gathers its incoming particles (through the previous substep's
+// rebinning records, as the fused kernel does) into the other state buffer at
+// its own range, in the setup order -- by rank within its cell in incoming
+// order, then cell -- and the host copies that buffer back and makes the
+// previous-step lists the identity, as after setup.  Values are moved, never
+// changed; the simulation does not depend on the order.
+template <int NT>
+__global__ void __launch_bounds__(NT, 4) reorder_gather_kernel(SceneDev sc, ModelDev md, int parity, Scalars* scal) {
+  __shared__ uint32_t src_of[kMaxParticlesPerBlock];
+  __shared__ uint32_t key[kMaxParticlesPerBlock];
+  __shared__ uint8_t cell[kMaxParticlesPerBlock];
+  __shared__ uint32_t wcnt[(NT / 32) * 64];
+  __shared__ uint32_t base[64];
+  __shared__ SharedSmall sh;
+  const BlockListDev cur = md.bl[parity];
+  const BlockListDev prev = md.bl[parity ^ 1];
+  const StateDev sin = md.st[parity];
+  const StateDev sdst = md.st[parity ^ 1];
+  const uint32_t nb = *cur.nblocks;
+  for (uint32_t slot = blockIdx.x; slot < nb; slot += gridDim.x) {
+    const int4 k4 = cur.keys[slot];
+    const uint32_t start = cur.start[slot];
+    if (threadIdx.x < 32) incoming_groups(sc, prev, k4, sh.off, sh.idx, sh.src);
+    __syncthreads();
+    const uint32_t room = start < md.cap_particles ? md.cap_particles - start : 0u;
+    const uint32_t n = min(min(cur.count[slot], sh.off[27]), room);
+    if (n > static_cast<uint32_t>(kMaxParticlesPerBlock)) {
+      if (threadIdx.x == 0) set_status(scal, kStatusCapacity);
+      __syncthreads();
+      continue;
+    }
+    for (uint32_t j = threadIdx.x; j < n; j += NT) {
+      const int d = find_group(sh.off, j);
+      const uint32_t ii = sh.idx[d] + (j - sh.off[d]);
+      uint32_t iin = ii < md.cap_particles ? sh.src[d] + prev.idx[ii] : 0xFFFFFFFFu;
+      if (iin >= md.cap_particles) {  // corrupted record: flag, never read out of range
+        set_status(scal, kStatusConsistency);
+        iin = 0;
+      }
+      src_of[j] = iin;
+      // the cell within the block, as setup_order_kernel numbers it ((c - 2) mod 4 per axis)
+      const int lx = (static_cast<int>(sin.x[0][iin] * sc.inv_dx + 0.25f) - 2) & 3;
+      const int ly = (static_cast<int>(sin.x[1][iin] * sc.inv_dx + 0.25f) - 2) & 3;
+      const int lz = (static_cast<int>(sin.x[2][iin] * sc.inv_dx + 0.25f) - 2) & 3;
+      cell[j] = static_cast<uint8_t>(lx * 16 + ly * 4 + lz);
+    }
+    __syncthreads();
+    uint32_t m = 1;
+    while (m < n) m <<= 1;
+    cell_order_keys<NT>(cell, n, m, key, wcnt, base);
+    block_bitonic_sort<NT>(key, m);
+    // Replace each key by the source index it selects, then move one array at a
+    // time (few registers, many loads in flight).
+    for (uint32_t k = threadIdx.x; k < n; k += NT) key[k] = src_of[key[k] & 4095u];
+    __syncthreads();
+    for (int a = 0; a < 23; ++a) {
+      const float* from = a < 3 ? sin.x[a] : a < 12 ? sin.F[a - 3] : a == 12 ? sin.aux : a < 22 ? sin.Q[a - 13]
+                                                                               : reinterpret_cast<const float*>(sin.id);
+      float* to = a < 3 ? sdst.x[a] : a < 12 ? sdst.F[a - 3] : a == 12 ? sdst.aux : a < 22 ? sdst.Q[a - 13]
+                                                                      : reinterpret_cast<float*>(sdst.id);
+      if (!from) continue;
+      for (uint32_t k = threadIdx.x; k < n; k += NT) to[start + k] = from[key[k]];
+    }
     __syncthreads();
   }
 }

@@ -288,7 +288,7 @@ extern "C" ckmpm_status ckmpm_simulate_noalloc(const ckmpm_scene_desc* desc, con
                                                              d.ticket, scal);
   NA_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * d.cap_slots, st));
   setup_place_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, flat, d.bl[0], cursor, perm);
-  setup_order_kernel<256><<<ctas, 256, 0, st>>>(d.bl[0], perm, scal);
+  setup_order_kernel<256><<<ctas, 256, 0, st>>>(sc, d.bl[0], x, perm, scal);
   uint32_t counts[2] = {0, 0};
   NA_CUDA(cudaMemcpyAsync(&counts[0], d.bl[0].nblocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   NA_CUDA(cudaMemcpyAsync(&counts[1], d.bl[0].nparticles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));

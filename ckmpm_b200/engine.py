@@ -425,6 +425,11 @@ class Scene:
         t = capi.Tuning(threads, ctas_per_sm, graph_chunk, 0.0)
         capi.check(capi.lib().ckmpm_set_tuning(self._h, C.byref(t)), "ckmpm_set_tuning", self._h)
 
+    def set_reorder_interval(self, substeps: int) -> None:
+        """Substeps between re-layouts of each block's particles into the setup order
+        (default 128, 0 = never); the results do not depend on it."""
+        capi.check(capi.lib().ckmpm_set_reorder_interval(self._h, substeps), "ckmpm_set_reorder_interval", self._h)
+
     def autotune(self, probe_steps: int, dt: float) -> tuple[dict, list[dict]]:
         """Time every launch shape on this scene and keep the fastest; the
         simulation state is left unchanged.  Returns (best, all candidates)."""

@@ -332,6 +332,14 @@ typedef struct ckmpm_tuning {
 
 ckmpm_status ckmpm_set_tuning(ckmpm_scene* s, const ckmpm_tuning* t);
 
+/* Substeps between re-layouts of each block's particles (default 128; 0 =
+ * never).  Setup orders the particles of every block so that the 32 a warp
+ * handles lie in 32 different cells; the substeps keep each block's order, but
+ * the layout fades as particles change cells, and a re-layout restores it
+ * before the next substep (it moves the state twice, about the cost of one
+ * substep).  Results do not depend on it.  No counterpart in the reference. */
+ckmpm_status ckmpm_set_reorder_interval(ckmpm_scene* s, uint32_t substeps);
+
 /* max_ctas_per_sm2 (may be NULL): occupancy limit at 128 and 256 threads (at
  * 1024 threads it is 1). */
 ckmpm_status ckmpm_get_tuning(ckmpm_scene* s, ckmpm_tuning* t, uint32_t* max_ctas_per_sm2);

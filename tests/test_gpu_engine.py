@@ -233,6 +233,47 @@ def test_deterministic_bitwise(engine_lib):
         assert np.array_equal(a.v.view(np.uint32), b.v.view(np.uint32))
 
 
+def _relayout_cases():
+    from ckmpm_b200.engine import compute_lame_parameters
+    cfg_j, jelly = scenes.jelly_cube(lo=(0.4, 0.42, 0.38), hi=(0.6, 0.58, 0.55), v0=(1.0, -1.0, 0.3))
+    cfg_s, sand = scenes.small_sand()
+    cfg_m, m1 = scenes.jelly_cube(lo=(0.3, 0.3, 0.3), hi=(0.42, 0.42, 0.42), v0=(1.0, 0.0, 0.0))
+    _, m2 = scenes.fluid_box(lo=(0.44, 0.3, 0.3), hi=(0.55, 0.4, 0.42), v0=(-1.0, 0.0, 0.0))
+    lam, mu = compute_lame_parameters(5e4, 0.3)
+    lin = MPMModel(m1[0].particle_mass, m1[0].particle_volume, m1[0].particle_position,
+                   np.asarray([[0.6, -0.8, 0.2]], np.float32), MPMMaterial.linear(lam, mu))
+    return {"jelly_fc": (cfg_j, jelly, 1e-4), "sand_dp": (cfg_s, sand, 5e-5), "two_models": (cfg_m, m1 + m2, 1e-4),
+            "linear": (cfg_m, [lin], 1e-4)}
+
+
+@pytest.mark.parametrize("case", ["jelly_fc", "sand_dp", "two_models", "linear"])
+def test_relayout_changes_no_result(engine_lib, case):
+    """ckmpm_set_reorder_interval: re-laying out every block's particles every 10
+    substeps (before graph chunks, between single substeps, and in the adaptive
+    loop) leaves every particle's x, v, F, aux and the counters bit for bit as
+    never re-laying out does; only where the particles are stored changes."""
+    cfg, models, dt = _relayout_cases()[case]
+    runs = []
+    for every in (0, 10):
+        s = Scene(cfg)
+        s.set_reorder_interval(every)
+        for m in models:
+            s.add_model(m)
+        s.setup()
+        s.step(47, dt)
+        s.step_async(23, dt)
+        s.status_check()
+        s.step_adaptive(25, dt, 0.4, 25 * dt)
+        runs.append(([s.state(i) for i in range(len(models))], s.counters()))
+        s.close()
+    (a, ca), (b, cb) = runs
+    assert ca == cb
+    for sa, sb in zip(a, b):
+        assert np.array_equal(sa.id, sb.id)
+        for name in ("x", "v", "F", "aux"):
+            assert np.array_equal(getattr(sa, name).view(np.uint32), getattr(sb, name).view(np.uint32)), (case, name)
+
+
 def test_first_substep_has_zero_advection(engine_lib):
     cfg, models = scenes.jelly_cube()
     s = run_engine(cfg, models, 1, 1e-4)
