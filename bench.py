@@ -50,6 +50,7 @@ REFERENCE_FAMILY = {"sand_column": "sand", "jelly_cube": "jelly", "dam_break_mix
 # NACC), x + F + stored stress (linear), x + J (fluid).
 STATE_BYTES = {0: 48, 1: 84, 2: 52, 3: 16, 4: 52, 5: 52}
 AUTOTUNE_MAX_PARTICLES = 64_000_000
+E2E_REPEATS = 3  # end-to-end region timings per line (the median is reported)
 
 
 def parse():
@@ -671,32 +672,42 @@ def run_ours(args, rank, world, local_rank):
     models_h = [dataclasses.replace(m, particle_position=pin(m.particle_position),
                                     particle_velocity=pin(m.particle_velocity)) for m in models]
     xbufs = [pin(np.zeros((len(m.particle_position), 3), np.float32)) for m in models]
-    torch.cuda.synchronize()
-    t_e2e = time.perf_counter()
-    s2 = Scene(cfg)
-    s2.set_stream(stream.cuda_stream)
-    s2.set_tuning(tuning["threads"], tuning["ctas_per_sm"], tuning["graph_chunk"])
-    for m in models_h:
-        s2.add_model(m)
-    s2.setup()
-    exports = 0
-    done = 0
-    while done < args.steps:
-        k = min(args.e2e_frame, args.steps - done)
-        s2.step(k, dt)  # one frame of substeps, then the device status word read back
-        for i in range(len(models)):
-            s2.export_positions_async(i, xbufs[i])  # its copy overlaps the next frame
-        exports += 1
-        done += k
-    s2.export_wait()
-    torch.cuda.synchronize()
-    e2e_ms = (time.perf_counter() - t_e2e) * 1e3
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    s2.close()
+
+    def one_e2e() -> tuple[float, int]:
+        torch.cuda.synchronize()
+        t_e2e = time.perf_counter()
+        s2 = Scene(cfg)
+        s2.set_stream(stream.cuda_stream)
+        s2.set_tuning(tuning["threads"], tuning["ctas_per_sm"], tuning["graph_chunk"])
+        for m in models_h:
+            s2.add_model(m)
+        s2.setup()
+        exports = 0
+        done = 0
+        while done < args.steps:
+            k = min(args.e2e_frame, args.steps - done)
+            s2.step(k, dt)  # one frame of substeps, then the device status word read back
+            for i in range(len(models)):
+                s2.export_positions_async(i, xbufs[i])  # its copy overlaps the next frame
+            exports += 1
+            done += k
+        s2.export_wait()
+        torch.cuda.synchronize()
+        e2e_ms = (time.perf_counter() - t_e2e) * 1e3
+        if world > 1:
+            t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        s2.close()
+        return e2e_ms, exports
+
+    # The region is short (tens of ms at the driver's setting) and dominated by one-off host and
+    # driver work (the dense grid's allocation varies by several ms from run to run), so it is
+    # timed E2E_REPEATS times, each with a new scene, and the median is reported with every sample.
+    samples = [one_e2e() for _ in range(E2E_REPEATS)]
+    e2e_ms, exports = sorted(samples)[len(samples) // 2]
     e2e = {"value": world * n_live * args.steps / (e2e_ms / 1e3), "unit": METRIC,
+           "samples_ms": [round(t, 3) for t, _ in samples], "statistic": f"median of {E2E_REPEATS}",
            "h2d_bytes_per_step": (n_total * 12 + 12) / args.steps,
            "d2h_bytes_per_step": exports * (n_total * 12 + 4 * len(models) + 64) / args.steps,
            "includes": "host clock from before ckmpm_create to the last export landing: scene creation, setup "
@@ -728,6 +739,7 @@ def run_reference(args, rank, world):
                                                     "substep, no autograd binding)"}
     cfg, models = workload(args.workload)
     family = REFERENCE_FAMILY.get(args.workload)
+    e2e_samples = None
     harness = ROOT / "oracle" / "_ref" / f"ref_{family}"
     if family and harness.exists() and args.workload == "batched_256":
         # The reference runs one scene per process: loop it over every 8th scene.
@@ -747,13 +759,19 @@ def run_reference(args, rank, world):
                          f"{args.warmup + args.steps} substeps each; host timer around each frame loop, summed"}
     elif family and harness.exists():
         from oracle import ref_runner
-        res = ref_runner.time_reference_e2e(family, cfg, models, args.steps, args.warmup)
-        value = res["value"]
+        # As for ours: the end-to-end region is timed E2E_REPEATS times (one harness process each)
+        # and the median taken, except for scenes too large to build three times in the bench's time.
+        n_particles = sum(len(m.particle_position) for m in models)
+        reps = E2E_REPEATS if n_particles <= AUTOTUNE_MAX_PARTICLES else 1
+        runs = [ref_runner.time_reference_e2e(family, cfg, models, args.steps, args.warmup) for _ in range(reps)]
+        res = sorted(runs, key=lambda r: r["e2e_value"] or r["value"])[len(runs) // 2]
+        value = sorted(r["value"] for r in runs)[len(runs) // 2]
         e2e_value = res["e2e_value"] or value
+        e2e_samples = [r["e2e_value"] for r in runs]
         cpu = {"value": value, "unit": METRIC, "cores": 1, "kind": "reference",
                "sample": f"reference CUDA build (oracle/_ref/ref_{family}) via MPMEngine::Simulate in profile mode: "
                          f"{res['substeps']} substeps of the {res['particles']}-particle scene, its own host timer "
-                         "around its frame loop",
+                         f"around its frame loop; median of {reps} process runs",
                "runs_on": "one B200: the reference's implementation of this path is CUDA code"}
     else:
         cpu = cpu_baseline_oracle(cfg, models, args.cpu_seconds)
@@ -765,6 +783,9 @@ def run_reference(args, rank, world):
             "config": {"workload": WORKLOADS[args.workload], "particles": sum(len(m.particle_position) for m in models)},
             "impl": "reference", "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if e2e_samples:
+        line["e2e"]["samples"] = e2e_samples
+        line["e2e"]["statistic"] = f"median of {len(e2e_samples)}"
     if e2e_value != value:
         line["e2e"]["includes"] = ("the harness's host clock from before MPMEngine::Initialize to the end of "
                                    "Simulate's frame loop (Initialize, InitializeParticle with the upload of x and v, "

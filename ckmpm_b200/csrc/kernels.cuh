@@ -505,7 +505,10 @@ __device__ __forceinline__ void p2g_scatter(unsigned* __restrict__ ptile, const 
 
 // Epilogue shared by the substep and the initial rasterisation: add this
 // block's tile into the 2x2x2 grid blocks it covers with 64-bit integer
-// reductions, one node (4 channels) per thread, skipping nodes nothing touched.
+// reductions, one node (4 channels) per thread, skipping nodes nothing touched,
+// and leave the tile zero for the CTA's next block (each node's words are
+// cleared as they are read; the padding words are never written, and the
+// kernels zero the whole tile once before their first block).
 // Integer addition is associative, so the grid sums are bitwise deterministic
 // whatever order the up to 8 covering particle blocks flush in, and no block
 // waits for another (the reference adds floats with atomicAdd,
@@ -513,7 +516,7 @@ __device__ __forceinline__ void p2g_scatter(unsigned* __restrict__ ptile, const 
 // stamped before the launch; ratio rescales a model's per-unit-mass sums to
 // the grid's unit (1 when the scene has one particle mass).
 template <int NT>
-__device__ __forceinline__ void flush_tile(const SceneDev& sc, int4 key, const unsigned* __restrict__ ptile,
+__device__ __forceinline__ void flush_tile(const SceneDev& sc, int4 key, unsigned* __restrict__ ptile,
                                            double ratio, long long* __restrict__ gout) {
   int64_t fb[8];
 #pragma unroll
@@ -527,7 +530,6 @@ __device__ __forceinline__ void flush_tile(const SceneDev& sc, int4 key, const u
 #pragma unroll
     for (int k = 1; k < 8; ++k)
       if (e == k) f = fb[k];
-    if (f < 0) continue;
     const int w = i & 127;
     const int gi = w >> 6, cell = w & 63;
     const int lx = (e >> 2) * 4 + (cell >> 4), ly = ((e >> 1) & 1) * 4 + ((cell >> 2) & 3), lz = (e & 1) * 4 + (cell & 3);
@@ -536,6 +538,12 @@ __device__ __forceinline__ void flush_tile(const SceneDev& sc, int4 key, const u
 #pragma unroll
     for (int c = 0; c < 4; ++c) v[c] = tile_sum(ptile, node + c * kTileNodes);
     if ((v[0] | v[1] | v[2] | v[3]) == 0ull) continue;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      ptile[node + c * kTileNodes] = 0u;
+      ptile[node + c * kTileNodes + kTilePlane] = 0u;
+    }
+    if (f < 0) continue;
     if (ratio != 1.0) {
 #pragma unroll
       for (int c = 0; c < 4; ++c)
@@ -686,6 +694,8 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
   const float dx = sc.dx, inv_dx = sc.inv_dx;
   const uint32_t maxp = min(md.max_per_block, static_cast<uint32_t>(kMaxParticlesPerBlock));
 
+  for (int i = threadIdx.x; i < 2 * kTilePlane / 4; i += NT)
+    reinterpret_cast<uint4*>(ptile)[i] = make_uint4(0u, 0u, 0u, 0u);
   for (;;) {
     if (threadIdx.x == 0) sh.item = atomicAdd(md.ticket, 1u);
     __syncthreads();
@@ -718,8 +728,6 @@ __global__ void __launch_bounds__(NT, fused_min_ctas<NT>())
       window_blocks(sc, stin, read_epoch, key, sh.blk, threadIdx.x - 32);
     for (int i = threadIdx.x; i < static_cast<int>(sizeof(rk.wcnt) / sizeof(uint32_t)); i += NT)
       (&rk.wcnt[0][0])[i] = 0u;
-    for (int i = threadIdx.x; i < 2 * kTilePlane / 4; i += NT)
-      reinterpret_cast<uint4*>(ptile)[i] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
     load_velocity_tile<NT>(sc, gin, sh.blk, key, unit, dt, vtile);
     __syncthreads();
@@ -955,6 +963,8 @@ __global__ void __launch_bounds__(NT, 2) rasterize_kernel(SceneDev sc, ModelDev 
   const uint32_t nb = *cur.nblocks;
   const float inv_dx = sc.inv_dx;
   const float Z[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = threadIdx.x; i < 2 * kTilePlane / 4; i += NT)
+    reinterpret_cast<uint4*>(ptile)[i] = make_uint4(0u, 0u, 0u, 0u);
   for (;;) {
     if (threadIdx.x == 0) sh.item = atomicAdd(md.ticket, 1u);
     __syncthreads();
@@ -963,9 +973,6 @@ __global__ void __launch_bounds__(NT, 2) rasterize_kernel(SceneDev sc, ModelDev 
     const int4 key = cur.keys[item];
     const uint32_t start = cur.start[item];
     const uint32_t n = cur.count[item];
-    for (int i = threadIdx.x; i < 2 * kTilePlane / 4; i += NT)
-      reinterpret_cast<uint4*>(ptile)[i] = make_uint4(0u, 0u, 0u, 0u);
-    __syncthreads();
     const int kk[3] = {key.x, key.y, key.z};
     for (uint32_t q = threadIdx.x; q < n; q += NT) {
       const uint32_t i = start + q;
