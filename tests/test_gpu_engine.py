@@ -233,6 +233,35 @@ def test_deterministic_bitwise(engine_lib):
         assert np.array_equal(a.v.view(np.uint32), b.v.view(np.uint32))
 
 
+@pytest.mark.parametrize("scene", ["jelly", "sand"])
+def test_setup_lays_particles_out_across_cells(engine_lib, scene):
+    """Setup's particle layout: within every block the particles are stored by (rank within
+    their cell, cell), the cells numbered x-major over the block, so 32 consecutive particles
+    lie in 32 different cells of a half block wherever the counts allow.  Read back in storage
+    order (a scene without ids exports in block order), each block's sequence of keys
+    (occurrences of its cell so far, cell) must increase strictly."""
+    cfg, models = scenes.jelly_cube(track_ids=False) if scene == "jelly" else scenes.small_sand(track_ids=False)
+    s = run_engine(cfg, models, 0, 1e-4)
+    x = s.state(0).x
+    s.close()
+    c = (x.astype(np.float32) * np.float32(1.0 / cfg.dx) + np.float32(0.25)).astype(np.int64)
+    block = (c - 2) // 4  # all positions are well inside the domain: floor equals truncation
+    cell = ((c - 2) % 4) @ np.array([16, 4, 1])
+    starts = np.flatnonzero(np.any(block[1:] != block[:-1], axis=1)) + 1
+    runs = np.split(np.arange(len(x)), starts)
+    assert len({tuple(block[r[0]]) for r in runs}) == len(runs), "a block's particles are not contiguous"
+    full_warps = 0
+    for r in runs:
+        seen = {}
+        keys = []
+        for ci in cell[r]:
+            keys.append(seen.get(ci, 0) * 64 + ci)
+            seen[ci] = seen.get(ci, 0) + 1
+        assert all(a < b for a, b in zip(keys, keys[1:])), "block not in (rank, cell) order"
+        full_warps += sum(len(set(cell[r][i:i + 32])) == 32 for i in range(0, len(r) - 31, 32))
+    assert full_warps > 0
+
+
 def _relayout_cases():
     from ckmpm_b200.engine import compute_lame_parameters
     cfg_j, jelly = scenes.jelly_cube(lo=(0.4, 0.42, 0.38), hi=(0.6, 0.58, 0.55), v0=(1.0, -1.0, 0.3))
