@@ -241,3 +241,19 @@ def test_batch_shares_a_boundary_field(engine_lib):
     cfg.boundary_field = BoundaryField(cfg).slip_walls(8).fixed_box((20, 0, 20), (44, 12, 44)).arrays()
     b = run_batch(cfg, models, 16)
     check_against_alone_and_own_batch(cfg, models, b, 16)
+
+
+def test_batch_relayout_changes_no_result(engine_lib):
+    """A batch re-laid out every 10 substeps (ckmpm_set_reorder_interval; every scene's blocks
+    gather their particles into the setup order) gives the same particles bit for bit as one
+    never re-laid out."""
+    cfg, models = small_batch()
+    runs = []
+    for every in (0, 10):
+        b = SceneBatch(cfg, models)
+        b.set_reorder_interval(every)
+        b.setup()
+        b.step(37, DT)
+        runs.append(b.state())
+        b.close()
+    assert_same_state(runs[0], runs[1], "batch with and without re-layout")
