@@ -2,6 +2,7 @@
 // setup, CUDA-graph substep replay and the C ABI declared in include/ckmpm.h.
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -212,6 +213,31 @@ cudaError_t set_fused_attributes(int* occ) {
   return cudaSuccess;
 }
 
+// The fused and rasterisation kernels' attributes belong to the process and the
+// device, not to a scene: they are set, and the fused kernels' occupancy at
+// 128 / 256 / 1024 threads queried (39 kernel variants), once per device, by
+// the first scene created on it.  A failure is not cached.
+std::mutex g_attr_mutex;
+std::map<int, std::array<int, 3>> g_attr_occ;
+
+cudaError_t fused_attributes(int device, int* occ3) {
+  std::lock_guard<std::mutex> lock(g_attr_mutex);
+  auto it = g_attr_occ.find(device);
+  if (it == g_attr_occ.end()) {
+    std::array<int, 3> occ{0, 0, 0};
+    cudaError_t e = set_fused_attributes<128>(&occ[0]);
+    if (e == cudaSuccess) e = set_fused_attributes<256>(&occ[1]);
+    if (e == cudaSuccess) e = set_fused_attributes<1024>(&occ[2]);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(reinterpret_cast<const void*>(rasterize_kernel<kFusedThreads>),
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemFused));
+    if (e != cudaSuccess) return e;
+    it = g_attr_occ.emplace(device, occ).first;
+  }
+  for (int k = 0; k < 3; ++k) occ3[k] = it->second[k];
+  return cudaSuccess;
+}
+
 // Compaction of one model's next block list into list `out`.
 cudaError_t launch_compact(ckmpm_scene* s, const ModelHost& m, const BlockListDev& out) {
   compact_reduce_kernel<<<m.ntiles, kCompactThreads, 0, s->stream>>>(s->sc, m.dev.dense_total, m.dev.tile_sums);
@@ -389,10 +415,7 @@ ckmpm_status create_impl(const ckmpm_scene_desc* desc, uint32_t nstack, ckmpm_sc
     sc.bparam = param;
   }
 
-  if (set_fused_attributes<128>(&s->occ[0]) != cudaSuccess || set_fused_attributes<256>(&s->occ[1]) != cudaSuccess ||
-      set_fused_attributes<1024>(&s->occ[2]) != cudaSuccess ||
-      cudaFuncSetAttribute(reinterpret_cast<const void*>(rasterize_kernel<kFusedThreads>),
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemFused)) != cudaSuccess)
+  if (fused_attributes(desc->device, s->occ) != cudaSuccess)
     return bail(fail(s, CKMPM_ERR_CUDA, "cudaFuncSetAttribute failed"));
   // Default launch shape: 256 threads, as many resident CTAs as fit, graphs of 8.
   s->tune.threads = kFusedThreads;
