@@ -1406,8 +1406,8 @@ __device__ __forceinline__ void cell_order_keys(const uint8_t* cell, uint32_t n,
     }
     __syncthreads();
     if (j < n) key[j] = (((wcnt[w * 64 + c] + below) * 64u + c) << 12) | j;
+    __syncthreads();  // every key read its counter before the next chunk clears them
   }
-  __syncthreads();
 }
 
 // Setup ordering of each block's range, in two sorts in shared memory:
