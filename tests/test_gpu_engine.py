@@ -239,11 +239,16 @@ def test_setup_lays_particles_out_across_cells(engine_lib, scene):
     their cell, cell), the cells numbered x-major over the block, so 32 consecutive particles
     lie in 32 different cells of a half block wherever the counts allow.  Read back in storage
     order (a scene without ids exports in block order), each block's sequence of keys
-    (occurrences of its cell so far, cell) must increase strictly."""
+    (occurrences of its cell so far, cell) must increase strictly, and two setups of the same
+    scene store the particles in the same order."""
     cfg, models = scenes.jelly_cube(track_ids=False) if scene == "jelly" else scenes.small_sand(track_ids=False)
-    s = run_engine(cfg, models, 0, 1e-4)
-    x = s.state(0).x
-    s.close()
+    xs = []
+    for _ in range(2):
+        s = run_engine(cfg, models, 0, 1e-4)
+        xs.append(s.state(0).x)
+        s.close()
+    x = xs[0]
+    assert np.array_equal(xs[0], xs[1]), "the storage order differs between two setups of the same scene"
     c = (x.astype(np.float32) * np.float32(1.0 / cfg.dx) + np.float32(0.25)).astype(np.int64)
     block = (c - 2) // 4  # all positions are well inside the domain: floor equals truncation
     cell = ((c - 2) % 4) @ np.array([16, 4, 1])
