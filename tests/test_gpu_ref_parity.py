@@ -1,7 +1,8 @@
 """The CUDA engine against the reference CUDA build run live on the same seeded inputs, at the
 benchmark scenes the reference harness covers: the jelly cube (16,795 particles, fixed-corotated,
 sticky walls, dt = 1e-4, 1000 substeps) and the sand column (1,686,824 particles, Drucker-Prager
-on a slip floor, dt = 5e-5, 500 substeps).
+on a slip floor, dt = 5e-5, 500 substeps), and a J-fluid box on the jelly cube's grid thrown at
+its sticky floor (25,229 particles, bulk 1e4, gamma 7.15, viscosity 0.1, dt = 1e-4, 1000 substeps).
 
 The reference runs through its own MPMEngine (Initialize -> InitializeParticle -> InitialSetup ->
 Simulate, oracle/_ref built from its headers by oracle/Makefile); its state after K substeps is
@@ -18,7 +19,7 @@ Integer contract (binning and the block table), checked exactly:
     reference's at setup and after 1 and 10 substeps; later, wherever a particle's block
     differs the two positions straddle a block face within the float tolerance on x below.
 Float contract: the reference's P2G sums with float atomics, so two runs of it differ; x, v, F
-(and logJp for the sand) of the engine must lie within a few times that run-to-run spread of
+(and logJp for the sand, J for the fluid) of the engine must lie within a few times that run-to-run spread of
 the reference, with a floor (the tolerances are stated at FLOAT_TOL).  The reference runs three
 times; the engine is compared with the first run and the spread is the largest distance between
 any two of the three, which one pair alone estimates too noisily after hundreds of substeps (at
@@ -37,7 +38,12 @@ pytestmark = pytest.mark.gpu
 CASES = {
     "jelly_cube": ("jelly", [0, 1, 10, 100, 1000]),
     "sand_column": ("sand", [0, 1, 10, 100, 500]),
+    "fluid_box": ("jelly", [0, 1, 10, 100, 1000]),
 }
+SCENES = {"jelly_cube": scenes.jelly_cube, "sand_column": scenes.sand_column,
+          # thrown at the sticky floor: it lands after ~20 ms and splashes, so J and the pressure move
+          "fluid_box": lambda track_ids: scenes.fluid_box(lo=(0.3, 0.15, 0.3), hi=(0.5, 0.45, 0.5),
+                                                          v0=(0.5, -1.0, -0.25), track_ids=track_ids)}
 EARLY = (0, 1, 10)  # substep counts at which every integer output must agree exactly
 
 # Engine-vs-reference error allowed at each compared substep count, per quantity:
@@ -88,7 +94,7 @@ def run(request, engine_lib):
     family, ks = CASES[name]
     if not ref.available(family):
         pytest.skip(f"oracle/_ref/ref_{family} is not built (make -C oracle ref)")
-    cfg, models = scenes.WORKLOADS[name](track_ids=True)
+    cfg, models = SCENES[name](track_ids=True)
     dt = cfg.dt
     refs = [ref.dump(family, models, dt, ks) for _ in range(3)]
     s = Scene(cfg)
