@@ -323,7 +323,9 @@ __global__ void follow_kernel(Partition partition, Partition prev, Buffer data, 
 // The velocity G2P gives a particle on the updated grid: 0.5 x the sum over both staggered grids
 // of w_i v_i, with the reference's cell index, weights and summation order
 // (CollectConservationMetric, include/mpm_algorithm.cuh:1270-1320), the node values read from
-// the grid blocks instead of the shared tile they are copied into.
+// the grid blocks instead of the shared tile they are copied into.  With rigid particles on, G2P
+// reads attribute 3 of every particle as J and gives a particle with J == 0 (a rigid one) zero
+// velocity (G2P2G, include/mpm_algorithm.cuh:1540-1543, 1609-1615); so does this read-back.
 template <typename Grid>
 __global__ void velocity_kernel(Partition partition, const Grid grid, uint32_t n, const float* attr, int nattr,
                                 float* out_v) {
@@ -357,6 +359,7 @@ __global__ void velocity_kernel(Partition partition, const Grid grid, uint32_t n
     });
   });
   vel = 0.5f * vel;
+  if (harness::kRigid && attr[static_cast<size_t>(p) * nattr + 3] == 0.f) vel = Vector<float, 3>{};
   out_v[3 * p] = vel[0];
   out_v[3 * p + 1] = vel[1];
   out_v[3 * p + 2] = vel[2];

@@ -2,7 +2,10 @@
 benchmark scenes the reference harness covers: the jelly cube (16,795 particles, fixed-corotated,
 sticky walls, dt = 1e-4, 1000 substeps) and the sand column (1,686,824 particles, Drucker-Prager
 on a slip floor, dt = 5e-5, 500 substeps), and a J-fluid box on the jelly cube's grid thrown at
-its sticky floor (25,229 particles, bulk 1e4, gamma 7.15, viscosity 0.1, dt = 1e-4, 1000 substeps).
+its sticky floor (25,229 particles, bulk 1e4, gamma 7.15, viscosity 0.1, dt = 1e-4, 1000 substeps),
+and on the same grid the other materials' cubes (8,626 particles, 500 substeps): von Mises in shear,
+the same with its first 2048 particles rigid (the harness's rigid family), NACC squeezed by a
+converging velocity field, and linear elasticity.
 
 The reference runs through its own MPMEngine (Initialize -> InitializeParticle -> InitialSetup ->
 Simulate, oracle/_ref built from its headers by oracle/Makefile); its state after K substeps is
@@ -19,7 +22,7 @@ Integer contract (binning and the block table), checked exactly:
     reference's at setup and after 1 and 10 substeps; later, wherever a particle's block
     differs the two positions straddle a block face within the float tolerance on x below.
 Float contract: the reference's P2G sums with float atomics, so two runs of it differ; x, v, F
-(and logJp for the sand, J for the fluid) of the engine must lie within a few times that run-to-run spread of
+(and logJp for the sand, J for the fluid, alpha for NACC, the rigid flag) of the engine must lie within a few times that run-to-run spread of
 the reference, with a floor (the tolerances are stated at FLOAT_TOL).  The reference runs three
 times; the engine is compared with the first run and the spread is the largest distance between
 any two of the three, which one pair alone estimates too noisily after hundreds of substeps (at
@@ -39,12 +42,36 @@ CASES = {
     "jelly_cube": ("jelly", [0, 1, 10, 100, 1000]),
     "sand_column": ("sand", [0, 1, 10, 100, 500]),
     "fluid_box": ("jelly", [0, 1, 10, 100, 1000]),
+    "von_mises": ("jelly", [0, 1, 10, 100, 500]),
+    "nacc": ("jelly", [0, 1, 10, 100, 500]),
+    "linear": ("jelly", [0, 1, 10, 100, 500]),
+    "vm_rigid": ("rigid", [0, 1, 10, 100, 500]),
 }
 SCENES = {"jelly_cube": scenes.jelly_cube, "sand_column": scenes.sand_column,
           # thrown at the sticky floor: it lands after ~20 ms and splashes, so J and the pressure move
           "fluid_box": lambda track_ids: scenes.fluid_box(lo=(0.3, 0.15, 0.3), hi=(0.5, 0.45, 0.5),
-                                                          v0=(0.5, -1.0, -0.25), track_ids=track_ids)}
-EARLY = (0, 1, 10)  # substep counts at which every integer output must agree exactly
+                                                          v0=(0.5, -1.0, -0.25), track_ids=track_ids),
+          # the reference's other materials, each cube loaded at once by its initial velocity field
+          "von_mises": lambda track_ids: scenes.material_cube("von_mises", track_ids=track_ids),
+          "nacc": lambda track_ids: scenes.material_cube("nacc", track_ids=track_ids),
+          "linear": lambda track_ids: scenes.material_cube("linear", track_ids=track_ids),
+          "vm_rigid": lambda track_ids: _vm_rigid(track_ids)}
+# Scenes whose scalar is not compared: fixed-corotated and linear keep none; von Mises without rigid
+# particles keeps its rigid flag (1) in the engine, while the reference, which reads that slot only
+# when rigid particles exist (include/mpm_algorithm.cuh:1540-1543), writes its unread J register
+# (0) there from the first substep on (:1643-1644, :512-516); the state test checks both values.
+NO_SCALAR = ("jelly_cube", "linear", "von_mises")
+EARLY = (0, 1, 10)
+
+
+def _vm_rigid(track_ids):
+    """The von Mises cube on the harness's rigid family: its first 2048 particles are rigid and
+    move with (2, 0.5 frame - 1, -1) (oracle/ref_harness.cu); every dumped substep lies in frame 0."""
+    cfg, models = scenes.material_cube("von_mises", track_ids=track_ids)
+    cfg.exist_rigid_particle = True
+    cfg.rigid_particle_count = 2048
+    cfg.rigid_particle_velocity = lambda frame: (2.0, 0.5 * frame - 1.0, -1.0)
+    return cfg, models  # substep counts at which every integer output must agree exactly
 
 # Engine-vs-reference error allowed at each compared substep count, per quantity:
 # max |engine - reference run 1| <= max(SPREAD_FACTOR * (max |reference run i - reference run j|), floor).
@@ -56,6 +83,11 @@ EARLY = (0, 1, 10)  # substep counts at which every integer output must agree ex
 # substeps 1.1-1.4x), and the FP64 oracle sits as far from the reference as the engine does.
 SPREAD_FACTOR = 8.0
 FLOAT_TOL = {"x": 1e-5, "v": 1e-4, "F": 1e-4, "aux": 1e-4}
+# Per-scene floors where the reference's own float rounding, which its run-to-run spread (atomic
+# order alone) does not show, is larger: on the von Mises cube, in plastic shear from the first
+# substeps, the FP64 oracle's velocities after 500 substeps lie 9.1e-5 (relative) from the
+# reference's, the engine's 1.1e-4, while three reference runs differ by 1.0e-5 at most.
+FLOAT_TOL_SCENE = {"von_mises": {"v": 2.5e-4}, "vm_rigid": {"v": 2.5e-4}}
 # Position difference allowed for a particle that the engine bins into another block than the
 # reference: the bound of the state test for x, max(SPREAD_FACTOR * reference spread, X_TOL_BLOCK).
 X_TOL_BLOCK = 1e-5
@@ -202,6 +234,17 @@ def _errors(p, q, scale_v):
     return {k: (float(v.max()), float(np.quantile(v, 0.999))) for k, v in d.items()}
 
 
+def _compared(name, m):
+    """The quantities compared: x, v, F and the scalar, except that NACC stores F = U S V, fixed
+    only up to a rotation on the right (each implementation's SVD picks its own), so for it F F^T,
+    which everything the model computes depends on, stands in for F."""
+    F = np.asarray(m["F"], np.float64).reshape(-1, 3, 3)
+    if name == "nacc":
+        F = F @ F.transpose(0, 2, 1)
+    aux = np.zeros(len(F)) if name in NO_SCALAR else m["aux"]
+    return {"x": m["x"], "v": m["v"], "F": F, "aux": aux}
+
+
 def test_state_within_reference_spread(run):
     name = run["name"]
     rows = []
@@ -211,10 +254,11 @@ def test_state_within_reference_spread(run):
         assert all(np.array_equal(ma["id"], r[k]["models"][0]["id"]) for r in run["refs"])
         assert np.array_equal(ma["id"], st.id)
         scale_v = max(float(np.abs(ma["v"]).max()), 1e-6)
-        ours = {"x": st.x, "v": st.v, "F": st.F.reshape(-1, 3, 3), "aux": st.aux}
-        if name == "jelly_cube":
-            ours["aux"] = np.zeros_like(st.aux)  # fixed-corotated keeps no scalar
-        pair_errors = [_errors(p, q, scale_v) for p, q in _pairs(run, k)]
+        if name == "von_mises":
+            assert np.all(st.aux == 1.0) and np.all(ma["aux"] == (1.0 if k == 0 else 0.0)), k
+        ours = _compared(name, {"x": st.x, "v": st.v, "F": st.F, "aux": st.aux})
+        ma = _compared(name, ma)
+        pair_errors = [_errors(_compared(name, p), _compared(name, q), scale_v) for p, q in _pairs(run, k)]
         spread = {q: tuple(max(e[q][i] for e in pair_errors) for i in range(2)) for q in pair_errors[0]}
         err = _errors(ours, ma, scale_v)
         rows.append((k, err, spread))
@@ -223,5 +267,5 @@ def test_state_within_reference_spread(run):
               + " ".join(f"{q} {spread[q][0]:.2e}/{spread[q][1]:.2e}" for q in spread))
     for k, err, spread in rows:
         for q in err:
-            bound = max(SPREAD_FACTOR * spread[q][0], FLOAT_TOL[q])
+            bound = max(SPREAD_FACTOR * spread[q][0], FLOAT_TOL_SCENE.get(name, FLOAT_TOL).get(q, FLOAT_TOL[q]))
             assert err[q][0] <= bound, (name, k, q, err[q], bound)
