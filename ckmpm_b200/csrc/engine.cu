@@ -79,7 +79,7 @@ struct ckmpm_scene {
   std::string err;
   int sm_count = 0;
   int fused_ctas = 0;
-  int occ[3] = {0, 0, 0};  // resident fused CTAs per SM at 128 / 256 / 1024 threads
+  int occ[4] = {0, 0, 0, 0};  // resident fused CTAs per SM at 128 / 256 / 1024 / 192 threads
   uint32_t nstack = 1;     // stacked domains: 1, or the scene count of a batch
   ckmpm_tuning tune{};
   // Every device allocation with its size; the first n_state_allocs hold the
@@ -175,13 +175,16 @@ cudaError_t launch_fused_nt(ckmpm_scene* s, const ModelHost& m) {
 cudaError_t launch_fused_any(ckmpm_scene* s, const ModelHost& m) {
   switch (s->tune.threads) {
     case 128: return launch_fused_nt<128>(s, m);
+    case 192: return launch_fused_nt<192>(s, m);
     case 1024: return launch_fused_nt<1024>(s, m);
     default: return launch_fused_nt<256>(s, m);
   }
 }
 
 // Index of a CTA size in ckmpm_scene::occ (-1 for a size that has no kernel).
-int shape_index(uint32_t threads) { return threads == 128 ? 0 : threads == 256 ? 1 : threads == 1024 ? 2 : -1; }
+int shape_index(uint32_t threads) {
+  return threads == 128 ? 0 : threads == 256 ? 1 : threads == 1024 ? 2 : threads == 192 ? 3 : -1;
+}
 
 template <int NT>
 cudaError_t set_fused_attributes(int* occ) {
@@ -215,26 +218,27 @@ cudaError_t set_fused_attributes(int* occ) {
 
 // The fused and rasterisation kernels' attributes belong to the process and the
 // device, not to a scene: they are set, and the fused kernels' occupancy at
-// 128 / 256 / 1024 threads queried (39 kernel variants), once per device, by
-// the first scene created on it.  A failure is not cached.
+// 128 / 256 / 1024 / 192 threads queried (52 kernel variants), once per device,
+// by the first scene created on it.  A failure is not cached.
 std::mutex g_attr_mutex;
-std::map<int, std::array<int, 3>> g_attr_occ;
+std::map<int, std::array<int, 4>> g_attr_occ;
 
-cudaError_t fused_attributes(int device, int* occ3) {
+cudaError_t fused_attributes(int device, int* occ4) {
   std::lock_guard<std::mutex> lock(g_attr_mutex);
   auto it = g_attr_occ.find(device);
   if (it == g_attr_occ.end()) {
-    std::array<int, 3> occ{0, 0, 0};
+    std::array<int, 4> occ{0, 0, 0, 0};
     cudaError_t e = set_fused_attributes<128>(&occ[0]);
     if (e == cudaSuccess) e = set_fused_attributes<256>(&occ[1]);
     if (e == cudaSuccess) e = set_fused_attributes<1024>(&occ[2]);
+    if (e == cudaSuccess) e = set_fused_attributes<192>(&occ[3]);
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(reinterpret_cast<const void*>(rasterize_kernel<kFusedThreads>),
                                cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemFused));
     if (e != cudaSuccess) return e;
     it = g_attr_occ.emplace(device, occ).first;
   }
-  for (int k = 0; k < 3; ++k) occ3[k] = it->second[k];
+  for (int k = 0; k < 4; ++k) occ4[k] = it->second[k];
   return cudaSuccess;
 }
 
@@ -429,7 +433,7 @@ ckmpm_status create_impl(const ckmpm_scene_desc* desc, uint32_t nstack, ckmpm_sc
 }
 
 ckmpm_status apply_tuning(ckmpm_scene* s, const ckmpm_tuning& t) {
-  if (shape_index(t.threads) < 0) return fail(s, CKMPM_ERR_INVALID, "threads must be 128, 256 or 1024");
+  if (shape_index(t.threads) < 0) return fail(s, CKMPM_ERR_INVALID, "threads must be 128, 192, 256 or 1024");
   const int occ = s->occ[shape_index(t.threads)];
   if (t.ctas_per_sm < 1 || t.ctas_per_sm > static_cast<uint32_t>(occ))
     return fail(s, CKMPM_ERR_INVALID, "ctas_per_sm must be between 1 and the kernel's occupancy");
@@ -1202,7 +1206,7 @@ ckmpm_status ckmpm_autotune(ckmpm_scene* s, uint32_t probe_steps, float dt, ckmp
   CK_CUDA(s, checkpoint_copy(s, static_cast<unsigned char*>(saved), true));
   const ckmpm_tuning before = s->tune;
   std::vector<ckmpm_tuning> cands;
-  for (uint32_t nt : {256u, 128u, 1024u}) {
+  for (uint32_t nt : {256u, 192u, 128u, 1024u}) {
     const int occ = s->occ[shape_index(nt)];
     for (int c = occ; c >= 1; --c)
       for (uint32_t chunk : {8u, 32u}) cands.push_back(ckmpm_tuning{nt, static_cast<uint32_t>(c), chunk, 0.f});

@@ -324,7 +324,7 @@ ckmpm_status ckmpm_get_blocks_in(ckmpm_scene* s, uint32_t scene, int32_t model, 
  * not depend on it: the P2G tile and the grid hold exact integer sums, so the
  * order in which blocks deposit never changes a bit. */
 typedef struct ckmpm_tuning {
-  uint32_t threads;      /* CTA size: 128, 256 or 1024 (one CTA per SM; for small scenes) */
+  uint32_t threads;      /* CTA size: 128, 192, 256 or 1024 (one CTA per SM; for small scenes) */
   uint32_t ctas_per_sm;  /* resident persistent CTAs per SM, 1..occupancy */
   uint32_t graph_chunk;  /* substeps per captured CUDA graph, even, 2..64 */
   float probe_ms;        /* ckmpm_autotune: measured ms per substep; 0 otherwise */

@@ -136,7 +136,7 @@ def test_batch_scenes_match_oracle(engine_lib, oracle_mod):
 def test_launch_shape_does_not_change_results(engine_lib):
     cfg, models = small_batch(n=6, seed=7)
     ref = run_batch(cfg, models, 16).state()
-    for tuning in ((128, 1, 2), (128, 5, 32), (256, 2, 8), (256, 4, 64), (1024, 1, 8)):
+    for tuning in ((128, 1, 2), (128, 5, 32), (192, 5, 8), (256, 2, 8), (256, 4, 64), (1024, 1, 8)):
         got = run_batch(cfg, models, 16, tuning).state()
         assert_same_state(got, ref, f"tuning {tuning}")
 

@@ -219,7 +219,7 @@ def test_deterministic_bitwise(engine_lib):
     cfg, models = scenes.jelly_cube(v0=(0.7, -1.3, 0.4))
     a = run_engine(cfg, models, 50, 1e-4).state(0)
     runs = [run_engine(cfg, models, 50, 1e-4).state(0)]
-    for shape in ((1024, 1, 8), (128, 3, 32)):
+    for shape in ((1024, 1, 8), (128, 3, 32), (192, 5, 8)):
         s = Scene(cfg)
         s.set_tuning(*shape)
         for m in models:
