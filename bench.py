@@ -498,6 +498,9 @@ def run_batched(args, rank, world, local_rank):
                 "kernel": "g2p2g_kernel<kMixed> (all scenes of the shard in one launch)",
                 "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_fused,
                 "peak_source": f"{peak_kind} hbm_gbs", "fused_share": fused_ms / max(fused_ms + other_ms, 1e-9)}
+    # One untimed export: the export path's kernels load before the end-to-end region.
+    b.export_positions_async(0, np.zeros((sum(len(m.particle_position) for m in sub), 3), np.float32))
+    b.export_wait()
     b.close()
 
     looped = None
@@ -657,6 +660,11 @@ def run_ours(args, rank, world, local_rank):
     if len(models) > 1:
         roofline["note"] = ("per substep: algorithmic_bytes_per_launch and avg_launch_ms cover the substep's "
                             f"{len(models)} fused launches together (one per model)")
+    # One untimed export, so that the export path's kernels are loaded (CUDA loads a kernel at its
+    # first launch) before the end-to-end region, as every other kernel of the region already is.
+    for i, m in enumerate(models):
+        s.export_positions_async(i, np.zeros((len(m.particle_position), 3), np.float32))
+    s.export_wait()
     s.close()
 
     # ---- end to end through the public API with host buffers: the inputs sit in
