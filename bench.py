@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sand_column")
     ap.add_argument("--ncu-case", action="store_true",
                     help="profiling driver: set up the workload, run warmup + steps substeps, no timing or baselines")
+    ap.add_argument("--ncu-tuning", default=None,
+                    help="profiling driver: launch shape threads,ctas_per_sm,graph_chunk (default: the engine's)")
     ap.add_argument("--ncu-scenes", type=int, default=256,
                     help="profiling driver, batched workload: profile the first K of the 256 scenes")
     return ap.parse_args()
@@ -932,13 +934,15 @@ def main():
         cfg, models = workload(args.workload)
         cfg.device = local_rank
         s = Scene(cfg)
+        if args.ncu_tuning:
+            s.set_tuning(*(int(t) for t in args.ncu_tuning.split(",")))
         for m in models:
             s.add_model(m)
         s.setup()
         s.step(args.warmup, cfg.dt)
         s.step(args.steps, cfg.dt)
         print(json.dumps({"ncu_case": WORKLOADS[args.workload], "particles": s.count(0),
-                          "substeps": args.warmup + args.steps}))
+                          "substeps": args.warmup + args.steps, "tuning": s.tuning()}))
         return
     if args.impl == "reference":
         if rank != 0:
