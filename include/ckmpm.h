@@ -105,7 +105,11 @@ typedef struct ckmpm_material {
 } ckmpm_material;
 
 /* Replaces MPMEngine<GridConfig>::GetInstance() + Initialize(config)
- * (include/mpm_engine.cuh:80-84,171-191). */
+ * (include/mpm_engine.cuh:80-84,171-191).  Allocates the scene's dense grids,
+ * stamps and scalars in one device allocation.  Each scene also takes one
+ * page-locked host word (its export count) from slabs of 1024 that the
+ * library allocates as needed (64 KB each) and keeps for the life of the
+ * process; ckmpm_destroy returns the word. */
 ckmpm_status ckmpm_create(const ckmpm_scene_desc* desc, ckmpm_scene** out);
 
 /* Replaces MPMModel(mass, volume, x, v, material) (include/mpm_model.h:19-33)
