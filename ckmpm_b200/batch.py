@@ -65,7 +65,12 @@ class SceneBatch(Scene):
     every live particle in input order with its scene index.
     """
 
-    def __init__(self, config: MPMConfig, scenes: Sequence[MPMModel]):
+    def __init__(self, config: MPMConfig, scenes: Sequence[MPMModel], x: np.ndarray | None = None,
+                 v: np.ndarray | None = None):
+        """x, v (optional): every scene's positions and per-particle velocities already concatenated in
+        scene order, float32 C-contiguous arrays of shape (total particles, 3), the layout
+        ckmpm_add_batch takes; in pinned host memory the upload is a DMA.  Without them they are
+        concatenated from the scenes (a scene with one velocity row gives it to all its particles)."""
         if not scenes:
             raise ValueError("empty batch")
         if len(scenes) > capi.MAX_BATCH_SCENES:
@@ -73,22 +78,29 @@ class SceneBatch(Scene):
         self.config = config
         self._h = C.c_void_p()
         self._exports_in_flight: list[np.ndarray] = []
-        L = capi.lib()
-        desc = config.to_c()
-        capi.check(L.ckmpm_create_batch(C.byref(desc), len(scenes), C.byref(self._h)), "ckmpm_create_batch", None)
         self.models = list(scenes)
         self.counts = np.array([len(m.particle_position) for m in scenes], np.int64)
         self.offsets = np.concatenate([[0], np.cumsum(self.counts)])
+        total = int(self.counts.sum())
+        if (x is None) != (v is None):
+            raise ValueError("give both x and v, or neither")
+        if x is None:
+            x = np.ascontiguousarray(np.concatenate([m.particle_position for m in scenes]), np.float32)
+            v = np.ascontiguousarray(np.concatenate([
+                m.particle_velocity if len(m.particle_velocity) == len(m.particle_position)
+                else np.repeat(m.particle_velocity, len(m.particle_position), 0) for m in scenes]), np.float32)
+        for name, a in (("x", x), ("v", v)):
+            if a.dtype != np.float32 or not a.flags.c_contiguous or a.shape != (total, 3):
+                raise ValueError(f"{name} must be a C-contiguous float32 array of shape ({total}, 3)")
+        L = capi.lib()
+        desc = config.to_c()
+        capi.check(L.ckmpm_create_batch(C.byref(desc), len(scenes), C.byref(self._h)), "ckmpm_create_batch", None)
         arr = (capi.BatchScene * len(scenes))()
         for i, m in enumerate(scenes):
             arr[i].material = m.material.to_c()
             arr[i].mass = m.particle_mass
             arr[i].volume = m.particle_volume
             arr[i].n = len(m.particle_position)
-        x = np.ascontiguousarray(np.concatenate([m.particle_position for m in scenes]), np.float32)
-        v = np.ascontiguousarray(np.concatenate([
-            m.particle_velocity if len(m.particle_velocity) == len(m.particle_position)
-            else np.repeat(m.particle_velocity, len(m.particle_position), 0) for m in scenes]), np.float32)
         capi.check(L.ckmpm_add_batch(self._h, len(scenes), arr, capi.fptr(x), capi.fptr(v)), "ckmpm_add_batch",
                    self._h)
         if config.boundary == "field" and config.boundary_field is not None:

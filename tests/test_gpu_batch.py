@@ -257,3 +257,28 @@ def test_batch_relayout_changes_no_result(engine_lib):
         runs.append(b.state())
         b.close()
     assert_same_state(runs[0], runs[1], "batch with and without re-layout")
+
+
+def test_batch_from_concatenated_inputs(engine_lib):
+    """SceneBatch given the scenes' inputs already concatenated (x, v of every particle, here in
+    pinned host memory) equals the batch that concatenates them itself, bit for bit; malformed
+    arrays are refused."""
+    import torch
+    cfg, models = small_batch()
+    ref = run_batch(cfg, models, 12).state()
+    x = np.concatenate([m.particle_position for m in models]).astype(np.float32)
+    v = np.concatenate([np.broadcast_to(m.particle_velocity, m.particle_position.shape) for m in models])
+    xp = torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+    vp = torch.from_numpy(np.ascontiguousarray(v, np.float32)).pin_memory()
+    b = SceneBatch(cfg, models, x=xp.numpy(), v=vp.numpy())
+    b.setup()
+    b.step(12, DT)
+    st = b.state()
+    b.close()
+    for q in ("x", "v", "F", "aux", "id"):
+        assert np.array_equal(getattr(st, q), getattr(ref, q)), q
+    with pytest.raises(ValueError):
+        SceneBatch(cfg, models, x=x[:-1], v=v[:-1])
+    with pytest.raises(ValueError):
+        SceneBatch(cfg, models, x=x)
+
