@@ -13,6 +13,19 @@ from ckmpm_b200 import scenes
 from ckmpm_b200.batch import reduce_over_ranks, shard_scenes
 
 
+def test_scene_batch_checks_concatenated_inputs_before_any_device_call():
+    """SceneBatch(cfg, scenes, x=, v=) refuses inputs that are not the scenes' concatenation
+    (float32, C-contiguous, shape (total, 3), both or neither) before it creates anything."""
+    from ckmpm_b200.batch import SceneBatch
+    cfg, models = scenes.batched_scenes(n_scenes=3, seed=2, n_min=500, n_max=900)
+    total = sum(len(m.particle_position) for m in models)
+    good = np.zeros((total, 3), np.float32)
+    for x, v in ((good[:-1], good[:-1]), (good.astype(np.float64), good), (good, good[:, :2]),
+                 (np.asfortranarray(good), good), (good, None), (None, good)):
+        with pytest.raises(ValueError):
+            SceneBatch(cfg, models, x=x, v=v)
+
+
 def test_batched_scenes_follow_the_configuration():
     cfg, models = scenes.batched_scenes(n_scenes=48, seed=0)
     assert len(models) == 48 and cfg.domain_blocks == (16, 16, 16) and abs(cfg.dx - 1 / 64) < 1e-12
