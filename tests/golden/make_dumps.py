@@ -7,7 +7,8 @@ Run on a machine with a GPU and the reference harness built (make -C oracle ref)
 For each scene below it runs the reference's own MPMEngine twice through the harness's state
 dump (oracle/ref_runner.dump, mode 2 of oracle/ref_harness.cu) and stores, for every 8th
 particle by id of the first run, its position, the velocity the next G2P gives it, F and the
-model's scalar after 100 and 500 substeps, and per quantity the largest difference between the
+model's scalar after 100 and 500 substeps (for NACC, whose F is fixed only up to a rotation on the
+right, F F^T in place of F), and per quantity the largest difference between the
 two runs over those particles (the reference's own run-to-run spread from its float atomics; v
 relative to the first run's max |v|).  The golden position fixtures hold positions only; these
 pin the FP64 oracle's v, F and scalar too (tests/test_oracle_dumps.py).
@@ -38,7 +39,7 @@ def dump_scenes():
     yield "fluid", "jelly", cfg, m
     cfg, m = scenes.small_sand(r=0.06, h=0.15, track_ids=True)
     yield "sand_dp", "slip", cfg, m
-    for kind in ("von_mises", "linear"):
+    for kind in ("von_mises", "nacc", "linear"):
         cfg, m = scenes.material_cube(kind, track_ids=True)
         yield kind, "jelly", cfg, m
 
@@ -55,8 +56,12 @@ def main(outdir: Path) -> None:
             out[f"{name}_{k}_id"] = a["id"][keep].astype(np.uint32)
             scale_v = max(float(np.abs(a["v"]).max()), 1e-6)
             for q in QUANTITIES:
-                qa = np.asarray(a[q], np.float64)[keep].reshape(int(keep.sum()), -1)
-                qb = np.asarray(b[q], np.float64)[keep].reshape(int(keep.sum()), -1)
+                qa = np.asarray(a[q], np.float64)[keep]
+                qb = np.asarray(b[q], np.float64)[keep]
+                if q == "F" and name == "nacc":  # NACC's F is fixed only up to a rotation on the right
+                    qa, qb = qa @ qa.transpose(0, 2, 1), qb @ qb.transpose(0, 2, 1)
+                qa = qa.reshape(int(keep.sum()), -1)
+                qb = qb.reshape(int(keep.sum()), -1)
                 out[f"{name}_{k}_{q}"] = qa.astype(np.float32)
                 spread = float(np.abs(qa - qb).max()) if qa.size else 0.0
                 out[f"{name}_{k}_{q}_spread"] = np.float64(spread / scale_v if q == "v" else spread)
