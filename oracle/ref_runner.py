@@ -119,7 +119,7 @@ def dump(family: str, models, dt: float, ks, outdir: Path | None = None, timeout
     sorted by id]}}.  Ids are input indices, carried through the reference's own advection
     records; a particle the reference dropped is absent.  F is (n, 3, 3) row-major (identity
     where the model keeps none), aux the model's scalar (0 where it keeps none), v the velocity
-    the next substep's G2P gives the particle."""
+    the next substep's G2P gives the particle (zero for a rigid one, as G2P gives it)."""
     if not isinstance(models, (list, tuple)):
         models = [models]
     ks = sorted(set(int(k) for k in ks))
