@@ -7,7 +7,11 @@ import re
 import subprocess
 from pathlib import Path
 
+import pytest
+import torch
+
 from ckmpm_b200 import _capi as capi
+from ckmpm_b200 import scenes
 
 ROOT = Path(__file__).resolve().parents[1]
 
@@ -42,6 +46,40 @@ def test_null_arguments_are_rejected_without_a_device(engine_lib):
     assert engine_lib.ckmpm_setup(None) == 1
     assert engine_lib.ckmpm_step(None, 1, C.c_float(1e-4)) == 1
     assert engine_lib.ckmpm_destroy(None) == 0
+
+
+def test_scene_descriptor_is_checked_before_any_device_call(engine_lib):
+    """ckmpm_create / ckmpm_create_batch refuse a malformed descriptor with CKMPM_ERR_INVALID and a
+    message, before they look for a device; with no device a valid descriptor fails with
+    CKMPM_ERR_CUDA (there is no CPU path to fall back to)."""
+    def desc(**kw):
+        d = scenes.jelly_cube()[0].to_c()
+        for k, v in kw.items():
+            if k == "domain_blocks":
+                for a in range(3):
+                    d.domain_blocks[a] = v[a]
+            else:
+                setattr(d, k, v)
+        return d
+
+    bad = [(dict(dx=0.0), "dx"), (dict(dx=-1.0), "dx"), (dict(domain_blocks=(0, 16, 16)), "domain_blocks"),
+           (dict(domain_blocks=(4097, 16, 16)), "domain_blocks"),
+           (dict(domain_blocks=(4096, 4096, 32)), "too large"), (dict(boundary=9), "boundary"),
+           (dict(max_particles_per_block=4097), "4096")]
+    for kw, word in bad:
+        h = C.c_void_p()
+        d = desc(**kw)
+        assert engine_lib.ckmpm_create(C.byref(d), C.byref(h)) == capi.CKMPM_ERR_INVALID, kw
+        assert not h
+        assert word in engine_lib.ckmpm_last_error(None).decode(), (kw, engine_lib.ckmpm_last_error(None))
+    h = C.c_void_p()
+    d = desc()
+    assert engine_lib.ckmpm_create_batch(C.byref(d), 0, C.byref(h)) == capi.CKMPM_ERR_INVALID
+    if not torch.cuda.is_available():
+        assert engine_lib.ckmpm_create(C.byref(d), C.byref(h)) == 2  # CKMPM_ERR_CUDA
+        assert not h and "no CUDA device" in engine_lib.ckmpm_last_error(None).decode()
+    else:
+        pytest.skip("a device is present: the no-device answer is not testable here")
 
 
 def test_header_compiles_as_c():
